@@ -1,0 +1,808 @@
+// C ABI of the B200 docking engine (include/smina_b200.h): device state,
+// input validation, model packing and kernel launches.  Every entry point
+// returns a status code; no exception crosses the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "engine.h"
+
+namespace sg {
+
+// ---- launchers defined in the kernel files ---------------------------------------------------
+cudaError_t launch_cell_lists(int, const double*, const int*, const DGeom&, double, const double*, const double*, int*,
+                              const int*, int*, int, cudaStream_t);
+cudaError_t launch_grid_map64(const DGeom&, int, const double*, const int*, const double*, const int*, const int*,
+                              const DTables&, const int*, int, double**, double**, cudaStream_t);
+cudaError_t launch_grid_narrow(const double*, float*, __half*, size_t, cudaStream_t);
+size_t ws64_bytes(const DModel& hm);
+cudaError_t launch_eval64(const DModel*, size_t, const DTables&, const DReceptor*, int, const double*, const double[3],
+                          double, int, double*, double*, double*, int*, cudaStream_t);
+cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor*, int, double*, const double[3], double,
+                          int, int, int, double*, int*, cudaStream_t);
+cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
+                        const MCParams64&, int*, cudaStream_t);
+cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
+                            const double[3], int, int, int, double*, double*, int, int*, cudaStream_t);
+
+void DevBuf::reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+void DevBuf::alloc(size_t n) {
+    reset();
+    if (n == 0) n = 16;
+    if (cudaMalloc(&p, n) != cudaSuccess) {
+        p = nullptr;
+        throw EngineError(SG_ERR_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed");
+    }
+    bytes = n;
+}
+void DevBuf::upload(const void* src, size_t n, cudaStream_t s) {
+    alloc(n);
+    if (n) cuda_check(cudaMemcpyAsync(p, src, n, cudaMemcpyHostToDevice, s), "upload");
+}
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw EngineError(SG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DGeom make_geom(const sg_grid_dims& gd) {
+    DGeom g;
+    for (int i = 0; i < 3; i++) {
+        g.dim[i] = gd.n[i] + 1;
+        g.init[i] = gd.begin[i];
+        const double range = gd.end[i] - gd.begin[i];
+        g.dim_fl_minus_1[i] = g.dim[i] - 1.0;
+        g.factor[i] = g.dim_fl_minus_1[i] / range;
+        g.factor_inv[i] = 1 / g.factor[i];
+        g.gd_begin[i] = gd.begin[i];
+        g.gd_end[i] = gd.end[i];
+        g.gd_n[i] = gd.n[i];
+        g.cell_off[i] = (int)std::floor(gd.begin[i] / 3.0);
+        g.cell_dim[i] = (int)std::ceil(gd.end[i] / 3.0) - g.cell_off[i] + 1;
+    }
+    return g;
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+// ---- engine -----------------------------------------------------------------------------------
+sg_engine::~sg_engine() {
+    if (stream) cudaStreamDestroy(stream);
+}
+
+template <typename F>
+static int guarded(sg_engine* e, F f) {
+    try {
+        if (!e) return SG_ERR_ARG;
+        cuda_check(cudaSetDevice(e->device), "cudaSetDevice");
+        f();
+        return SG_OK;
+    } catch (EngineError& x) {
+        e->err = x.what();
+        return x.code;
+    } catch (std::bad_alloc&) {
+        e->err = "host allocation failed";
+        return SG_ERR_NOMEM;
+    } catch (std::exception& x) {
+        e->err = x.what();
+        return SG_ERR_ARG;
+    }
+}
+
+static void require(bool ok, const std::string& msg) {
+    if (!ok) throw EngineError(SG_ERR_ARG, msg);
+}
+
+// Reads the device error word, clears it, and turns it into a status.
+void sg_engine::check_device_errors() {
+    int h = 0;
+    cuda_check(cudaMemcpyAsync(&h, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "error word");
+    cuda_check(cudaStreamSynchronize(stream), "kernel");
+    if (h != kDevOk) {
+        const int zero = 0;
+        cuda_check(cudaMemcpy(d_err.p, &zero, sizeof(int), cudaMemcpyHostToDevice), "clear error word");
+        if (h == kDevOverlap) throw EngineError(SG_ERR_OVERLAP, "Ligand atom exactly overlaps receptor atom.");
+        throw EngineError(SG_ERR_ARG, "device reported an out-of-range access (error " + std::to_string(h) + ")");
+    }
+}
+
+extern "C" {
+
+int sg_create(int device, int precision, sg_engine** out) {
+    if (!out) return SG_ERR_ARG;
+    *out = nullptr;
+    if (precision < SG_PREC_FP64 || precision > SG_PREC_FP32_H16) return SG_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return SG_ERR_CUDA;
+    std::unique_ptr<sg_engine> e(new sg_engine());
+    e->device = device;
+    e->precision = precision;
+    int rc = guarded(e.get(), [&] {
+        cuda_check(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
+        e->d_err.alloc(sizeof(int));
+        cuda_check(cudaMemsetAsync(e->d_err.p, 0, sizeof(int), e->stream), "memset");
+        cudaDeviceProp prop;
+        cuda_check(cudaGetDeviceProperties(&prop, device), "device properties");
+        e->num_sms = prop.multiProcessorCount;
+        e->max_smem = (int)prop.sharedMemPerBlockOptin;
+    });
+    if (rc != SG_OK) return rc;
+    *out = e.release();
+    return SG_OK;
+}
+
+void sg_destroy(sg_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    delete e;
+}
+
+const char* sg_last_error(const sg_engine* e) { return e ? e->err.c_str() : "no engine"; }
+int sg_precision(const sg_engine* e) { return e ? e->precision : -1; }
+
+int sg_set_tables(sg_engine* e, const sg_tables_desc* t) {
+    return guarded(e, [&] {
+        require(t && t->smooth && t->fast, "tables: null pointers");
+        require(t->num_types == SG_NUM_TYPES, "tables: num_types must be 27");
+        require(t->num_components == 1 || t->num_components == 4, "tables: num_components must be 1 or 4");
+        require(t->factor > 0 && t->cutoff_sqr > 0, "tables: factor and cutoff must be positive");
+        require(t->n >= (int)(size_t)(t->factor * t->cutoff_sqr) + 3 && t->n < (1 << 24), "tables: n too small");
+        const size_t np = kNumTypePairs;
+        e->tab_smooth.upload(t->smooth, np * t->n * t->num_components * 2 * sizeof(double), e->stream);
+        e->tab_fast.upload(t->fast, np * t->n * t->num_components * sizeof(double), e->stream);
+        // FP32 (e, dor) pairs for the mixed-precision path (single component)
+        std::vector<float> s32;
+        if (t->num_components == 1) {
+            s32.resize(np * t->n * 2);
+            for (size_t i = 0; i < s32.size(); i++) s32[i] = (float)t->smooth[i];
+        } else {
+            s32.resize(np * t->n * 8);
+            for (size_t i = 0; i < s32.size(); i++) s32[i] = (float)t->smooth[i];
+        }
+        e->tab_smooth32.upload(s32.data(), s32.size() * sizeof(float), e->stream);
+        e->tables.nc = t->num_components;
+        e->tables.n = t->n;
+        e->tables.factor = t->factor;
+        e->tables.cutoff_sqr = t->cutoff_sqr;
+        e->tables.smooth = (const double*)e->tab_smooth.p;
+        e->tables.fast = (const double*)e->tab_fast.p;
+        e->tables.smooth32 = (const float2*)e->tab_smooth32.p;
+        e->has_tables = true;
+        for (auto& r : e->rec) r.clear_maps();  // maps depend on the tables
+        cuda_check(cudaStreamSynchronize(e->stream), "tables");
+    });
+}
+
+}  // extern "C"
+
+// ---- receptors and grid maps ----------------------------------------------------------------------
+namespace sg {
+
+RecState& receptor_for(sg_engine* e, int rid) {
+    require(rid >= 0 && rid < SG_MAX_RECEPTORS, "receptor id out of range");
+    require(e->rec[rid].set, "receptor " + std::to_string(rid) + " has not been set");
+    return e->rec[rid];
+}
+
+void refresh_header(sg_engine* e, RecState& r) {
+    DReceptor& h = r.hdr;
+    h.natoms = r.natoms;
+    h.xyz = r.xyz.as<double>();
+    h.type = r.type.as<int>();
+    h.charge = r.charge.as<double>();
+    h.pop_start = r.pop_start.as<int>();
+    h.pop_atoms = r.pop_atoms.as<int>();
+    h.full_start = r.full_start.as<int>();
+    h.full_atoms = r.full_atoms.as<int>();
+    h.g = r.geom;
+    for (int t = 0; t < kNumTypes; t++) {
+        h.map[t] = r.map64[t].as<double>();
+        h.cmap[t] = r.cmap64[t].as<double>();
+        h.map32[t] = r.map32[t].as<float>();
+        h.cmap32[t] = r.cmap32[t].as<float>();
+        h.map16[t] = r.map16[t].as<__half>();
+    }
+    if (!r.dhdr.p) r.dhdr.alloc(sizeof(DReceptor));
+    cuda_check(cudaMemcpyAsync(r.dhdr.p, &h, sizeof(DReceptor), cudaMemcpyHostToDevice, e->stream), "receptor header");
+    cuda_check(cudaStreamSynchronize(e->stream), "receptor header");
+}
+
+// build one family of cell lists (CSR) on the device
+static void build_cells(sg_engine* e, RecState& r, const std::vector<double>& lo, const std::vector<double>& hi,
+                        DevBuf& start, DevBuf& atoms) {
+    const DGeom& g = r.geom;
+    const int ncells = g.cell_dim[0] * g.cell_dim[1] * g.cell_dim[2];
+    DevBuf dlo, dhi, dcount;
+    dlo.upload(lo.data(), lo.size() * sizeof(double), e->stream);
+    dhi.upload(hi.data(), hi.size() * sizeof(double), e->stream);
+    dcount.alloc(ncells * sizeof(int));
+    cuda_check(launch_cell_lists(r.natoms, r.xyz.as<double>(), r.type.as<int>(), g, e->tables.cutoff_sqr,
+                                 dlo.as<double>(), dhi.as<double>(), dcount.as<int>(), nullptr, nullptr, 0, e->stream),
+               "cell count");
+    std::vector<int> cnt(ncells), st(ncells + 1, 0);
+    cuda_check(cudaMemcpyAsync(cnt.data(), dcount.p, ncells * sizeof(int), cudaMemcpyDeviceToHost, e->stream), "counts");
+    cuda_check(cudaStreamSynchronize(e->stream), "cell count");
+    for (int c = 0; c < ncells; c++) st[c + 1] = st[c] + cnt[c];
+    start.upload(st.data(), st.size() * sizeof(int), e->stream);
+    atoms.alloc(std::max(1, st[ncells]) * sizeof(int));
+    cuda_check(launch_cell_lists(r.natoms, r.xyz.as<double>(), r.type.as<int>(), g, e->tables.cutoff_sqr,
+                                 dlo.as<double>(), dhi.as<double>(), nullptr, start.as<int>(), atoms.as<int>(), 1,
+                                 e->stream),
+               "cell fill");
+    cuda_check(cudaStreamSynchronize(e->stream), "cell fill");
+}
+
+// Brick of every cell along each axis.  Populate: the first grid point of
+// the cell in loop order (floor/ceil of its coordinate, flat when it lies on
+// a face); direct sum: the full [3c, 3c + 3) brick.
+static void cell_bricks(const DGeom& g, bool first_query, std::vector<double>& lo, std::vector<double>& hi) {
+    lo.clear();
+    hi.clear();
+    const double nan = std::nan("");
+    for (int d = 0; d < 3; d++) {
+        std::vector<double> l(g.cell_dim[d], nan), h(g.cell_dim[d], nan);
+        if (first_query) {
+            for (int x = 0; x < g.dim[d]; x++) {
+                const double c = g.init[d] + g.factor_inv[d] * x;
+                const int cell = (int)std::floor(c / 3.0) - g.cell_off[d];
+                if (cell < 0 || cell >= g.cell_dim[d] || l[cell] == l[cell]) continue;
+                l[cell] = std::floor(c / 3.0) * 3.0;
+                h[cell] = std::ceil(c / 3.0) * 3.0;
+            }
+        } else {
+            for (int c = 0; c < g.cell_dim[d]; c++) {
+                l[c] = (double)(c + g.cell_off[d]) * 3.0;
+                h[c] = l[c] + 3.0;
+            }
+        }
+        lo.insert(lo.end(), l.begin(), l.end());
+        hi.insert(hi.end(), h.begin(), h.end());
+    }
+}
+
+void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes) {
+    require(e->has_tables, "no tables set");
+    std::vector<int> need;
+    for (int k = 0; k < ntypes; k++) {
+        const int t = types[k];
+        require(t >= 0 && t < kNumTypes, "grid type out of range");
+        if (!r.built[t] && std::find(need.begin(), need.end(), t) == need.end()) need.push_back(t);
+    }
+    if (need.empty()) return;
+    if (!r.pop_start.p) {
+        std::vector<double> lo, hi;
+        cell_bricks(r.geom, true, lo, hi);
+        build_cells(e, r, lo, hi, r.pop_start, r.pop_atoms);
+        cell_bricks(r.geom, false, lo, hi);
+        build_cells(e, r, lo, hi, r.full_start, r.full_atoms);
+    }
+    const size_t npts = (size_t)r.geom.dim[0] * r.geom.dim[1] * r.geom.dim[2];
+    const bool charged = e->tables.nc > 1;
+    std::vector<double*> maps, cmaps;
+    for (int t : need) {
+        r.map64[t].alloc(npts * sizeof(double));
+        maps.push_back(r.map64[t].as<double>());
+        if (charged) {
+            r.cmap64[t].alloc(npts * sizeof(double));
+            cmaps.push_back(r.cmap64[t].as<double>());
+        } else {
+            cmaps.push_back(nullptr);
+        }
+    }
+    DevBuf dtypes, dmaps, dcmaps;
+    dtypes.upload(need.data(), need.size() * sizeof(int), e->stream);
+    dmaps.upload(maps.data(), maps.size() * sizeof(double*), e->stream);
+    dcmaps.upload(cmaps.data(), cmaps.size() * sizeof(double*), e->stream);
+    cuda_check(launch_grid_map64(r.geom, r.natoms, r.xyz.as<double>(), r.type.as<int>(), r.charge.as<double>(),
+                                 r.pop_start.as<int>(), r.pop_atoms.as<int>(), e->tables, dtypes.as<int>(), (int)need.size(),
+                                 dmaps.as<double*>(), dcmaps.as<double*>(), e->stream),
+               "grid maps");
+    if (e->precision != SG_PREC_FP64) {
+        for (int t : need) {
+            r.map32[t].alloc(npts * sizeof(float));
+            if (e->precision == SG_PREC_FP32_H16) r.map16[t].alloc(npts * sizeof(__half));
+            cuda_check(launch_grid_narrow(r.map64[t].as<double>(), r.map32[t].as<float>(), r.map16[t].as<__half>(), npts,
+                                          e->stream),
+                       "narrow maps");
+            if (charged) {
+                r.cmap32[t].alloc(npts * sizeof(float));
+                cuda_check(launch_grid_narrow(r.cmap64[t].as<double>(), r.cmap32[t].as<float>(), nullptr, npts, e->stream),
+                           "narrow charge maps");
+            }
+        }
+    }
+    cuda_check(cudaStreamSynchronize(e->stream), "grid maps");
+    for (int t : need) r.built[t] = true;
+    refresh_header(e, r);
+}
+
+}  // namespace sg
+
+extern "C" {
+
+int sg_set_receptor(sg_engine* e, int rid, const sg_receptor_desc* r, const sg_grid_dims* gd) {
+    return guarded(e, [&] {
+        require(rid >= 0 && rid < SG_MAX_RECEPTORS, "receptor id out of range");
+        require(r && gd && r->num_atoms >= 0, "receptor: bad arguments");
+        require(r->num_atoms == 0 || (r->coords && r->type && r->charge), "receptor: null arrays");
+        require(e->has_tables, "set tables before the receptor");
+        for (int i = 0; i < 3; i++) {
+            require(gd->n[i] >= 1 && gd->n[i] <= 4096, "box: n must be in [1, 4096]");
+            require(gd->end[i] > gd->begin[i], "box: end must exceed begin");
+        }
+        for (int i = 0; i < r->num_atoms; i++) require(std::isfinite(r->coords[3 * i]) && std::isfinite(r->coords[3 * i + 1]) &&
+                                                           std::isfinite(r->coords[3 * i + 2]), "receptor: non-finite coordinate");
+        RecState& s = e->rec[rid];
+        s.clear_maps();
+        s.pop_start.reset(); s.pop_atoms.reset(); s.full_start.reset(); s.full_atoms.reset();
+        s.gd = *gd;
+        s.geom = make_geom(*gd);
+        s.natoms = r->num_atoms;
+        std::vector<int> types(r->type, r->type + r->num_atoms);
+        for (int& t : types) if (t < 0 || t > kNumTypes) t = kNumTypes;
+        s.xyz.upload(r->coords, sizeof(double) * 3 * std::max(1, r->num_atoms), e->stream);
+        s.type.upload(types.data(), sizeof(int) * std::max<size_t>(1, types.size()), e->stream);
+        s.charge.upload(r->charge, sizeof(double) * std::max(1, r->num_atoms), e->stream);
+        s.set = true;
+        std::vector<double> lo, hi;
+        cell_bricks(s.geom, true, lo, hi);
+        build_cells(e, s, lo, hi, s.pop_start, s.pop_atoms);
+        cell_bricks(s.geom, false, lo, hi);
+        build_cells(e, s, lo, hi, s.full_start, s.full_atoms);
+        refresh_header(e, s);
+    });
+}
+
+int sg_build_grids(sg_engine* e, int rid, const int* types, int ntypes) {
+    return guarded(e, [&] {
+        require(ntypes >= 0 && (ntypes == 0 || types), "build_grids: bad type list");
+        RecState& r = receptor_for(e, rid);
+        ensure_maps(e, r, types, ntypes);
+    });
+}
+
+int sg_get_grid(sg_engine* e, int rid, int type, double* data, double* chargedata) {
+    return guarded(e, [&] {
+        RecState& r = receptor_for(e, rid);
+        require(type >= 0 && type < kNumTypes && r.built[type], "grid map not built");
+        require(data != nullptr, "null output");
+        cuda_check(cudaMemcpy(data, r.map64[type].p, r.map64[type].bytes, cudaMemcpyDeviceToHost), "get grid");
+        if (chargedata && r.cmap64[type].p)
+            cuda_check(cudaMemcpy(chargedata, r.cmap64[type].p, r.cmap64[type].bytes, cudaMemcpyDeviceToHost), "get grid");
+    });
+}
+
+int sg_drop_receptor(sg_engine* e, int rid) {
+    return guarded(e, [&] {
+        require(rid >= 0 && rid < SG_MAX_RECEPTORS, "receptor id out of range");
+        RecState& s = e->rec[rid];
+        s.clear_maps();
+        s.pop_start.reset(); s.pop_atoms.reset(); s.full_start.reset(); s.full_atoms.reset();
+        s.xyz.reset(); s.type.reset(); s.charge.reset(); s.dhdr.reset();
+        s.set = false;
+    });
+}
+
+}  // extern "C"
+
+// ---- models -------------------------------------------------------------------------------------------
+namespace sg {
+
+// Validates one model descriptor on the host so that no device index can
+// leave its array, then appends its packed arrays.
+static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<double>& D, std::vector<size_t>& ioff,
+                     std::vector<size_t>& doff, DModel& hm) {
+    const int N = d.num_atoms, M = d.num_movable, F = d.num_frames, P = d.num_pairs;
+    require(N > 0 && N <= 4096 && M > 0 && M <= N, "model: atom counts out of range");
+    require(F > 0 && F <= 1024 && d.num_ligands >= 0 && d.num_flex >= 0 && d.num_ligands + d.num_flex > 0,
+            "model: frame / ligand counts out of range");
+    require(d.num_ligands <= 30, "model: at most 30 ligands per model");
+    require(P >= 0 && P <= 200000 && d.num_other_pairs >= 0 && d.num_other_pairs <= P, "model: pair counts out of range");
+    require(d.conf_size > 0 && d.conf_size <= 4096 && d.dof > 0 && d.dof <= 1024, "model: conf/dof sizes out of range");
+    require(d.atom_type && d.atom_charge && d.atom_local && d.atom_lab && d.frame_kind && d.frame_parent &&
+                d.frame_begin && d.frame_end && d.frame_conf && d.frame_dof && d.frame_origin && d.frame_axis &&
+                d.frame_init_origin && (P == 0 || d.pairs) && (d.num_ligands == 0 || (d.lig_pair_end &&
+                d.ligand_atom_begin && d.ligand_atom_end && d.ligand_root)),
+            "model: null arrays");
+    // frames
+    std::vector<int> depth(F, 0), atom_frame(N, -1);
+    int nlevels = 1, nlig_roots = 0, nflex_roots = 0;
+    for (int f = 0; f < F; f++) {
+        const int k = d.frame_kind[f], p = d.frame_parent[f];
+        require(k >= 0 && k <= 2, "model: bad frame kind");
+        require((k == SG_FRAME_SEGMENT) == (p >= 0), "model: only segments have parents");
+        require(p < f, "model: frames must be in depth-first order");
+        depth[f] = p < 0 ? 0 : depth[p] + 1;
+        nlevels = std::max(nlevels, depth[f] + 1);
+        require(d.frame_begin[f] >= 0 && d.frame_begin[f] <= d.frame_end[f] && d.frame_end[f] <= M,
+                "model: frame atom range out of range");
+        for (int i = d.frame_begin[f]; i < d.frame_end[f]; i++) {
+            require(atom_frame[i] < 0, "model: frames overlap");
+            atom_frame[i] = f;
+        }
+        if (k == SG_FRAME_RIGID) {
+            require(d.frame_conf[f] >= 0 && d.frame_conf[f] + 7 <= d.conf_size && d.frame_dof[f] >= 0 &&
+                        d.frame_dof[f] + 6 <= d.dof, "model: rigid conf/dof offsets out of range");
+            nlig_roots++;
+        } else {
+            require(d.frame_conf[f] >= 0 && d.frame_conf[f] < d.conf_size && d.frame_dof[f] >= 0 && d.frame_dof[f] < d.dof,
+                    "model: torsion conf/dof offsets out of range");
+            if (k == SG_FRAME_FIRST_SEGMENT) nflex_roots++;
+        }
+        for (int j = 0; j < 3; j++)
+            require(std::isfinite(d.frame_origin[3 * f + j]) && std::isfinite(d.frame_axis[3 * f + j]) &&
+                        std::isfinite(d.frame_init_origin[3 * f + j]), "model: non-finite frame data");
+    }
+    require(nlig_roots == d.num_ligands && nflex_roots == d.num_flex, "model: root counts disagree with ligands/flex");
+    for (int i = 0; i < M; i++) require(atom_frame[i] >= 0, "model: a movable atom belongs to no frame");
+    for (int i = 0; i < N; i++) {
+        require(d.atom_type[i] >= 0 && d.atom_type[i] <= kNumTypes, "model: atom type out of range");
+        for (int j = 0; j < 3; j++)
+            require(std::isfinite(d.atom_local[3 * i + j]) && std::isfinite(d.atom_lab[3 * i + j]), "model: non-finite atom data");
+    }
+    for (int l = 0; l < d.num_ligands; l++) {
+        require(d.ligand_root[l] >= 0 && d.ligand_root[l] < F && d.frame_kind[d.ligand_root[l]] == SG_FRAME_RIGID,
+                "model: ligand root is not a rigid frame");
+        require(d.ligand_atom_begin[l] >= 0 && d.ligand_atom_begin[l] <= d.ligand_atom_end[l] && d.ligand_atom_end[l] <= M,
+                "model: ligand atom range out of range");
+        const int prev = l == 0 ? d.num_other_pairs : d.lig_pair_end[l - 1];
+        require(d.lig_pair_end[l] >= prev && d.lig_pair_end[l] <= P, "model: ligand pair ranges out of order");
+    }
+    require(d.num_ligands == 0 || d.lig_pair_end[d.num_ligands - 1] == P, "model: pairs not covered by ligand ranges");
+    if (d.num_ligands == 0) require(d.num_other_pairs == P, "model: pairs not covered");
+    // levels, children
+    std::vector<int> level_start(nlevels + 1, 0), level_frames;
+    for (int lv = 0; lv < nlevels; lv++) {
+        level_start[lv] = (int)level_frames.size();
+        for (int f = 0; f < F; f++) if (depth[f] == lv) level_frames.push_back(f);
+    }
+    level_start[nlevels] = (int)level_frames.size();
+    std::vector<int> child_start(F + 1, 0), child_list;
+    for (int f = 0; f < F; f++) {
+        child_start[f] = (int)child_list.size();
+        for (int c = f + 1; c < F; c++) if (d.frame_parent[c] == f) child_list.push_back(c);
+    }
+    child_start[F] = (int)child_list.size();
+    // pairs, groups, per-atom ordered pair lists
+    std::vector<int> group(P, 0);
+    for (int k = 0; k < P; k++) {
+        const int a = d.pairs[2 * k], b = d.pairs[2 * k + 1];
+        require(a >= 0 && a < N && b >= 0 && b < N && a != b, "model: pair atom out of range");
+        if (k >= d.num_other_pairs)
+            for (int l = 0; l < d.num_ligands; l++)
+                if (k < d.lig_pair_end[l]) { group[k] = l + 1; break; }
+    }
+    std::vector<std::vector<int>> lists(M);
+    for (int k = 0; k < P; k++) {
+        const int a = d.pairs[2 * k], b = d.pairs[2 * k + 1];
+        if (a < M) lists[a].push_back(k << 1);
+        if (b < M) lists[b].push_back((k << 1) | 1);
+    }
+    std::vector<int> csr_start(M + 1, 0), csr;
+    for (int i = 0; i < M; i++) {
+        csr_start[i] = (int)csr.size();
+        csr.insert(csr.end(), lists[i].begin(), lists[i].end());
+    }
+    csr_start[M] = (int)csr.size();
+    std::vector<int> heavy;
+    for (int i = 0; i < M; i++) if (!is_h(d.atom_type[i])) heavy.push_back(i);
+    // conf blocks (ligands, then flexible residues) and their torsions
+    std::vector<int> root_of(F);
+    for (int f = 0; f < F; f++) root_of[f] = d.frame_parent[f] < 0 ? f : root_of[d.frame_parent[f]];
+    std::vector<int> blk_rigid, blk_conf, blk_dof, blk_ntors, tor_conf, tor_dof, tor_frame;
+    for (int pass = 0; pass < 2; pass++)
+        for (int f = 0; f < F; f++) {
+            if (d.frame_parent[f] >= 0) continue;
+            const bool rigid = d.frame_kind[f] == SG_FRAME_RIGID;
+            if ((pass == 0) != rigid) continue;
+            blk_rigid.push_back(rigid);
+            blk_conf.push_back(d.frame_conf[f]);
+            blk_dof.push_back(d.frame_dof[f]);
+            int nt = 0;
+            for (int g = 0; g < F; g++)
+                if (root_of[g] == f && d.frame_kind[g] != SG_FRAME_RIGID) {
+                    const int expect_c = d.frame_conf[f] + (rigid ? 7 : 0) + nt;
+                    const int expect_d = d.frame_dof[f] + (rigid ? 6 : 0) + nt;
+                    require(d.frame_conf[g] == expect_c && d.frame_dof[g] == expect_d,
+                            "model: torsions must follow their block in depth-first order");
+                    tor_conf.push_back(d.frame_conf[g]);
+                    tor_dof.push_back(d.frame_dof[g]);
+                    tor_frame.push_back(g);
+                    nt++;
+                }
+            blk_ntors.push_back(nt);
+        }
+    // pack
+    auto pi = [&](const int* src, size_t n) { ioff.push_back(I.size()); I.insert(I.end(), src, src + n); };
+    auto pv = [&](const std::vector<int>& v) { ioff.push_back(I.size()); I.insert(I.end(), v.begin(), v.end()); I.push_back(0); };
+    auto pd = [&](const double* src, size_t n) { doff.push_back(D.size()); D.insert(D.end(), src, src + n); };
+    ioff.clear();
+    doff.clear();
+    const size_t i0 = I.size(), d0 = D.size();
+    (void)i0; (void)d0;
+    pi(d.atom_type, N); pi(d.frame_kind, F); pi(d.frame_parent, F); pi(d.frame_begin, F); pi(d.frame_end, F);
+    pi(d.frame_conf, F); pi(d.frame_dof, F);
+    pv(atom_frame); pv(level_start); pv(level_frames); pv(child_start); pv(child_list);
+    if (P) pi(d.pairs, 2 * (size_t)P); else pv({});
+    pv(group); pv(csr_start); pv(csr); pv(heavy);
+    std::vector<int> lb(d.ligand_atom_begin, d.ligand_atom_begin + d.num_ligands),
+        le(d.ligand_atom_end, d.ligand_atom_end + d.num_ligands), lr(d.ligand_root, d.ligand_root + d.num_ligands),
+        lp(d.lig_pair_end, d.lig_pair_end + d.num_ligands);
+    pv(lb); pv(le); pv(lr); pv(lp);
+    pv(blk_rigid); pv(blk_conf); pv(blk_dof); pv(blk_ntors); pv(tor_conf); pv(tor_dof); pv(tor_frame);
+    pd(d.atom_charge, N); pd(d.atom_local, 3 * (size_t)N); pd(d.atom_lab, 3 * (size_t)N);
+    pd(d.frame_origin, 3 * (size_t)F); pd(d.frame_axis, 3 * (size_t)F); pd(d.frame_init_origin, 3 * (size_t)F);
+    hm.natoms = N; hm.nmov = M; hm.nframes = F; hm.nlig = d.num_ligands; hm.nflex = d.num_flex;
+    hm.conf_size = d.conf_size; hm.dof = d.dof; hm.npairs = P; hm.nother = d.num_other_pairs;
+    hm.nheavy = (int)heavy.size(); hm.nlevels = nlevels; hm.nblocks = (int)blk_rigid.size();
+    hm.ntors = (int)tor_conf.size();
+    require(hm.ntors + 6 * d.num_ligands == d.dof, "model: dof disagrees with the torsion count");
+}
+
+void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedModels& out) {
+    require(models && nmodels > 0 && nmodels <= (1 << 20), "models: bad array");
+    std::vector<int> I;
+    std::vector<double> D;
+    std::vector<std::vector<size_t>> ioffs(nmodels), doffs(nmodels);
+    out.host.assign(nmodels, DModel{});
+    for (int k = 0; k < nmodels; k++) pack_one(models[k], I, D, ioffs[k], doffs[k], out.host[k]);
+    out.ints.upload(I.data(), std::max<size_t>(1, I.size()) * sizeof(int), e->stream);
+    out.dbls.upload(D.data(), std::max<size_t>(1, D.size()) * sizeof(double), e->stream);
+    const int* ib = out.ints.as<int>();
+    const double* db = out.dbls.as<double>();
+    out.max_ws64 = 0;
+    for (int k = 0; k < nmodels; k++) {
+        DModel& h = out.host[k];
+        const std::vector<size_t>& io = ioffs[k];
+        const std::vector<size_t>& dd = doffs[k];
+        int j = 0;
+        h.type = ib + io[j++]; h.fkind = ib + io[j++]; h.fparent = ib + io[j++]; h.fbegin = ib + io[j++];
+        h.fend = ib + io[j++]; h.fconf = ib + io[j++]; h.fdof = ib + io[j++];
+        h.atom_frame = ib + io[j++]; h.level_start = ib + io[j++]; h.level_frames = ib + io[j++];
+        h.child_start = ib + io[j++]; h.child_list = ib + io[j++]; h.pairs = ib + io[j++];
+        h.pair_group = ib + io[j++]; h.csr_start = ib + io[j++]; h.csr = ib + io[j++]; h.heavy = ib + io[j++];
+        h.lig_begin = ib + io[j++]; h.lig_end = ib + io[j++]; h.lig_root = ib + io[j++]; h.lig_pair_end = ib + io[j++];
+        h.blk_rigid = ib + io[j++]; h.blk_conf = ib + io[j++]; h.blk_dof = ib + io[j++]; h.blk_ntors = ib + io[j++];
+        h.tor_conf = ib + io[j++]; h.tor_dof = ib + io[j++]; h.tor_frame = ib + io[j++];
+        int q = 0;
+        h.charge = db + dd[q++]; h.local = db + dd[q++]; h.lab = db + dd[q++];
+        h.forigin = db + dd[q++]; h.faxis = db + dd[q++]; h.finit = db + dd[q++];
+        out.max_ws64 = std::max(out.max_ws64, ws64_bytes(h));
+        out.max_conf = std::max(out.max_conf, h.conf_size);
+        out.max_dof = std::max(out.max_dof, h.dof);
+        out.max_heavy = std::max(out.max_heavy, h.nheavy);
+        out.max_atoms = std::max(out.max_atoms, h.natoms);
+        out.max_pairs = std::max(out.max_pairs, h.npairs);
+        out.max_frames = std::max(out.max_frames, h.nframes);
+    }
+    out.dmodels.upload(out.host.data(), out.host.size() * sizeof(DModel), e->stream);
+    cuda_check(cudaStreamSynchronize(e->stream), "model upload");
+}
+
+void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels) {
+    std::vector<int> types;
+    for (int k = 0; k < nmodels; k++)
+        for (int i = 0; i < models[k].num_movable; i++) {
+            const int t = models[k].atom_type[i];
+            if (t < kNumTypes && !is_h(t)) types.push_back(t);
+        }
+    (void)pm;
+    ensure_maps(e, r, types.data(), (int)types.size());
+}
+
+}  // namespace sg
+
+// device buffer that receives results and is copied back
+template <typename T>
+struct Staged {
+    sg::DevBuf d;
+    size_t n = 0;
+    void make(size_t count, cudaStream_t s, const T* init = nullptr) {
+        n = count;
+        d.alloc(std::max<size_t>(1, n) * sizeof(T));
+        if (init) sg::cuda_check(cudaMemcpyAsync(d.p, init, n * sizeof(T), cudaMemcpyHostToDevice, s), "stage in");
+    }
+    T* p() { return d.as<T>(); }
+    void fetch(T* host, cudaStream_t s) {
+        if (host && n) sg::cuda_check(cudaMemcpyAsync(host, d.p, n * sizeof(T), cudaMemcpyDeviceToHost, s), "stage out");
+    }
+};
+
+extern "C" {
+
+static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, const double* confs, const double v[3],
+                       double slope, double* out_e, double* out_g, double* out_coords, int direct) {
+    return guarded(e, [&] {
+        require(m && confs && v && out_e && out_g && nconfs > 0 && nconfs <= (1 << 24), "eval: bad arguments");
+        require(e->has_tables, "no tables set");
+        RecState& r = receptor_for(e, rid);
+        PackedModels pm;
+        pack_models(e, m, 1, pm);
+        if (!direct) ensure_model_maps(e, r, pm, m, 1);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        const DModel& h = pm.host[0];
+        Staged<double> dc, de, dg, dx;
+        dc.make((size_t)nconfs * h.conf_size, e->stream, confs);
+        de.make(nconfs, e->stream);
+        dg.make((size_t)nconfs * h.dof, e->stream);
+        if (out_coords) dx.make((size_t)nconfs * h.nmov * 3, e->stream);
+        cuda_check(launch_eval64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), nconfs, dc.p(), v,
+                                 slope, direct, de.p(), dg.p(), out_coords ? dx.p() : nullptr, e->d_err.as<int>(), e->stream),
+                   "eval launch");
+        de.fetch(out_e, e->stream);
+        dg.fetch(out_g, e->stream);
+        if (out_coords) dx.fetch(out_coords, e->stream);
+        e->check_device_errors();
+    });
+}
+
+int sg_eval(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, const double* confs, const double v[3],
+            double slope, double* out_e, double* out_g, double* out_coords) {
+    return eval_common(e, rid, m, nconfs, confs, v, slope, out_e, out_g, out_coords, 0);
+}
+
+int sg_eval_direct(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, const double* confs, const double v[3],
+                   double slope, double* out_e, double* out_g) {
+    return eval_common(e, rid, m, nconfs, confs, v, slope, out_e, out_g, nullptr, 1);
+}
+
+int sg_bfgs(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, double* confs, const double v[3], double slope,
+            int maxiters, int accurate_line, int early_term, double* out_e) {
+    return guarded(e, [&] {
+        require(m && confs && v && out_e && nconfs > 0 && maxiters >= 0, "bfgs: bad arguments");
+        RecState& r = receptor_for(e, rid);
+        PackedModels pm;
+        pack_models(e, m, 1, pm);
+        ensure_model_maps(e, r, pm, m, 1);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        const DModel& h = pm.host[0];
+        Staged<double> dc, de;
+        dc.make((size_t)nconfs * h.conf_size, e->stream, confs);
+        de.make(nconfs, e->stream);
+        cuda_check(launch_bfgs64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), nconfs, dc.p(), v,
+                                 slope, maxiters, accurate_line, early_term, de.p(), e->d_err.as<int>(), e->stream),
+                   "bfgs launch");
+        dc.fetch(confs, e->stream);
+        de.fetch(out_e, e->stream);
+        e->check_device_errors();
+    });
+}
+
+int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const sg_chain_input* chains, int nchains,
+            const sg_mc_params* p, sg_chain_result* out) {
+    return guarded(e, [&] {
+        require(chains && p && out && nchains > 0 && nchains <= (1 << 22), "dock: bad arguments");
+        require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->maxiters >= 0 && p->temperature > 0,
+                "dock: bad search parameters");
+        RecState& r = receptor_for(e, rid);
+        PackedModels pm;
+        pack_models(e, models, nmodels, pm);
+        ensure_model_maps(e, r, pm, models, nmodels);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        const int S = p->num_saved_mins;
+        // per-chain inputs and result storage (one device allocation each)
+        std::vector<double> conf0;
+        std::vector<uint32_t> mt((size_t)nchains * 625);
+        std::vector<size_t> conf_off(nchains), cres_off(nchains), xres_off(nchains);
+        size_t nconf_res = 0, nxyz_res = 0;
+        for (int k = 0; k < nchains; k++) {
+            const sg_chain_input& c = chains[k];
+            require(c.model >= 0 && c.model < nmodels && c.conf && c.mt, "dock: bad chain input");
+            require(c.mt[624] <= 624, "dock: mt19937 index out of range");
+            const DModel& h = pm.host[c.model];
+            conf_off[k] = conf0.size();
+            conf0.insert(conf0.end(), c.conf, c.conf + h.conf_size);
+            std::memcpy(&mt[(size_t)k * 625], c.mt, 625 * sizeof(uint32_t));
+            cres_off[k] = nconf_res;
+            nconf_res += (size_t)S * h.conf_size;
+            xres_off[k] = nxyz_res;
+            nxyz_res += (size_t)S * h.nheavy * 3;
+            require(out[k].e && out[k].conf && out[k].coords, "dock: null result arrays");
+        }
+        Staged<double> d_conf0, d_e, d_conf, d_xyz;
+        Staged<uint32_t> d_mt;
+        Staged<int> d_order, d_count;
+        Staged<unsigned long long> d_evals;
+        d_conf0.make(conf0.size(), e->stream, conf0.data());
+        d_mt.make(mt.size(), e->stream, mt.data());
+        d_e.make((size_t)nchains * S, e->stream);
+        d_conf.make(nconf_res, e->stream);
+        d_xyz.make(nxyz_res, e->stream);
+        d_order.make((size_t)nchains * S, e->stream);
+        d_count.make(nchains, e->stream);
+        d_evals.make(nchains, e->stream);
+        std::vector<Chain64> hc(nchains);
+        for (int k = 0; k < nchains; k++) {
+            hc[k].model = chains[k].model;
+            hc[k].steps = chains[k].num_steps;
+            hc[k].conf0 = d_conf0.p() + conf_off[k];
+            hc[k].mt = d_mt.p() + (size_t)k * 625;
+            hc[k].out_e = d_e.p() + (size_t)k * S;
+            hc[k].out_conf = d_conf.p() + cres_off[k];
+            hc[k].out_coords = d_xyz.p() + xres_off[k];
+            hc[k].out_order = d_order.p() + (size_t)k * S;
+            hc[k].out_count = d_count.p() + k;
+            hc[k].evals = d_evals.p() + k;
+        }
+        DevBuf d_chains;
+        d_chains.upload(hc.data(), hc.size() * sizeof(Chain64), e->stream);
+        MCParams64 P;
+        P.num_steps = p->num_steps;
+        P.temperature = p->temperature;
+        P.amplitude = p->mutation_amplitude;
+        P.min_rmsd = p->min_rmsd;
+        P.num_saved = S;
+        for (int i = 0; i < 3; i++) { P.hunt[i] = p->hunt_cap[i]; P.auth[i] = p->authentic_v[i]; }
+        P.maxiters = p->maxiters;
+        P.accurate_line = p->accurate_line;
+        P.early_term = p->early_term;
+        P.slope = p->cache_slope;
+        cuda_check(launch_mc64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(),
+                               d_chains.as<Chain64>(), nchains, P, e->d_err.as<int>(), e->stream),
+                   "dock launch");
+        std::vector<double> he((size_t)nchains * S), hconf(nconf_res), hxyz(nxyz_res);
+        std::vector<int> horder((size_t)nchains * S), hcount(nchains);
+        std::vector<unsigned long long> hev(nchains);
+        d_e.fetch(he.data(), e->stream);
+        d_conf.fetch(hconf.data(), e->stream);
+        d_xyz.fetch(hxyz.data(), e->stream);
+        d_order.fetch(horder.data(), e->stream);
+        d_count.fetch(hcount.data(), e->stream);
+        d_evals.fetch(hev.data(), e->stream);
+        e->check_device_errors();
+        for (int k = 0; k < nchains; k++) {
+            const DModel& h = pm.host[chains[k].model];
+            const int cnt = std::min(std::max(hcount[k], 0), S);
+            out[k].count = cnt;
+            out[k].evals = hev[k];
+            for (int j = 0; j < cnt; j++) {
+                const int slot = horder[(size_t)k * S + j];
+                require(slot >= 0 && slot < S, "dock: corrupt result order");
+                out[k].e[j] = he[(size_t)k * S + slot];
+                std::memcpy(out[k].conf + (size_t)j * h.conf_size, &hconf[cres_off[k] + (size_t)slot * h.conf_size],
+                            h.conf_size * sizeof(double));
+                std::memcpy(out[k].coords + (size_t)j * h.nheavy * 3, &hxyz[xres_off[k] + (size_t)slot * h.nheavy * 3],
+                            (size_t)h.nheavy * 3 * sizeof(double));
+            }
+        }
+    });
+}
+
+int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const int* pose_model, int nposes,
+              double* confs, const double cap[3], int maxiters, int accurate_line, int early_term, double* out_e,
+              double* out_coords) {
+    return guarded(e, [&] {
+        require(pose_model && confs && cap && out_e && nposes > 0 && maxiters >= 0, "refine: bad arguments");
+        RecState& r = receptor_for(e, rid);
+        PackedModels pm;
+        pack_models(e, models, nmodels, pm);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        for (int k = 0; k < nposes; k++) require(pose_model[k] >= 0 && pose_model[k] < nmodels, "refine: bad pose model");
+        const int cs = pm.max_conf, hs = pm.max_heavy;
+        Staged<double> dc, de, dx;
+        Staged<int> dpm;
+        dc.make((size_t)nposes * cs, e->stream, confs);
+        de.make(nposes, e->stream);
+        dx.make((size_t)nposes * hs * 3, e->stream);
+        dpm.make(nposes, e->stream, pose_model);
+        cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(), nposes,
+                                   dc.p(), cs, cap, maxiters, accurate_line, early_term, de.p(), dx.p(), hs,
+                                   e->d_err.as<int>(), e->stream),
+                   "refine launch");
+        dc.fetch(confs, e->stream);
+        de.fetch(out_e, e->stream);
+        if (out_coords) dx.fetch(out_coords, e->stream);
+        e->check_device_errors();
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+// Device-resident data of the engine: pair tables, receptor + grid maps,
+// packed docking models, and the launch parameters of the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include "../../include/smina_b200.h"
+#include "sg_math.cuh"
+
+namespace sg {
+
+constexpr int kNumTypes = SG_NUM_TYPES;
+constexpr int kNumTypePairs = kNumTypes * (kNumTypes + 1) / 2;
+
+SG_HD int tri_index(int i, int j) { return i + j * (j + 1) / 2; }  // i <= j
+SG_HD bool is_h(int t) { return t == 0 || t == 1; }
+
+// precalculate_linear tables
+struct DTables {
+    int nc, n;
+    double factor, cutoff_sqr;
+    const double* smooth;  // [pair][n][nc][2]
+    const double* fast;    // [pair][n][nc]
+    const float2* smooth32;  // [pair][n] (e, dor) for nc == 1, FP32 path
+};
+
+// grid_dims + grid::init geometry
+struct DGeom {
+    int dim[3];                  // n + 1 samples per axis
+    double init[3], factor[3], factor_inv[3], dim_fl_minus_1[3];
+    double gd_begin[3], gd_end[3];
+    int gd_n[3];
+    // 3 A receptor cell lists (szv_grid)
+    int cell_off[3], cell_dim[3];
+};
+
+struct DReceptor {
+    int natoms;
+    const double* xyz;     // [n][3]
+    const int* type;
+    const double* charge;
+    // cell lists for grid construction (first-query bricks) and for the
+    // direct evaluation (full 3 A bricks)
+    const int* pop_start;   // [ncells + 1]
+    const int* pop_atoms;
+    const int* full_start;  // [ncells + 1]
+    const int* full_atoms;
+    DGeom g;
+    const double* map[kNumTypes];        // FP64 maps or null
+    const double* cmap[kNumTypes];       // FP64 charge maps or null
+    const float* map32[kNumTypes];       // FP32 copies
+    const float* cmap32[kNumTypes];
+    const __half* map16[kNumTypes];      // FP16 copies
+};
+
+// A docking model packed for the device.  Arrays index into two pools
+// (ints, doubles); see pack_model() in engine.cu for the layout.
+struct DModel {
+    int natoms, nmov, nframes, nlig, nflex, conf_size, dof, npairs, nother, nheavy, nlevels, nblocks;
+    const int* type;
+    const double* charge;
+    const double* local;      // [natoms][3]
+    const double* lab;        // [natoms][3]
+    const int* atom_frame;    // [natoms], -1 for inflex
+    const int* fkind;
+    const int* fparent;
+    const int* fbegin;
+    const int* fend;
+    const int* fconf;
+    const int* fdof;
+    const double* forigin;    // [F][3]
+    const double* faxis;
+    const double* finit;
+    const int* level_start;   // [nlevels + 1]
+    const int* level_frames;  // frames by depth
+    const int* child_start;   // [F + 1]
+    const int* child_list;
+    const int* pairs;         // [P][2]
+    const int* pair_group;    // [P] 0 = other pairs (v[2]), l + 1 = ligand l (v[0])
+    const int* csr_start;     // [natoms + 1]
+    const int* csr;           // (pair << 1) | (atom is b)
+    const int* heavy;         // [nheavy]
+    const int* lig_begin;
+    const int* lig_end;
+    const int* lig_root;
+    const int* lig_pair_end;
+    const int* blk_rigid;     // [nblocks] conf blocks: ligands then flex
+    const int* blk_conf;
+    const int* blk_dof;
+    const int* blk_ntors;
+    int ntors;
+    const int* tor_conf;      // [ntors] conf index of each torsion (block order)
+    const int* tor_dof;       // [ntors] change index
+    const int* tor_frame;     // [ntors] frame of each torsion
+};
+
+// Per-warp FP64 workspace layout in shared memory (offsets in doubles)
+struct Ws64 {
+    int coords, mf, eatom, origin, axis, q, rot, fF, fT, pe, pf, pin;
+    int x_tmp, x_cand, x_new, x_orig, g, g_new, g_orig, p, y, mhy, h, bcast, rmsd, mt;
+    int total;  // doubles
+};
+
+SG_HD Ws64 ws64_layout(int natoms, int nframes, int npairs, int conf, int dof) {
+    Ws64 w;
+    int o = 0;
+    auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };
+    w.coords = take(3 * natoms);
+    w.mf = take(3 * natoms);
+    w.eatom = take(natoms);
+    w.origin = take(3 * nframes);
+    w.axis = take(3 * nframes);
+    w.q = take(4 * nframes);
+    w.rot = take(9 * nframes);
+    w.fF = take(3 * nframes);
+    w.fT = take(3 * nframes);
+    w.pe = take(npairs);
+    w.pf = take(3 * npairs);
+    w.pin = take((npairs + 7) / 8);  // one byte per pair
+    w.x_tmp = take(conf);
+    w.x_cand = take(conf);
+    w.x_new = take(conf);
+    w.x_orig = take(conf);
+    w.g = take(dof);
+    w.g_new = take(dof);
+    w.g_orig = take(dof);
+    w.p = take(dof);
+    w.y = take(dof);
+    w.mhy = take(dof);
+    w.h = take(dof * (dof + 1) / 2);
+    w.bcast = take(16);
+    w.rmsd = take(64);
+    w.mt = take(313);  // 625 uint32 words + padding
+    w.total = o;
+    return w;
+}
+
+// Chain bookkeeping for the plain path (global memory)
+struct Chain64 {
+    int model;
+    unsigned steps;
+    const double* conf0;
+    uint32_t* mt;        // [625] state (read + written)
+    double* out_e;       // [num_saved]
+    double* out_conf;    // [num_saved][conf_size]
+    double* out_coords;  // [num_saved][nheavy][3]
+    int* out_order;      // [num_saved] sorted order of the slots
+    int* out_count;
+    unsigned long long* evals;
+};
+
+struct MCParams64 {
+    unsigned num_steps;
+    double temperature, amplitude, min_rmsd;
+    int num_saved;
+    double hunt[3], auth[3];
+    int maxiters, accurate_line, early_term;
+    double slope;
+};
+
+// device error word (bounded failures report here instead of trapping)
+enum : int { kDevOk = 0, kDevOverlap = 1, kDevBadModel = 2 };
+
+}  // namespace sg

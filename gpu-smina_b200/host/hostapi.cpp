@@ -1,0 +1,123 @@
+/*
+ * C entry points of the host library (sgh_*): building models, receptors,
+ * pair tables, boxes, search parameters and chain seeds as the flat
+ * descriptors of include/smina_b200.h.  Errors come back as a non-zero
+ * status with a message in sgh_last_error().
+ */
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include "sg_host.h"
+#include "../../include/smina_b200_host.h"
+
+struct sgh_model { sgh::Model m; };
+struct sgh_receptor {
+    sgh::Receptor r;
+    std::vector<double> xyz, q;
+    std::vector<int> t;
+};
+struct sgh_tables { sgh::Tables t; };
+
+static thread_local std::string g_err;
+
+template <typename F>
+static int guarded(F f) {
+    try {
+        f();
+        return SG_OK;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return SG_ERR_ARG;
+    }
+}
+
+extern "C" {
+
+const char* sgh_last_error(void) { return g_err.c_str(); }
+
+int sgh_model_from_pdbqt(const char* text, sgh_model** out) {
+    *out = nullptr;
+    return guarded([&] {
+        sgh_model* m = new sgh_model();
+        try { m->m = sgh::read_pdbqt_ligand(text); } catch (...) { delete m; throw; }
+        *out = m;
+    });
+}
+void sgh_model_free(sgh_model* m) { delete m; }
+int sgh_model_desc(const sgh_model* m, sg_model_desc* out) {
+    *out = m->m.desc();
+    return SG_OK;
+}
+int sgh_model_heavy(const sgh_model* m) { return m->m.num_heavy_movable(); }
+int sgh_model_torsdof(const sgh_model* m) { return m->m.torsdof; }
+
+int sgh_make_receptor(int heavy_atoms, uint64_t seed, const double center[3], double cavity_radius,
+                      sgh_receptor** out) {
+    *out = nullptr;
+    return guarded([&] {
+        sgh_receptor* r = new sgh_receptor();
+        r->r = sgh::make_receptor(heavy_atoms, seed, center, cavity_radius);
+        *out = r;
+    });
+}
+void sgh_receptor_free(sgh_receptor* r) { delete r; }
+int sgh_receptor_desc(sgh_receptor* r, sg_receptor_desc* out) {
+    *out = r->r.desc(r->xyz, r->t, r->q);
+    return SG_OK;
+}
+int sgh_receptor_pdbqt(const sgh_receptor* r, char* buf, int buflen) {
+    std::string s = sgh::receptor_pdbqt(r->r);
+    if ((int)s.size() + 1 > buflen) return (int)s.size() + 1;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return 0;
+}
+
+int sgh_make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3], char* buf, int buflen) {
+    std::string s;
+    int rc = guarded([&] { s = sgh::make_ligand_pdbqt(heavy, rotors, seed, center); });
+    if (rc) return -1;
+    if ((int)s.size() + 1 > buflen) return (int)s.size() + 1;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return 0;
+}
+
+int sgh_tables_create(const char* builtin_name, const char* custom_text, double factor, sgh_tables** out) {
+    *out = nullptr;
+    return guarded([&] {
+        sgh::Scoring sf;
+        if (custom_text && *custom_text) sgh::scoring_from_text(custom_text, sf);
+        else if (!sgh::builtin_scoring(builtin_name ? builtin_name : "vina", sf))
+            throw std::runtime_error(std::string("unknown builtin scoring function ") + builtin_name);
+        if (sf.indep.empty() && sf.dep.empty()) throw std::runtime_error("scoring function has no distance terms");
+        sgh_tables* t = new sgh_tables();
+        sgh::build_linear_tables(sf, factor, t->t);
+        *out = t;
+    });
+}
+void sgh_tables_free(sgh_tables* t) { delete t; }
+int sgh_tables_desc(const sgh_tables* t, sg_tables_desc* out) {
+    *out = t->t.desc();
+    return SG_OK;
+}
+
+int sgh_make_box(const double center[3], const double size[3], double granularity, sg_grid_dims* out) {
+    *out = sgh::make_box(center, size, granularity);
+    return SG_OK;
+}
+
+int sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out) {
+    *out = sgh::search_params(m->m, num_modes);
+    return SG_OK;
+}
+
+int sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims* box, double* confs, uint32_t* mt) {
+    return guarded([&] {
+        std::vector<sgh::ChainStart> cs = sgh::seed_chains(m->m, seed, tasks, *box);
+        for (int k = 0; k < tasks; k++) {
+            std::memcpy(confs + (size_t)k * m->m.conf_size, cs[k].conf.data(), m->m.conf_size * sizeof(double));
+            std::memcpy(mt + (size_t)k * 625, cs[k].mt, 625 * sizeof(uint32_t));
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,396 @@
+"""Python binding of the B200 docking engine (ctypes over the C ABI).
+
+The compute lives in ``libsmina_b200.so`` (CUDA kernels for sm_100a plus the
+C++ host library); this module only marshals numpy arrays into the flat
+descriptors of ``include/smina_b200.h`` / ``include/smina_b200_host.h``.
+There is no CPU fallback: :func:`load` raises if the library is missing.
+
+Reference interfaces mirrored (paths inside the reference project):
+  Engine.eval        model::eval_deriv                 src/lib/model.cpp:969-985
+  Engine.dock        monte_carlo::operator() per chain  src/lib/monte_carlo.cpp:95-130
+  Engine.refine      refine_structure                  src/main/main.cpp:165-190
+  Engine.grid        cache::populate                   src/lib/cache.cpp:116-206
+  GpuDocking         gpusmina::GpuDocking              src/gpu/gpu_docking.h:51-114
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsmina_b200.so")
+
+SG_OK, SG_ERR_ARG, SG_ERR_CUDA, SG_ERR_NOMEM, SG_ERR_OVERLAP, SG_ERR_TIMEOUT, SG_ERR_STATE = range(7)
+PREC_FP64, PREC_FP32, PREC_FP32_H16 = 0, 1, 2
+NUM_TYPES = 27
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_up = C.POINTER(C.c_uint32)
+
+
+class GridDims(C.Structure):
+    _fields_ = [("begin", C.c_double * 3), ("end", C.c_double * 3), ("n", C.c_int * 3)]
+
+
+class TablesDesc(C.Structure):
+    _fields_ = [("num_types", C.c_int), ("num_components", C.c_int), ("n", C.c_int),
+                ("factor", C.c_double), ("cutoff_sqr", C.c_double), ("smooth", _dp), ("fast", _dp)]
+
+
+class ReceptorDesc(C.Structure):
+    _fields_ = [("num_atoms", C.c_int), ("coords", _dp), ("type", _ip), ("charge", _dp)]
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [("num_atoms", C.c_int), ("num_movable", C.c_int), ("num_frames", C.c_int),
+                ("num_ligands", C.c_int), ("num_flex", C.c_int), ("conf_size", C.c_int), ("dof", C.c_int),
+                ("num_pairs", C.c_int), ("num_other_pairs", C.c_int),
+                ("lig_pair_end", _ip), ("ligand_atom_begin", _ip), ("ligand_atom_end", _ip), ("ligand_root", _ip),
+                ("atom_type", _ip), ("atom_charge", _dp), ("atom_local", _dp), ("atom_lab", _dp),
+                ("frame_kind", _ip), ("frame_parent", _ip), ("frame_begin", _ip), ("frame_end", _ip),
+                ("frame_conf", _ip), ("frame_dof", _ip), ("frame_origin", _dp), ("frame_axis", _dp),
+                ("frame_init_origin", _dp), ("pairs", _ip)]
+
+
+class MCParams(C.Structure):
+    _fields_ = [("num_steps", C.c_uint), ("temperature", C.c_double), ("mutation_amplitude", C.c_double),
+                ("min_rmsd", C.c_double), ("num_saved_mins", C.c_int), ("hunt_cap", C.c_double * 3),
+                ("authentic_v", C.c_double * 3), ("maxiters", C.c_int), ("accurate_line", C.c_int),
+                ("early_term", C.c_int), ("cache_slope", C.c_double)]
+
+
+class ChainInput(C.Structure):
+    _fields_ = [("model", C.c_int), ("num_steps", C.c_uint), ("conf", _dp), ("mt", _up)]
+
+
+class ChainResult(C.Structure):
+    _fields_ = [("count", C.c_int), ("e", _dp), ("conf", _dp), ("coords", _dp), ("evals", C.c_uint64)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libsmina_b200.so; raises OSError if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"{path} missing: run __graft_entry__.build() first")
+        _lib = C.CDLL(path)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    vp = C.c_void_p
+    L.sgh_last_error.restype = C.c_char_p
+    L.sg_last_error.restype = C.c_char_p
+    L.sg_last_error.argtypes = [vp]
+    for name, args in {
+        "sgh_model_from_pdbqt": [C.c_char_p, C.POINTER(vp)],
+        "sgh_model_desc": [vp, C.POINTER(ModelDesc)],
+        "sgh_model_heavy": [vp], "sgh_model_torsdof": [vp],
+        "sgh_make_receptor": [C.c_int, C.c_uint64, C.c_double * 3, C.c_double, C.POINTER(vp)],
+        "sgh_receptor_desc": [vp, C.POINTER(ReceptorDesc)],
+        "sgh_receptor_pdbqt": [vp, C.c_char_p, C.c_int],
+        "sgh_make_ligand_pdbqt": [C.c_int, C.c_int, C.c_uint64, C.c_double * 3, C.c_char_p, C.c_int],
+        "sgh_tables_create": [C.c_char_p, C.c_char_p, C.c_double, C.POINTER(vp)],
+        "sgh_tables_desc": [vp, C.POINTER(TablesDesc)],
+        "sgh_make_box": [C.c_double * 3, C.c_double * 3, C.c_double, C.POINTER(GridDims)],
+        "sgh_search_params": [vp, C.c_int, C.POINTER(MCParams)],
+        "sgh_seed_chains": [vp, C.c_int, C.c_int, C.POINTER(GridDims), _dp, _up],
+        "sg_create": [C.c_int, C.c_int, C.POINTER(vp)],
+        "sg_set_tables": [vp, C.POINTER(TablesDesc)],
+        "sg_set_receptor": [vp, C.c_int, C.POINTER(ReceptorDesc), C.POINTER(GridDims)],
+        "sg_build_grids": [vp, C.c_int, _ip, C.c_int],
+        "sg_get_grid": [vp, C.c_int, C.c_int, _dp, _dp],
+        "sg_drop_receptor": [vp, C.c_int],
+        "sg_eval": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, _dp, _dp, _dp],
+        "sg_eval_direct": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, _dp, _dp],
+        "sg_dock": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(ChainInput), C.c_int,
+                    C.POINTER(MCParams), C.POINTER(ChainResult)],
+        "sg_refine": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _ip, C.c_int, _dp, C.c_double * 3,
+                      C.c_int, C.c_int, C.c_int, _dp, _dp],
+        "sg_bfgs": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, C.c_int, C.c_int,
+                    C.c_int, _dp],
+    }.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.sg_destroy.argtypes = [vp]
+    L.sg_destroy.restype = None
+    for name in ("sgh_model_free", "sgh_receptor_free", "sgh_tables_free"):
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = None
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def uptr(a):
+    return a.ctypes.data_as(_up) if a is not None else None
+
+
+def vec3(x):
+    return (C.c_double * 3)(*[float(v) for v in x])
+
+
+class SminaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _check_host(rc):
+    if rc != 0:
+        raise SminaError(rc, load().sgh_last_error().decode())
+
+
+# ---- host-side objects -------------------------------------------------------------
+class Model:
+    """A docking model (ligand torsion tree, pairs) read from PDBQT text."""
+
+    def __init__(self, pdbqt: str):
+        L = load()
+        h = C.c_void_p()
+        _check_host(L.sgh_model_from_pdbqt(pdbqt.encode(), C.byref(h)))
+        self._h = h
+        self.pdbqt = pdbqt
+        self.desc = ModelDesc()
+        L.sgh_model_desc(h, C.byref(self.desc))
+        self.heavy = L.sgh_model_heavy(h)
+        self.torsdof = L.sgh_model_torsdof(h)
+
+    @property
+    def conf_size(self):
+        return self.desc.conf_size
+
+    @property
+    def dof(self):
+        return self.desc.dof
+
+    @property
+    def num_movable(self):
+        return self.desc.num_movable
+
+    def types(self):
+        return [self.desc.atom_type[i] for i in range(self.desc.num_movable)]
+
+    def search_params(self, num_modes=9) -> MCParams:
+        p = MCParams()
+        load().sgh_search_params(self._h, num_modes, C.byref(p))
+        return p
+
+    def seed_chains(self, seed: int, tasks: int, box: GridDims):
+        confs = np.zeros((tasks, self.conf_size))
+        mt = np.zeros((tasks, 625), dtype=np.uint32)
+        _check_host(load().sgh_seed_chains(self._h, seed, tasks, C.byref(box), dptr(confs), uptr(mt)))
+        return confs, mt
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sgh_model_free(self._h)
+            self._h = None
+
+
+class Receptor:
+    def __init__(self, heavy_atoms: int, seed: int, center=(0.0, 0.0, 0.0), cavity_radius=8.0):
+        L = load()
+        h = C.c_void_p()
+        _check_host(L.sgh_make_receptor(heavy_atoms, seed, vec3(center), cavity_radius, C.byref(h)))
+        self._h = h
+        self.desc = ReceptorDesc()
+        L.sgh_receptor_desc(h, C.byref(self.desc))
+        n = self.desc.num_atoms
+        self.coords = np.ctypeslib.as_array(self.desc.coords, shape=(n, 3)).copy()
+        self.types = np.ctypeslib.as_array(self.desc.type, shape=(n,)).copy()
+
+    def pdbqt(self) -> str:
+        L = load()
+        need = L.sgh_receptor_pdbqt(self._h, None, 0)
+        buf = C.create_string_buffer(need)
+        L.sgh_receptor_pdbqt(self._h, buf, need)
+        return buf.value.decode()
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sgh_receptor_free(self._h)
+            self._h = None
+
+
+def make_ligand_pdbqt(heavy: int, rotors: int, seed: int, center=(0.0, 0.0, 0.0)) -> str:
+    L = load()
+    need = L.sgh_make_ligand_pdbqt(heavy, rotors, seed, vec3(center), None, 0)
+    if need < 0:
+        raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
+    buf = C.create_string_buffer(need)
+    L.sgh_make_ligand_pdbqt(heavy, rotors, seed, vec3(center), buf, need)
+    return buf.value.decode()
+
+
+class Tables:
+    """precalculate_linear tables for a builtin or custom scoring function."""
+
+    def __init__(self, builtin: str = "vina", custom_text: str | None = None, factor: float = 32.0):
+        L = load()
+        h = C.c_void_p()
+        _check_host(L.sgh_tables_create(builtin.encode(), (custom_text or "").encode(), factor, C.byref(h)))
+        self._h = h
+        self.desc = TablesDesc()
+        L.sgh_tables_desc(h, C.byref(self.desc))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sgh_tables_free(self._h)
+            self._h = None
+
+
+def make_box(center, size, granularity=0.375) -> GridDims:
+    gd = GridDims()
+    load().sgh_make_box(vec3(center), vec3(size), granularity, C.byref(gd))
+    return gd
+
+
+def grid_points(gd: GridDims) -> int:
+    return (gd.n[0] + 1) * (gd.n[1] + 1) * (gd.n[2] + 1)
+
+
+@dataclass
+class ChainBatch:
+    """Owns the arrays behind an array of sg_chain_input / sg_chain_result."""
+    inputs: object
+    results: object
+    keep: list = field(default_factory=list)
+    e: np.ndarray = None
+    conf: np.ndarray = None
+    coords: np.ndarray = None
+    count: np.ndarray = None
+
+
+def make_chain_batch(models, model_of_chain, confs, mts, steps, num_saved, heavy_of_model):
+    n = len(model_of_chain)
+    ins = (ChainInput * n)()
+    outs = (ChainResult * n)()
+    keep = []
+    max_conf = max(m.conf_size for m in models)
+    max_heavy = max(heavy_of_model)
+    e = np.zeros((n, num_saved))
+    conf = np.zeros((n, num_saved, max_conf))
+    coords = np.zeros((n, num_saved, max_heavy, 3))
+    for k in range(n):
+        c = np.ascontiguousarray(confs[k], dtype=np.float64)
+        m = np.ascontiguousarray(mts[k], dtype=np.uint32)
+        keep += [c, m]
+        ins[k].model = int(model_of_chain[k])
+        ins[k].num_steps = int(steps[k] if hasattr(steps, "__len__") else steps)
+        ins[k].conf = dptr(c)
+        ins[k].mt = uptr(m)
+        outs[k].e = e[k].ctypes.data_as(_dp)
+        outs[k].conf = conf[k].ctypes.data_as(_dp)
+        outs[k].coords = coords[k].ctypes.data_as(_dp)
+    return ChainBatch(ins, outs, keep, e, conf, coords)
+
+
+# ---- engine ---------------------------------------------------------------------------
+class Engine:
+    """One device engine (sg_create).  precision: PREC_FP64 / PREC_FP32 / PREC_FP32_H16."""
+
+    def __init__(self, device: int = 0, precision: int = PREC_FP64):
+        L = load()
+        h = C.c_void_p()
+        rc = L.sg_create(device, precision, C.byref(h))
+        if rc != 0:
+            raise SminaError(rc, f"sg_create failed on device {device}")
+        self._h = h
+        self.precision = precision
+
+    def _check(self, rc):
+        if rc != 0:
+            raise SminaError(rc, load().sg_last_error(self._h).decode())
+
+    def set_tables(self, t: Tables):
+        self._check(load().sg_set_tables(self._h, C.byref(t.desc)))
+
+    def set_receptor(self, rid: int, r: Receptor, gd: GridDims):
+        self._check(load().sg_set_receptor(self._h, rid, C.byref(r.desc), C.byref(gd)))
+
+    def build_grids(self, rid: int, types):
+        t = np.ascontiguousarray(sorted(set(int(x) for x in types)), dtype=np.int32)
+        self._check(load().sg_build_grids(self._h, rid, iptr(t), len(t)))
+
+    def grid(self, rid: int, typ: int, gd: GridDims, charged=False):
+        n = grid_points(gd)
+        d = np.zeros(n)
+        c = np.zeros(n) if charged else None
+        self._check(load().sg_get_grid(self._h, rid, typ, dptr(d), dptr(c)))
+        return d, c
+
+    def eval(self, rid, m: Model, confs, v=(10, 10, 10), slope=1e6, coords=False):
+        confs = np.ascontiguousarray(confs, dtype=np.float64).reshape(-1, m.conf_size)
+        n = len(confs)
+        e = np.zeros(n)
+        g = np.zeros((n, m.dof))
+        xyz = np.zeros((n, m.num_movable, 3)) if coords else None
+        self._check(load().sg_eval(self._h, rid, C.byref(m.desc), n, dptr(confs), vec3(v), slope, dptr(e), dptr(g),
+                                   dptr(xyz)))
+        return (e, g, xyz) if coords else (e, g)
+
+    def eval_direct(self, rid, m: Model, confs, v=(1000, 1000, 1000), slope=10.0):
+        confs = np.ascontiguousarray(confs, dtype=np.float64).reshape(-1, m.conf_size)
+        n = len(confs)
+        e = np.zeros(n)
+        g = np.zeros((n, m.dof))
+        self._check(load().sg_eval_direct(self._h, rid, C.byref(m.desc), n, dptr(confs), vec3(v), slope, dptr(e),
+                                          dptr(g)))
+        return e, g
+
+    def bfgs(self, rid, m: Model, confs, v=(10, 10, 10), slope=1e6, maxiters=10, accurate=0, early=0):
+        confs = np.ascontiguousarray(confs, dtype=np.float64).reshape(-1, m.conf_size).copy()
+        e = np.zeros(len(confs))
+        self._check(load().sg_bfgs(self._h, rid, C.byref(m.desc), len(confs), dptr(confs), vec3(v), slope, maxiters,
+                                   accurate, early, dptr(e)))
+        return confs, e
+
+    def dock(self, rid, models, model_of_chain, confs, mts, params: MCParams, steps=None):
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        heavy = [m.heavy for m in models]
+        batch = make_chain_batch(models, model_of_chain, confs, mts,
+                                 params.num_steps if steps is None else steps, params.num_saved_mins, heavy)
+        self._check(load().sg_dock(self._h, rid, descs, len(models), batch.inputs, len(model_of_chain),
+                                   C.byref(params), batch.results))
+        batch.count = np.array([batch.results[k].count for k in range(len(model_of_chain))])
+        batch.evals = np.array([batch.results[k].evals for k in range(len(model_of_chain))], dtype=np.uint64)
+        return batch
+
+    def refine(self, rid, models, pose_model, confs, cap=(1000, 1000, 1000), maxiters=10, accurate_line=0,
+               early_term=0):
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        pm = np.ascontiguousarray(pose_model, dtype=np.int32)
+        confs = np.ascontiguousarray(confs, dtype=np.float64).copy()
+        n = len(pm)
+        e = np.zeros(n)
+        H = max(m.heavy for m in models)
+        xyz = np.zeros((n, H, 3))
+        self._check(load().sg_refine(self._h, rid, descs, len(models), iptr(pm), n, dptr(confs), vec3(cap), maxiters,
+                                     accurate_line, early_term, dptr(e), dptr(xyz)))
+        return confs, e, xyz
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().sg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,235 @@
+/*
+ * smina_b200.h - C ABI of the B200 docking engine.
+ *
+ * The engine runs smina's docking search (Monte Carlo chains, each doing
+ * BFGS local optimisation of a ligand conformation scored against receptor
+ * grid maps and an intramolecular pair table) on one B200.  Everything that
+ * crosses this boundary is plain data: pointers, sizes and int status codes.
+ * No exception, C++ type or torch type crosses it.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   sg_create / sg_destroy       gpusmina::GpuDocking ctor/dtor          src/gpu/gpu_docking.h:51-114
+ *                                (Engine<T> per device                   src/gpu/gpu_docking.cpp:237-264)
+ *   sg_set_tables                Engine::ensure_tables / flatten_tables src/gpu/gpu_flatten.cpp:239-332
+ *   sg_set_receptor              ensure_receptor / DeviceGrids::build   src/gpu/gpu_device.cu:199-250
+ *                                (cache::populate                       src/lib/cache.cpp:116-206)
+ *   sg_build_grids               build_grids_kernel                     src/gpu/gpu_device.cu:133-186
+ *   sg_eval                      eval_confs (model::eval_deriv)          src/gpu/gpu_kernels.h:22-126,
+ *                                                                        src/lib/model.cpp:969-985
+ *   sg_dock                      run_monte_carlo (monte_carlo::operator()) src/gpu/gpu_kernels_impl.cuh:659-885,
+ *                                                                        src/lib/monte_carlo.cpp:95-130
+ *   sg_refine                    run_refine (refine_structure)          src/gpu/gpu_kernels_impl.cuh:999-1098,
+ *                                                                        src/main/main.cpp:165-190
+ *   sg_dock_batch32              GpuDocking::dock_batch (batched screen) src/gpu/gpu_docking.cpp:756-831
+ *   sg_serve_*                   (no counterpart: continuous-batching request loop)
+ *   sg_last_error                the std::runtime_error text the reference throws
+ *
+ * Conventions
+ *   - All energies, coordinates, confs and changes are double on the ABI.
+ *   - A conf is laid out per ligand as position(3), orientation quaternion
+ *     (4: a, b, c, d = R_component_1..4), torsions; then the torsions of
+ *     each flexible residue.  A change (gradient) is laid out per ligand as
+ *     position(3), orientation(3), torsions; then flex torsions
+ *     (conf.h: change::operator()(index)).
+ *   - Atom order, frame order and pair order are smina's model order (see
+ *     sg_model_desc).
+ */
+#ifndef SMINA_B200_H
+#define SMINA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define SG_OK            0
+#define SG_ERR_ARG       1  /* bad argument / unsupported input            */
+#define SG_ERR_CUDA      2  /* CUDA runtime error                          */
+#define SG_ERR_NOMEM     3  /* device allocation failed / admission refused*/
+#define SG_ERR_OVERLAP   4  /* ligand atom exactly overlaps receptor atom  */
+#define SG_ERR_TIMEOUT   5  /* bounded device wait gave up / cancelled     */
+#define SG_ERR_STATE     6  /* call out of order (e.g. no tables set)      */
+
+/* ---- precision modes -------------------------------------------------- */
+#define SG_PREC_FP64      0  /* plain path: bit-exact with the CPU restatement */
+#define SG_PREC_FP32      1  /* FP32 eval/tree, FP64 BFGS update + Armijo test */
+#define SG_PREC_FP32_H16  2  /* as FP32, grid maps stored as FP16             */
+
+#define SG_NUM_TYPES 27       /* smina_atom_type::NumTypes */
+
+/* frame kinds of the torsion tree (tree.h) */
+#define SG_FRAME_RIGID          0  /* rigid_body: ligand root            */
+#define SG_FRAME_SEGMENT        1  /* segment: branch below a parent     */
+#define SG_FRAME_FIRST_SEGMENT  2  /* first_segment: flex residue root   */
+
+/* grid_dims: n[i] intervals, n[i]+1 sample points per axis */
+typedef struct sg_grid_dims {
+    double begin[3];
+    double end[3];
+    int n[3];
+} sg_grid_dims;
+
+/* precalculate_linear tables (precalculate.h:187-308).  Type pair index
+ * for types i <= j is i + j*(j+1)/2 (triangular_matrix_index). */
+typedef struct sg_tables_desc {
+    int num_types;        /* SG_NUM_TYPES                                   */
+    int num_components;   /* 1, or 4 with charge-dependent terms            */
+    int n;                /* samples per type pair: int(factor*cutoff_sqr)+3 */
+    double factor;        /* samples per A^2 (default 32)                   */
+    double cutoff_sqr;    /* scoring cutoff squared (64)                    */
+    const double* smooth; /* [npairs][n][nc][2]: (e, dor)                    */
+    const double* fast;   /* [npairs][n][nc]: midpoint energies (grid build) */
+} sg_tables_desc;
+
+/* rigid receptor atoms (model::grid_atoms); hydrogens and untyped atoms
+ * are allowed and skipped exactly as smina skips them */
+typedef struct sg_receptor_desc {
+    int num_atoms;
+    const double* coords; /* [num_atoms][3] */
+    const int* type;      /* smina type, SG_NUM_TYPES = unassigned */
+    const double* charge;
+} sg_receptor_desc;
+
+/* The movable part of one smina `model`: its ligands and flexible
+ * residues, flattened in model order.
+ *   atoms:  [0, num_movable) move (ligand atoms, then flex side chains);
+ *           [num_movable, num_atoms) are "inflex" atoms with fixed lab
+ *           coordinates.
+ *   frames: every tree node in depth-first pre-order, ligands first, then
+ *           flexible residues; a frame's atoms are [begin, end).
+ *   pairs:  other_pairs first (ligand-flex, flex-flex, flex-inflex ...,
+ *           curled with v[2]), then each ligand's internal pairs in
+ *           ligand order (curled with v[0]); lig_pair_end[l] is the end of
+ *           ligand l's pairs. */
+typedef struct sg_model_desc {
+    int num_atoms;
+    int num_movable;
+    int num_frames;
+    int num_ligands;
+    int num_flex;
+    int conf_size;
+    int dof;
+    int num_pairs;
+    int num_other_pairs;
+    const int*    lig_pair_end;      /* [num_ligands]                        */
+    const int*    ligand_atom_begin; /* [num_ligands] ligand atom range      */
+    const int*    ligand_atom_end;   /* [num_ligands]                        */
+    const int*    ligand_root;       /* [num_ligands] root frame index       */
+    const int*    atom_type;         /* [num_atoms]                          */
+    const double* atom_charge;       /* [num_atoms]                          */
+    const double* atom_local;        /* [num_atoms][3] frame-local coords (movable);
+                                        lab coords (inflex)                  */
+    const double* atom_lab;          /* [num_atoms][3] the model's coords as
+                                        read (model::coords before any set)  */
+    const int*    frame_kind;        /* [num_frames] SG_FRAME_*              */
+    const int*    frame_parent;      /* [num_frames] -1 for roots            */
+    const int*    frame_begin;       /* [num_frames]                         */
+    const int*    frame_end;         /* [num_frames]                         */
+    const int*    frame_conf;        /* rigid: position offset in conf; else torsion offset */
+    const int*    frame_dof;         /* rigid: position offset in change; else torsion offset */
+    const double* frame_origin;      /* [num_frames][3] rigid: initial origin;
+                                        segment: origin relative to parent;
+                                        first_segment: lab origin           */
+    const double* frame_axis;        /* [num_frames][3] segment: relative axis;
+                                        first_segment: lab axis             */
+    const double* frame_init_origin; /* [num_frames][3] lab origin as read   */
+    const int*    pairs;             /* [num_pairs][2] atom indices a < b     */
+} sg_model_desc;
+
+/* monte_carlo + minimization_params (monte_carlo.h:29-37, main.cpp:513-529) */
+typedef struct sg_mc_params {
+    unsigned num_steps;
+    double temperature;         /* 1.2                                    */
+    double mutation_amplitude;  /* 2                                      */
+    double min_rmsd;            /* 1.0 during the search                  */
+    int num_saved_mins;         /* max(20, num_modes)                     */
+    double hunt_cap[3];         /* (10, 10, 10)                           */
+    double authentic_v[3];      /* (1000, 1000, 1000)                     */
+    int maxiters;               /* BFGS iterations: (25 + N_movable) / 3  */
+    int accurate_line;          /* 1: accurate_line_search                */
+    int early_term;             /* minimization_params::early_term        */
+    double cache_slope;         /* grid out-of-box slope (1e6)            */
+} sg_mc_params;
+
+/* One chain of the plain (FP64) path: its starting conf and the
+ * mt19937 state after randomisation (624 words + index). */
+typedef struct sg_chain_input {
+    int model;          /* index into the models array                   */
+    unsigned num_steps;
+    const double* conf; /* [conf_size]                                   */
+    const uint32_t* mt; /* [625]: state words then index (0..624)        */
+} sg_chain_input;
+
+/* Result container of one chain (output_container, sorted ascending). */
+typedef struct sg_chain_result {
+    int count;          /* entries written, <= num_saved_mins            */
+    double* e;          /* [num_saved_mins]                              */
+    double* conf;       /* [num_saved_mins][conf_size]                   */
+    double* coords;     /* [num_saved_mins][num_heavy_movable][3]        */
+    uint64_t evals;     /* eval_deriv calls this chain made              */
+} sg_chain_result;
+
+typedef struct sg_engine sg_engine;
+
+/* ---- engine ----------------------------------------------------------- */
+int  sg_create(int device, int precision, sg_engine** out);
+void sg_destroy(sg_engine* e);
+const char* sg_last_error(const sg_engine* e);
+int  sg_precision(const sg_engine* e);
+
+/* Pair tables (copied to the device). */
+int sg_set_tables(sg_engine* e, const sg_tables_desc* t);
+
+/* Receptor + box.  Keeps the receptor resident under `receptor_id`
+ * (0..SG_MAX_RECEPTORS-1) and builds grid maps on demand. */
+#define SG_MAX_RECEPTORS 16
+int sg_set_receptor(sg_engine* e, int receptor_id, const sg_receptor_desc* r,
+                    const sg_grid_dims* gd);
+/* Build the maps of the listed ligand atom types (cache::populate). */
+int sg_build_grids(sg_engine* e, int receptor_id, const int* types, int ntypes);
+/* Copy one built map back: data [(n0+1)(n1+1)(n2+1)] (x fastest) and, with
+ * charge-dependent terms, chargedata (NULL otherwise). */
+int sg_get_grid(sg_engine* e, int receptor_id, int type, double* data, double* chargedata);
+/* Drop a receptor and its maps. */
+int sg_drop_receptor(sg_engine* e, int receptor_id);
+
+/* model::eval_deriv for nconfs confs of one model against receptor maps
+ * (cache) of `receptor_id`.  out_e [nconfs], out_g [nconfs][dof],
+ * out_coords [nconfs][num_movable][3] (may be NULL). */
+int sg_eval(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs,
+            const double* confs, const double v[3], double slope,
+            double* out_e, double* out_g, double* out_coords);
+
+/* Direct receptor evaluation (non_cache::eval_deriv) with box penalty
+ * slope; returns SG_ERR_OVERLAP like smina's exception. */
+int sg_eval_direct(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs,
+                   const double* confs, const double v[3], double slope,
+                   double* out_e, double* out_g);
+
+/* monte_carlo::operator() for every chain, all chains in one launch. */
+int sg_dock(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+            const sg_chain_input* chains, int nchains, const sg_mc_params* p,
+            sg_chain_result* out);
+
+/* quasi_newton (BFGS, bfgs.h:202-282) of each conf against the maps;
+ * confs [n][conf_size] updated in place, out_e [n]. */
+int sg_bfgs(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs, double* confs,
+            const double v[3], double slope, int maxiters, int accurate_line, int early_term,
+            double* out_e);
+
+/* refine_structure for each pose: BFGS on the direct receptor sum with box
+ * slope 10, 100, ... (<= 5 tries) until every movable heavy atom is inside
+ * the box.  confs [n][max conf_size over models] in/out, out_e [n] (max
+ * double if it never got inside), out_coords [n][max heavy atoms][3]
+ * (may be NULL). */
+int sg_refine(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+              const int* pose_model, int nposes, double* confs, const double cap[3],
+              int maxiters, int accurate_line, int early_term,
+              double* out_e, double* out_coords);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMINA_B200_H */

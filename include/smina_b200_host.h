@@ -1,0 +1,67 @@
+/*
+ * smina_b200_host.h - C ABI of the host library that prepares inputs for the
+ * engine (include/smina_b200.h): PDBQT ligand models, receptors, pair tables,
+ * boxes, search parameters and chain seeds.
+ *
+ * Reference functions restated (paths inside the reference project):
+ *   sgh_model_from_pdbqt   parse_ligand_stream_pdbqt + model::initialize
+ *                          src/lib/parse_pdbqt.cpp:209-353,487-495,
+ *                          src/lib/model.cpp:448-636
+ *   sgh_tables_create      precalculate_linear(weighted_terms, factor)
+ *                          src/lib/precalculate.h:187-308, src/main/main.cpp:1408-1421;
+ *                          builtin / custom scoring src/lib/builtinscoring.cpp:63-105,
+ *                          src/lib/custom_terms.cpp:56-71
+ *   sgh_make_box           grid_dims from center/size src/main/main.cpp:801-809
+ *   sgh_search_params      setup_search src/main/main.cpp:513-529
+ *   sgh_seed_chains        parallel_mc task seeding src/lib/parallel_mc.cpp:80-98 and
+ *                          conf::randomize src/lib/conf.h:355-360
+ *   sgh_make_receptor /    synthetic inputs (no counterpart: the reference reads
+ *   sgh_make_ligand_pdbqt  files through OpenBabel)
+ */
+#ifndef SMINA_B200_HOST_H
+#define SMINA_B200_HOST_H
+
+#include <stdint.h>
+#include "smina_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sgh_model sgh_model;
+typedef struct sgh_receptor sgh_receptor;
+typedef struct sgh_tables sgh_tables;
+
+const char* sgh_last_error(void);
+
+int  sgh_model_from_pdbqt(const char* text, sgh_model** out);
+void sgh_model_free(sgh_model* m);
+/* descriptor pointing into the model (valid while the model lives) */
+int  sgh_model_desc(const sgh_model* m, sg_model_desc* out);
+int  sgh_model_heavy(const sgh_model* m);
+int  sgh_model_torsdof(const sgh_model* m);
+
+int  sgh_make_receptor(int heavy_atoms, uint64_t seed, const double center[3], double cavity_radius,
+                       sgh_receptor** out);
+void sgh_receptor_free(sgh_receptor* r);
+int  sgh_receptor_desc(sgh_receptor* r, sg_receptor_desc* out);
+/* returns 0, or the buffer size needed */
+int  sgh_receptor_pdbqt(const sgh_receptor* r, char* buf, int buflen);
+/* returns 0, -1 on error, or the buffer size needed */
+int  sgh_make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3], char* buf, int buflen);
+
+/* builtin_name: "vina"/"default", "vinardo", "dkoes_scoring", "dkoes_fast",
+ * "ad4_scoring"; custom_text (if non-empty) takes precedence */
+int  sgh_tables_create(const char* builtin_name, const char* custom_text, double factor, sgh_tables** out);
+void sgh_tables_free(sgh_tables* t);
+int  sgh_tables_desc(const sgh_tables* t, sg_tables_desc* out);
+
+int  sgh_make_box(const double center[3], const double size[3], double granularity, sg_grid_dims* out);
+int  sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out);
+/* confs [tasks][conf_size], mt [tasks][625] */
+int  sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims* box, double* confs, uint32_t* mt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
