@@ -218,6 +218,9 @@ std::string receptor_pdbqt(const Receptor& rec) {
 // ---- ligand ------------------------------------------------------------------------
 std::string make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3]) {
     if (heavy < 1) throw std::runtime_error("a ligand needs at least one heavy atom");
+    // an acyclic tree of h heavy atoms has at most h - 3 bonds between two
+    // non-terminal atoms
+    rotors = std::max(0, std::min(rotors, heavy - 3));
     const P3 c{center[0], center[1], center[2]};
     for (int attempt = 0; attempt < 2000; attempt++) {
         Rng r(seed * 1000003ull + attempt);
@@ -233,8 +236,11 @@ std::string make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double
             double u = r.uni();
             int e = u < 0.70 ? 0 : u < 0.82 ? 1 : u < 0.95 ? 2 : u < 0.97 ? 3 : u < 0.98 ? 4 : u < 0.995 ? 5 : 6;
             bool placed = false;
+            // grow chains (attach to the newest atom) more often when many
+            // rotatable bonds are wanted
+            const double linear = std::min(0.9, (double)rotors / std::max(1, heavy - 3) + attempt * 0.002);
             for (int t = 0; t < 60 && !placed; t++) {
-                int p = r.below((int)pos.size());
+                int p = (t < 20 && r.uni() < linear) ? (int)pos.size() - 1 : r.below((int)pos.size());
                 if ((int)nb[p].size() >= valence[el[p]] - (el[p] == 0 ? 0 : 0)) continue;
                 if (el[p] >= 4) continue;
                 double bl = el[p] == 0 && e == 0 ? 1.54 : cov[el[p]] + cov[e];
