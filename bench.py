@@ -1,0 +1,329 @@
+"""Throughput of the batched mixed-precision docking search on B200.
+
+Workload: the 1,000-ligand synthetic virtual screen -- one receptor of
+3,000 heavy atoms (seeded random-walk chains, 8 A cavity), 22 A box at
+0.375 A, ligands with heavy atoms uniform in [10, 50] and rotatable bonds
+uniform in [0, 12], exhaustiveness 8, smina's own step and BFGS-iteration
+counts per ligand, default (vina) scoring, FP32 evaluation with FP64 BFGS
+update/acceptance.  One step = one persistent search launch over a batch of
+ligands (default: the whole screen) followed by the FP64 refinement of the
+merged poses.  Metric: ligands docked per second.
+
+  value          ligands / device time of the step's launches (receptor
+                 maps resident, CUDA events on the engine's stream)
+  e2e            the same through the C-ABI call with host buffers
+                 (model upload, result download, host merge included)
+  roofline       algorithmic gather bytes of the search kernel (32 B per
+                 packed grid cell, 16 B per in-cutoff pair table entry)
+                 over its event-timed duration, against measured HBM
+                 copy bandwidth
+  cpu_baseline   the CPU restatement of smina's search (FP64, one thread
+                 per chain) on a bounded sample of the screen's ligands
+
+Multi-GPU: replicas only (every rank docks its own copy of the screen with
+its own random streams; no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-smina_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import smina_b200 as sb  # noqa: E402
+
+METRIC = "ligands docked/sec on 1 B200 (batched FP32 vs plain FP64); p50/p99 latency"
+UNIT = "ligands/s"
+CENTER = (0.5, 0.25, -0.3)
+G_BYTES = {sb.PREC_FP32: 32, sb.PREC_FP32_H16: 16}  # one packed grid cell
+T_BYTES = 16  # one (e_i, dor_i, e_i+1, dor_i+1) table entry, nc = 1
+
+
+def screen(n, seed):
+    """The synthetic screen: (heavy, rotors, ligand seed) per ligand."""
+    rng = np.random.default_rng(seed)
+    heavy = rng.integers(10, 51, size=n)
+    rotors = rng.integers(0, 13, size=n)
+    return [(int(h), int(r), 10_000 + k) for k, (h, r) in enumerate(zip(heavy, rotors))]
+
+
+def build_models(spec):
+    return [sb.Model(sb.make_ligand_pdbqt(h, r, s, CENTER)) for h, r, s in spec]
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r.split(",") for r in self.out.strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[4 + i] and "Not" not in r[4 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_params(models):
+    p = models[0].search_params(9)
+    p.num_steps = 0
+    return p
+
+
+def jobs_for(models, idx, exh, seed, key_base):
+    jobs = []
+    for j, k in enumerate(idx):
+        sp = models[k].search_params(9)
+        jobs.append(sb.LigandJob(model=k, num_chains=exh, num_steps=sp.num_steps, maxiters=sp.maxiters,
+                                 seed=seed, ligand_key=key_base + k))
+    return jobs
+
+
+def cpu_sample(models, gd, receptor, tables, exh, seed, nlig, threads, parallel=1):
+    """CPU restatement of the same search (oracle: FP64, one thread per chain)
+    over ``nlig`` ligands spread evenly over the screen; ligands/s."""
+    from oracle_lib import Oracle, merge
+    orc = Oracle(tables, receptor, gd, full_cells=True)
+    idx = [int(i) for i in np.linspace(0, len(models) - 1, nlig)]
+    orc.ensure([models[k] for k in idx])
+
+    def one(k):
+        m = models[k]
+        p = m.search_params(9)
+        confs, mts = m.seed_chains(seed + k, exh, gd)
+        b = orc.dock([m], np.zeros(exh, np.int32), confs, mts, p, threads=threads)
+        e, conf, _ = merge(b, m, 2.0, p.num_saved_mins)
+        orc.refine([m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v), maxiters=p.maxiters,
+                   accurate=p.accurate_line, early=p.early_term)
+
+    t0 = time.perf_counter()
+    for base in range(0, len(idx), parallel):
+        ts = [threading.Thread(target=one, args=(k,)) for k in idx[base:base + parallel]]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+    dt = time.perf_counter() - t0
+    return len(idx) / dt, dt, idx
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=1800))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of smina's search on all host
+    cores, on the same workload, each step a bounded sample of ligands."""
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    parallel = max(1, cores // args.exhaustiveness)
+    spec = screen(args.ligands, args.seed)
+    models = build_models(spec)
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    times = []
+    for s in range(args.warmup + args.steps):
+        sub = [models[(s * parallel + i) % len(models)] for i in range(parallel)]
+        v, dt, _ = cpu_sample(sub, gd, R, T, args.exhaustiveness, args.seed, len(sub), args.exhaustiveness, parallel)
+        if s >= args.warmup:
+            times.append((len(sub), dt))
+    n = sum(a for a, _ in times)
+    t = sum(b for _, b in times)
+    value = n / t
+    sample = (f"{n} ligands of the screen ({parallel} at a time, {args.exhaustiveness} chains each at smina's full "
+              f"step count, merge + refine)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), receptor "
+                               "3000 heavy atoms, 22 A box, exhaustiveness 8", "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": parallel * args.exhaustiveness, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ligands", type=int, default=1000, help="ligands in the screen")
+    ap.add_argument("--batch", type=int, default=0, help="ligands per step (0: the whole screen)")
+    ap.add_argument("--exhaustiveness", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
+    ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--chains-per-block", type=int, default=0)
+    args = ap.parse_args()
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    prec = sb.PREC_FP32 if args.precision == "fp32" else sb.PREC_FP32_H16
+    spec = screen(args.ligands, args.seed)
+    models = build_models(spec)
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    eng = sb.Engine(local, prec)
+    eng.set_tables(T)
+    eng.set_receptor(0, R, gd)
+    eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
+    if args.chains_per_block:
+        eng.set_chains_per_block(args.chains_per_block)
+    p = make_params(models)
+    B = args.batch or args.ligands
+    nb = max(1, args.ligands // B)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
+    key_base = 1_000_000 * rank
+
+    def step(s):
+        idx = list(range((s % nb) * B, (s % nb) * B + B))
+        jobs = jobs_for(models, idx, args.exhaustiveness, args.seed, key_base)
+        sub = [models[k] for k in idx]
+        for j, jb in enumerate(jobs):
+            jb.model = j
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = eng.dock_batch(0, sub, jobs, p, refine=True)
+        wall = time.perf_counter() - t0
+        st = eng.batch_stats()
+        return len(idx), wall, st, res
+
+    for s in range(args.warmup):
+        step(s)
+    barrier(pg)
+    torch.cuda.synchronize()
+    recs = []
+    with Clocks(local) as clk:
+        for s in range(args.steps):
+            recs.append(step(args.warmup + s))
+    torch.cuda.synchronize()
+    barrier(pg)
+    n_lig = sum(r[0] for r in recs)
+    dev_s = sum((r[2]["mc_ms"] + r[2]["refine_ms"]) / 1000 for r in recs)
+    mc_s = sum(r[2]["mc_ms"] / 1000 for r in recs)
+    wall_s = sum(r[1] for r in recs)
+    dev_max = reduce_max(pg, dev_s)
+    wall_max = reduce_max(pg, wall_s)
+    value = n_lig * world / dev_max
+    e2e = n_lig * world / wall_max
+    gbytes = sum(r[2]["grid_lookups"] * G_BYTES[prec] + r[2]["pair_lookups"] * T_BYTES for r in recs)
+    achieved = gbytes / mc_s / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak, peak_src = (peaks["hbm_gbs"], "measured") if "hbm_gbs" in peaks else (6650.0, "fallback")
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "k_mc32_traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get("bytes_per_launch")
+    evals = sum(r[2]["evals"] for r in recs)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = args.exhaustiveness
+        v, dt, idx = cpu_sample(models, gd, R, T, args.exhaustiveness, args.seed, args.cpu_ligands, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(idx)} ligands spread over the screen (indices {idx}), {args.exhaustiveness} chains "
+                         f"each at smina's full step count, one thread per chain, merge + refine; {dt:.1f} s"}
+    if rank == 0:
+        clocks = clk.summary()
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dev_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), "
+                                   f"receptor 3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness "
+                                   f"{args.exhaustiveness}, smina step counts, {B} ligands per step",
+                       "precision": args.precision, "ligands_per_step": B, "global_batch": B * world,
+                       "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)",
+                       "chains_per_block": recs[-1][2]["chains_per_block"], "blocks": recs[-1][2]["blocks"]},
+            "e2e": {"value": e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": int(sum(r[2]["h2d_bytes"] for r in recs) / len(recs)),
+                    "d2h_bytes_per_step": int(sum(r[2]["d2h_bytes"] for r in recs) / len(recs))},
+            "gpu_launches": 2 * args.steps,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "kernel": "k_mc32"},
+            "cpu_baseline": cpu,
+            "evals_per_s": evals / mc_s,
+            "search_ms_per_step": 1000 * mc_s / args.steps,
+        }), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

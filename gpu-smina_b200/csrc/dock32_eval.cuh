@@ -1,0 +1,498 @@
+// Mixed-precision path, part 1: one warp evaluates model::eval_deriv in FP32.
+//
+// Energy, gradient and torsion-tree math run in FP32; the conf (position,
+// orientation quaternion, torsions) stays in FP64 and is narrowed when the
+// tree is set.  Grid maps are read in the packed-corner layout (one 32 B or
+// 16 B load per atom); a pair interpolation is one float4 table load.
+// Reference semantics: model.cpp:837-841,904-928,969-985; grid.cpp:111-236;
+// tree.h:108-243; precalculate.h:111-151.
+#pragma once
+#include "sg_dev.cuh"
+
+namespace sg {
+
+constexpr unsigned kFull32 = 0xffffffffu;
+
+// Section timers (compile with -DSG_PROFILE): lane 0 of every warp adds
+// clock64() spans per section; sg_profile_read() copies them out.
+// Sections: 0 set_conf, 1 grid, 2 pairs, 3 derivative, 4 line-search
+// bookkeeping, 5 BFGS algebra, 7 whole chain.
+#ifdef SG_PROFILE
+__device__ unsigned long long g_prof[16];
+#define SG_T0(name) const long long name = clock64()
+#define SG_T1(name, k) \
+    if ((threadIdx.x & 31) == 0) atomicAdd(&g_prof[k], (unsigned long long)(clock64() - name))
+#else
+#define SG_T0(name)
+#define SG_T1(name, k)
+#endif
+
+// per-warp workspace (bytes, 16 B aligned)
+struct Ws32 {
+    int model;                                                   // DModel copy
+    int coords, force, origin, axis, quat, rot;                  // float4 arrays (rot: 3 rows per frame)
+    int x_tmp, x_cand, x_new, x_orig, g, g_new, g_orig, p, y, mhy, h;  // double arrays (h: n x n)
+    int pf, pc;                                                  // prefix sums over atoms (float4)
+    int scratch;                                                 // 64 floats
+    int total;
+};
+SG_HD Ws32 ws32_layout(int natoms, int nframes, int conf, int dof) {
+    Ws32 w;
+    int o = 0;
+    auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
+    w.model = take((int)sizeof(DModel));
+    w.coords = take(16 * natoms);
+    w.force = take(16 * natoms);
+    w.origin = take(16 * nframes);
+    w.axis = take(16 * nframes);
+    w.quat = take(16 * nframes);
+    w.rot = take(48 * nframes);
+    w.x_tmp = take(8 * conf);
+    w.x_cand = take(8 * conf);
+    w.x_new = take(8 * conf);
+    w.x_orig = take(8 * conf);
+    w.g = take(8 * dof);
+    w.g_new = take(8 * dof);
+    w.g_orig = take(8 * dof);
+    w.p = take(8 * dof);
+    w.y = take(8 * dof);
+    w.mhy = take(8 * dof);
+    w.h = take(8 * dof * dof);
+    w.pf = take(16 * (natoms + 1));
+    w.pc = take(16 * (natoms + 1));
+    w.scratch = take(4 * 64);
+    w.total = o;
+    return w;
+}
+
+// ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw 2011) -------------------------------
+struct Philox {
+    uint32_t k0, k1;  // key: request seed
+    uint32_t c2, c3;  // counter words fixed per chain: (ligand, chain)
+    uint32_t n;       // draw index
+};
+__device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+// uniform double in [0, 1) with 53 random bits; every lane computes the same value
+__device__ __forceinline__ double ph_u01(Philox& r) {
+    const uint4 o = philox10(make_uint4(r.n++, 0u, r.c2, r.c3), r.k0, r.k1);
+    const uint64_t v = ((uint64_t)(o.x >> 5) << 26) | (o.y >> 6);
+    return (double)v * (1.0 / 9007199254740992.0);
+}
+__device__ __forceinline__ double ph_range(Philox& r, double a, double b) { return a + (b - a) * ph_u01(r); }
+__device__ __forceinline__ int ph_int(Philox& r, int n) {  // [0, n)
+    const int k = (int)(ph_u01(r) * n);
+    return k < n ? k : n - 1;
+}
+__device__ __forceinline__ double ph_normal(Philox& r) {  // Box-Muller
+    const double u1 = 1.0 - ph_u01(r), u2 = ph_u01(r);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+struct W32 {
+    char* s;  // this warp's workspace
+    Ws32 L;
+    const DModel* m;  // staged copy in shared memory
+    const DTables32* T;
+    const DMaps32* G;
+    int lane;
+    unsigned long long evals;
+    unsigned long long grid_hits, pair_hits;  // per-lane gather counts (algorithmic bytes)
+    __device__ float4* coords() const { return (float4*)(s + L.coords); }
+    __device__ float4* force() const { return (float4*)(s + L.force); }
+    __device__ float4* origin() const { return (float4*)(s + L.origin); }
+    __device__ float4* axis() const { return (float4*)(s + L.axis); }
+    __device__ float4* quat() const { return (float4*)(s + L.quat); }
+    __device__ float4* rot() const { return (float4*)(s + L.rot); }
+    __device__ double* d(int off) const { return (double*)(s + off); }
+    __device__ float* scratch() const { return (float*)(s + L.scratch); }
+    // stage the chain's model descriptor in this warp's shared memory
+    __device__ void bind_model(const DModel* gm) {
+        const int4* src = (const int4*)gm;
+        int4* dst = (int4*)(s + L.model);
+        for (int i = lane; i < (int)(sizeof(DModel) / 16); i += 32) dst[i] = src[i];
+        __syncwarp();
+        m = (const DModel*)(s + L.model);
+    }
+};
+static_assert(sizeof(DModel) % 16 == 0, "DModel is copied in 16 byte pieces");
+
+// fire-and-forget add into this warp's shared workspace (shared state
+// space: no generic-address round trip, no return value)
+__device__ __forceinline__ void red_shared(float* p, float v) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
+__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 rot_apply(const float4* R, float3 v) {  // rows R[0..2]
+    return make_float3(R[0].x * v.x + R[0].y * v.y + R[0].z * v.z, R[1].x * v.x + R[1].y * v.y + R[1].z * v.z,
+                       R[2].x * v.x + R[2].y * v.y + R[2].z * v.z);
+}
+__device__ __forceinline__ void quat_rows(float4 q, float4* R) {
+    const float a = q.x, b = q.y, c = q.z, d = q.w;
+    const float aa = a * a, ab = a * b, ac = a * c, ad = a * d, bb = b * b, bc = b * c, bd = b * d, cc = c * c,
+                cd = c * d, dd = d * d;
+    R[0] = make_float4(aa + bb - cc - dd, 2 * (-ad + bc), 2 * (ac + bd), 0);
+    R[1] = make_float4(2 * (ad + bc), aa - bb + cc - dd, 2 * (-ab + cd), 0);
+    R[2] = make_float4(2 * (-ac + bd), 2 * (ab + cd), aa - bb - cc + dd, 0);
+}
+__device__ __forceinline__ float4 qmul32(float4 l, float4 r) {
+    return make_float4(l.x * r.x - l.y * r.y - l.z * r.z - l.w * r.w, l.x * r.y + l.y * r.x + l.z * r.w - l.w * r.z,
+                       l.x * r.z - l.y * r.w + l.z * r.x + l.w * r.y, l.x * r.w + l.y * r.z - l.z * r.y + l.w * r.x);
+}
+// rotate v by unit quaternion q = (w; x, y, z)
+__device__ __forceinline__ float3 qrot(float4 q, float3 v) {
+    const float3 u = make_float3(q.y, q.z, q.w);
+    const float3 t = 2.0f * cross3(u, v);
+    return v + q.x * t + cross3(u, t);
+}
+__device__ __forceinline__ float4 axis_angle32(float3 ax, float angle) {
+    // bring the angle into [-pi, pi] (normalize_angle) before halving it
+    const float twopi = 6.28318530717958647692f;
+    angle -= twopi * rintf(angle * (1.0f / twopi));
+    float s, c;
+    __sincosf(0.5f * angle, &s, &c);
+    return make_float4(c, s * ax.x, s * ax.y, s * ax.z);
+}
+__device__ __forceinline__ float4 q_norm_approx32(float4 q) {
+    const float s = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    if (fabsf(s - 1.f) < 1e-6f) return q;
+    const float inv = rsqrtf(s);
+    return make_float4(q.x * inv, q.y * inv, q.z * inv, q.w * inv);
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull32, v, o);
+    return v;
+}
+
+
+// model::set in FP32.  Each frame's transform relative to its parent is a
+// rotation about its parent-frame axis plus its parent-frame origin offset:
+// turning about the lab axis R_p a equals R_p turning about a, so
+// q_f = q_p r(a_f, theta_f) and o_f = o_p + R_p t_f.  These local transforms
+// need no parent data; the lab transforms are their ordered compositions
+// along the path to the root, done by pointer jumping in log2(depth) warp
+// shuffles.  Trees of more than 32 frames go level by level.
+__device__ __noinline__ void set_conf32(W32& w, const double* conf) {
+    const DModel& m = *w.m;
+    float4* O = w.origin();
+    float4* A = w.axis();
+    float4* Q = w.quat();
+    float4* R = w.rot();
+    if (m.nframes <= 32) {
+        const int f = w.lane;
+        const bool act = f < m.nframes;
+        float4 q = make_float4(1, 0, 0, 0);
+        float3 t = make_float3(0, 0, 0);
+        int anc = -1, parent = -1, kind = 0;
+        if (act) {
+            kind = __ldg(m.fkind + f);
+            const int ci = __ldg(m.fconf + f);
+            if (kind == SG_FRAME_RIGID) {
+                const double* c = conf + ci;
+                t = make_float3((float)c[0], (float)c[1], (float)c[2]);
+                q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
+            } else {
+                if (kind == SG_FRAME_SEGMENT) parent = anc = __ldg(m.fparent + f);
+                t = f3(__ldg(m.forigin32 + f));
+                q = axis_angle32(f3(__ldg(m.faxis32 + f)), (float)conf[ci]);
+            }
+        }
+        for (int it = 0; it < 6 && __any_sync(kFull32, anc >= 0); it++) {
+            const int src = anc >= 0 ? anc : f;
+            const float qa0 = __shfl_sync(kFull32, q.x, src), qa1 = __shfl_sync(kFull32, q.y, src),
+                        qa2 = __shfl_sync(kFull32, q.z, src), qa3 = __shfl_sync(kFull32, q.w, src);
+            const float ta0 = __shfl_sync(kFull32, t.x, src), ta1 = __shfl_sync(kFull32, t.y, src),
+                        ta2 = __shfl_sync(kFull32, t.z, src);
+            const int aa = __shfl_sync(kFull32, anc, src);
+            if (anc >= 0) {
+                const float4 qa = make_float4(qa0, qa1, qa2, qa3);
+                t = make_float3(ta0, ta1, ta2) + qrot(qa, t);
+                q = qmul32(qa, q);
+                anc = aa;
+            }
+        }
+        q = q_norm_approx32(q);
+        // lab axis of a segment: its relative axis turned by the parent's orientation
+        const int ps = parent >= 0 ? parent : f;
+        const float4 pq = make_float4(__shfl_sync(kFull32, q.x, ps), __shfl_sync(kFull32, q.y, ps),
+                                      __shfl_sync(kFull32, q.z, ps), __shfl_sync(kFull32, q.w, ps));
+        if (act) {
+            O[f] = make_float4(t.x, t.y, t.z, 0);
+            Q[f] = q;
+            quat_rows(q, R + 3 * f);
+            if (kind == SG_FRAME_SEGMENT) {
+                const float3 ax = qrot(pq, f3(__ldg(m.faxis32 + f)));
+                A[f] = make_float4(ax.x, ax.y, ax.z, 0);
+            } else if (kind == SG_FRAME_FIRST_SEGMENT) {
+                A[f] = __ldg(m.faxis32 + f);
+            }
+        }
+        __syncwarp();
+    } else {
+        for (int lv = 0; lv < m.nlevels; lv++) {
+            for (int idx = m.level_start[lv] + w.lane; idx < m.level_start[lv + 1]; idx += 32) {
+                const int f = __ldg(m.level_frames + idx);
+                const int kind = __ldg(m.fkind + f);
+                float4 q;
+                if (kind == SG_FRAME_RIGID) {
+                    const double* c = conf + __ldg(m.fconf + f);
+                    O[f] = make_float4((float)c[0], (float)c[1], (float)c[2], 0);
+                    q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
+                } else if (kind == SG_FRAME_SEGMENT) {
+                    const int p = __ldg(m.fparent + f);
+                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(__ldg(m.forigin32 + f)));
+                    const float3 ax = rot_apply(R + 3 * p, f3(__ldg(m.faxis32 + f)));
+                    O[f] = make_float4(o.x, o.y, o.z, 0);
+                    A[f] = make_float4(ax.x, ax.y, ax.z, 0);
+                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[__ldg(m.fconf + f)]), Q[p]));
+                } else {
+                    const float3 ax = f3(__ldg(m.faxis32 + f));
+                    O[f] = __ldg(m.forigin32 + f);
+                    A[f] = make_float4(ax.x, ax.y, ax.z, 0);
+                    q = axis_angle32(ax, (float)conf[__ldg(m.fconf + f)]);
+                }
+                Q[f] = q;
+                quat_rows(q, R + 3 * f);
+            }
+            __syncwarp();
+        }
+    }
+    float4* X = w.coords();
+    for (int i = w.lane; i < m.nmov; i += 32) {
+        const int f = __ldg(m.atom_frame + i);
+        const float3 c = f3(O[f]) + rot_apply(R + 3 * f, f3(__ldg(m.local32 + i)));
+        X[i] = make_float4(c.x, c.y, c.z, 0);
+    }
+    __syncwarp();
+}
+
+// grid::evaluate_aux on the packed-corner map
+__device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge_map, float3 loc, float slope, float v,
+                                            float3& deriv) {
+    float s[3] = {(loc.x - G.init[0]) * G.factor[0], (loc.y - G.init[1]) * G.factor[1], (loc.z - G.init[2]) * G.factor[2]};
+    float miss[3] = {0, 0, 0};
+    int region[3], a[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (s[i] < 0) { miss[i] = -s[i]; region[i] = -1; a[i] = 0; s[i] = 0; }
+        else if (s[i] >= G.dim_fl_minus_1[i]) { miss[i] = s[i] - G.dim_fl_minus_1[i]; region[i] = 1; a[i] = G.cdim[i] - 1; s[i] = 1; }
+        else { region[i] = 0; a[i] = min((int)s[i], G.cdim[i] - 1); s[i] -= (float)a[i]; }
+    }
+    const float penalty = slope * (miss[0] * G.factor_inv[0] + miss[1] * G.factor_inv[1] + miss[2] * G.factor_inv[2]);
+    const size_t cell = (size_t)a[0] + (size_t)G.cdim[0] * ((size_t)a[1] + (size_t)G.cdim[1] * a[2]);
+    float4 lo, hi;
+    if (!charge_map && G.half) {
+        const uint4 u = __ldg(G.m16[t] + cell);
+        const float2 p0 = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+        const float2 p1 = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+        const float2 p2 = __half22float2(*reinterpret_cast<const __half2*>(&u.z));
+        const float2 p3 = __half22float2(*reinterpret_cast<const __half2*>(&u.w));
+        lo = make_float4(p0.x, p0.y, p1.x, p1.y);
+        hi = make_float4(p2.x, p2.y, p3.x, p3.y);
+    } else {
+        const float4* b = (charge_map ? G.c32[t] : G.m32[t]) + 2 * cell;
+        lo = __ldg(b);
+        hi = __ldg(b + 1);
+    }
+    const float x = s[0], y = s[1], z = s[2], mx = 1 - x, my = 1 - y, mz = 1 - z;
+    // lo = (f000 f100 f010 f110), hi = (f001 f101 f011 f111)
+    const float e00 = lo.x * mx + lo.y * x, e10 = lo.z * mx + lo.w * x;
+    const float e01 = hi.x * mx + hi.y * x, e11 = hi.z * mx + hi.w * x;
+    const float ez0 = e00 * my + e10 * y, ez1 = e01 * my + e11 * y;
+    float f = ez0 * mz + ez1 * z;
+    const float dx0 = (lo.y - lo.x) * my + (lo.w - lo.z) * y, dx1 = (hi.y - hi.x) * my + (hi.w - hi.z) * y;
+    float3 grad = make_float3(dx0 * mz + dx1 * z, (e10 - e00) * mz + (e11 - e01) * z, ez1 - ez0);
+    if (f > 0) {  // soft curl
+        const float tt = (v < 1.1920929e-07f) ? 0.f : (v / (v + f));
+        f *= tt;
+        grad = (tt * tt) * grad;
+    }
+    deriv.x = G.factor[0] * (region[0] == 0 ? grad.x : 0.f) + slope * region[0];
+    deriv.y = G.factor[1] * (region[1] == 0 ? grad.y : 0.f) + slope * region[1];
+    deriv.z = G.factor[2] * (region[2] == 0 ? grad.z : 0.f) + slope * region[2];
+    return f + penalty;
+}
+
+// table lookup with charge-weighted components (precalculate_linear element eval_deriv)
+__device__ __forceinline__ void table32_nc(const DTables32& T, int tp, float qa, float qb, float r2, float& e, float& dor) {
+    const int p = tp & 0x1fffffff;
+    if (tp & (1 << 30)) { const float t = qa; qa = qb; qb = t; }
+    const float rf = T.factor * r2;
+    const int i1 = (int)rf;
+    const float rem = rf - (float)i1;
+    const float4* b = T.tab + ((size_t)p * T.n + i1) * T.nc;
+    const float4 c0 = __ldg(b), c1 = __ldg(b + 1), c2 = __ldg(b + 2), c3 = __ldg(b + 3);
+    const float aa = fabsf(qa), bb = fabsf(qb), ab = qa * qb;
+    const float e1 = c0.x + aa * c1.x + bb * c2.x + ab * c3.x, e2 = c0.z + aa * c1.z + bb * c2.z + ab * c3.z;
+    const float d1 = c0.y + aa * c1.y + bb * c2.y + ab * c3.y, d2 = c0.w + aa * c1.w + bb * c2.w + ab * c3.w;
+    e = e1 + rem * (e2 - e1);
+    dor = d1 + rem * (d2 - d1);
+}
+
+// model::eval_deriv in FP32; returns the energy (same on every lane), writes g (FP64)
+__device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const float v[3], float slope, double* g) {
+    const DModel& m = *w.m;
+    SG_T0(t_set);
+    set_conf32(w, conf);
+    SG_T1(t_set, 0);
+    SG_T0(t_grid);
+    float4* X = w.coords();
+    float4* Fz = w.force();
+    float e = 0;
+    // grid part; every movable atom gets its force reset (hydrogens: zero)
+    for (int i = w.lane; i < m.nmov; i += 32) {
+        const int t = __ldg(m.type + i);
+        float3 d = make_float3(0, 0, 0);
+        if (t < kNumTypes && !is_h(t)) {
+            const float3 loc = f3(X[i]);
+            e += grid_aux32(*w.G, t, false, loc, slope, v[1], d);
+            w.grid_hits++;
+            const float q = __ldg(m.local32 + i).w;
+            if (q != 0.f && w.G->c32[t]) {
+                float3 cd;
+                e += q * grid_aux32(*w.G, t, true, loc, slope, v[1], cd);
+                d = d + q * cd;
+                w.grid_hits++;
+            }
+        }
+        Fz[i] = make_float4(d.x, d.y, d.z, 0);
+    }
+    __syncwarp();
+    SG_T1(t_grid, 1);
+    SG_T0(t_pairs);
+    // pairs: intramolecular (v[0]) and other (v[2]); two pairs per lane in flight
+    const int P = m.npairs;
+    const float cut2 = w.T->cutoff_sqr;
+    for (int base = 0; base < P; base += 64) {
+        int2 ab[2];
+        int tp[2];
+        float3 r[2];
+        float r2[2];
+        bool ok[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int k = base + 32 * u + w.lane;
+            ok[u] = k < P;
+            ab[u] = ok[u] ? __ldg(m.pairs32 + k) : make_int2(0, 0);
+            tp[u] = ok[u] ? __ldg(m.tp32 + k) : 0;
+            r[u] = f3(X[ab[u].y]) - f3(X[ab[u].x]);
+            r2[u] = dot3(r[u], r[u]);
+            ok[u] = ok[u] && r2[u] < cut2;
+        }
+        float4 tv[2];
+        float rem[2];
+        if (w.T->nc == 1) {  // issue both table loads before using either
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const float rf = w.T->factor * r2[u];
+                const int i1 = ok[u] ? (int)rf : 0;
+                rem[u] = rf - (float)i1;
+                tv[u] = ok[u] ? __ldg(w.T->tab + ((size_t)(tp[u] & 0x1fffffff) * w.T->n + i1)) : make_float4(0, 0, 0, 0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            if (!ok[u]) continue;
+            float pe, dor;
+            if (w.T->nc == 1) {
+                pe = tv[u].x + rem[u] * (tv[u].z - tv[u].x);
+                dor = tv[u].y + rem[u] * (tv[u].w - tv[u].y);
+            } else {
+                table32_nc(*w.T, tp[u], __ldg(m.local32 + ab[u].x).w, __ldg(m.local32 + ab[u].y).w, r2[u], pe, dor);
+            }
+            float3 f = dor * r[u];
+            const float vv = (tp[u] & (1 << 29)) ? v[0] : v[2];
+            if (pe > 0) {
+                const float tt = (vv < 1.1920929e-07f) ? 0.f : (vv / (vv + pe));
+                pe *= tt;
+                f = (tt * tt) * f;
+            }
+            e += pe;
+            w.pair_hits++;
+            red_shared(&Fz[ab[u].x].x, -f.x); red_shared(&Fz[ab[u].x].y, -f.y); red_shared(&Fz[ab[u].x].z, -f.z);
+            red_shared(&Fz[ab[u].y].x, f.x); red_shared(&Fz[ab[u].y].y, f.y); red_shared(&Fz[ab[u].y].z, f.z);
+        }
+    }
+    e = warp_sum(e);
+    __syncwarp();
+    SG_T1(t_pairs, 2);
+    SG_T0(t_der);
+    // Derivative.  A frame's subtree owns the contiguous atom range
+    // [fbegin, fsub_end), so its force and torque are differences of two
+    // prefix sums over atoms: F_sub = PF[E] - PF[b], and with
+    // c_i = (x_i - o_ref) x F_i, T_sub = PC[E] - PC[b] - (o_f - o_ref) x F_sub.
+    // Torques are taken about the first root's origin to keep them small.
+    float4* O = w.origin();
+    float4* PF = (float4*)(w.s + w.L.pf);
+    float4* PC = (float4*)(w.s + w.L.pc);
+    const float3 oref = f3(O[0]);
+    float3 cf = make_float3(0, 0, 0), cc = make_float3(0, 0, 0);
+    for (int base = 0; base < m.nmov; base += 32) {
+        const int i = base + w.lane;
+        float3 F = make_float3(0, 0, 0), Cq = make_float3(0, 0, 0);
+        if (i < m.nmov) {
+            F = f3(Fz[i]);
+            Cq = cross3(f3(X[i]) - oref, F);
+        }
+        float3 iF = F, iC = Cq;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const float a0 = __shfl_up_sync(kFull32, iF.x, off), a1 = __shfl_up_sync(kFull32, iF.y, off),
+                        a2 = __shfl_up_sync(kFull32, iF.z, off), b0 = __shfl_up_sync(kFull32, iC.x, off),
+                        b1 = __shfl_up_sync(kFull32, iC.y, off), b2 = __shfl_up_sync(kFull32, iC.z, off);
+            if (w.lane >= off) {
+                iF = iF + make_float3(a0, a1, a2);
+                iC = iC + make_float3(b0, b1, b2);
+            }
+        }
+        if (i < m.nmov) {  // exclusive prefix at i
+            const float3 eF = cf + (iF - F), eC = cc + (iC - Cq);
+            PF[i] = make_float4(eF.x, eF.y, eF.z, 0);
+            PC[i] = make_float4(eC.x, eC.y, eC.z, 0);
+        }
+        cf = cf + make_float3(__shfl_sync(kFull32, iF.x, 31), __shfl_sync(kFull32, iF.y, 31), __shfl_sync(kFull32, iF.z, 31));
+        cc = cc + make_float3(__shfl_sync(kFull32, iC.x, 31), __shfl_sync(kFull32, iC.y, 31), __shfl_sync(kFull32, iC.z, 31));
+    }
+    if (w.lane == 0) {
+        PF[m.nmov] = make_float4(cf.x, cf.y, cf.z, 0);
+        PC[m.nmov] = make_float4(cc.x, cc.y, cc.z, 0);
+    }
+    __syncwarp();
+    for (int f = w.lane; f < m.nframes; f += 32) {
+        const int b = __ldg(m.fbegin + f), E = __ldg(m.fsub_end + f);
+        const float3 F = f3(PF[E]) - f3(PF[b]);
+        const float3 T = (f3(PC[E]) - f3(PC[b])) - cross3(f3(O[f]) - oref, F);
+        const int dof0 = __ldg(m.fdof + f);
+        if (__ldg(m.fkind + f) == SG_FRAME_RIGID) {
+            g[dof0] = F.x; g[dof0 + 1] = F.y; g[dof0 + 2] = F.z;
+            g[dof0 + 3] = T.x; g[dof0 + 4] = T.y; g[dof0 + 5] = T.z;
+        } else {
+            g[dof0] = dot3(T, f3(w.axis()[f]));
+        }
+    }
+    __syncwarp();
+    SG_T1(t_der, 3);
+    w.evals++;
+    return e;
+}
+
+}  // namespace sg

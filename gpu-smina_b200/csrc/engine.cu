@@ -12,21 +12,7 @@
 
 namespace sg {
 
-// ---- launchers defined in the kernel files ---------------------------------------------------
-cudaError_t launch_cell_lists(int, const double*, const int*, const DGeom&, double, const double*, const double*, int*,
-                              const int*, int*, int, cudaStream_t);
-cudaError_t launch_grid_map64(const DGeom&, int, const double*, const int*, const double*, const int*, const int*,
-                              const DTables&, const int*, int, double**, double**, cudaStream_t);
-cudaError_t launch_grid_narrow(const double*, float*, __half*, size_t, cudaStream_t);
-size_t ws64_bytes(const DModel& hm);
-cudaError_t launch_eval64(const DModel*, size_t, const DTables&, const DReceptor*, int, const double*, const double[3],
-                          double, int, double*, double*, double*, int*, cudaStream_t);
-cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor*, int, double*, const double[3], double,
-                          int, int, int, double*, int*, cudaStream_t);
-cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
-                        const MCParams64&, int*, cudaStream_t);
-cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
-                            const double[3], int, int, int, double*, double*, int, int*, cudaStream_t);
+
 
 void DevBuf::reset() {
     if (p) cudaFree(p);
@@ -76,29 +62,6 @@ using namespace sg;
 // ---- engine -----------------------------------------------------------------------------------
 sg_engine::~sg_engine() {
     if (stream) cudaStreamDestroy(stream);
-}
-
-template <typename F>
-static int guarded(sg_engine* e, F f) {
-    try {
-        if (!e) return SG_ERR_ARG;
-        cuda_check(cudaSetDevice(e->device), "cudaSetDevice");
-        f();
-        return SG_OK;
-    } catch (EngineError& x) {
-        e->err = x.what();
-        return x.code;
-    } catch (std::bad_alloc&) {
-        e->err = "host allocation failed";
-        return SG_ERR_NOMEM;
-    } catch (std::exception& x) {
-        e->err = x.what();
-        return SG_ERR_ARG;
-    }
-}
-
-static void require(bool ok, const std::string& msg) {
-    if (!ok) throw EngineError(SG_ERR_ARG, msg);
 }
 
 // Reads the device error word, clears it, and turns it into a status.
@@ -159,23 +122,27 @@ int sg_set_tables(sg_engine* e, const sg_tables_desc* t) {
         const size_t np = kNumTypePairs;
         e->tab_smooth.upload(t->smooth, np * t->n * t->num_components * 2 * sizeof(double), e->stream);
         e->tab_fast.upload(t->fast, np * t->n * t->num_components * sizeof(double), e->stream);
-        // FP32 (e, dor) pairs for the mixed-precision path (single component)
-        std::vector<float> s32;
-        if (t->num_components == 1) {
-            s32.resize(np * t->n * 2);
-            for (size_t i = 0; i < s32.size(); i++) s32[i] = (float)t->smooth[i];
-        } else {
-            s32.resize(np * t->n * 8);
-            for (size_t i = 0; i < s32.size(); i++) s32[i] = (float)t->smooth[i];
+        // (e_i, dor_i, e_i+1, dor_i+1) per component: one 16 B load per lookup
+        {
+            const int nc = t->num_components, n = t->n;
+            std::vector<float> t4(np * n * nc * 4, 0.f);
+            for (size_t pr = 0; pr < np; pr++)
+                for (int i = 0; i < n; i++)
+                    for (int c = 0; c < nc; c++) {
+                        const double* a = t->smooth + ((pr * n + i) * nc + c) * 2;
+                        float* o = &t4[((pr * n + i) * nc + c) * 4];
+                        o[0] = (float)a[0];
+                        o[1] = (float)a[1];
+                        if (i + 1 < n) { o[2] = (float)a[nc * 2]; o[3] = (float)a[nc * 2 + 1]; }
+                    }
+            e->tab32.upload(t4.data(), t4.size() * sizeof(float), e->stream);
         }
-        e->tab_smooth32.upload(s32.data(), s32.size() * sizeof(float), e->stream);
         e->tables.nc = t->num_components;
         e->tables.n = t->n;
         e->tables.factor = t->factor;
         e->tables.cutoff_sqr = t->cutoff_sqr;
         e->tables.smooth = (const double*)e->tab_smooth.p;
         e->tables.fast = (const double*)e->tab_fast.p;
-        e->tables.smooth32 = (const float2*)e->tab_smooth32.p;
         e->has_tables = true;
         for (auto& r : e->rec) r.clear_maps();  // maps depend on the tables
         cuda_check(cudaStreamSynchronize(e->stream), "tables");
@@ -207,9 +174,9 @@ void refresh_header(sg_engine* e, RecState& r) {
     for (int t = 0; t < kNumTypes; t++) {
         h.map[t] = r.map64[t].as<double>();
         h.cmap[t] = r.cmap64[t].as<double>();
-        h.map32[t] = r.map32[t].as<float>();
-        h.cmap32[t] = r.cmap32[t].as<float>();
-        h.map16[t] = r.map16[t].as<__half>();
+        h.map32[t] = r.map32[t].as<float4>();
+        h.cmap32[t] = r.cmap32[t].as<float4>();
+        h.map16[t] = r.map16[t].as<uint4>();
     }
     if (!r.dhdr.p) r.dhdr.alloc(sizeof(DReceptor));
     cuda_check(cudaMemcpyAsync(r.dhdr.p, &h, sizeof(DReceptor), cudaMemcpyHostToDevice, e->stream), "receptor header");
@@ -307,16 +274,17 @@ void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes) {
                                  dmaps.as<double*>(), dcmaps.as<double*>(), e->stream),
                "grid maps");
     if (e->precision != SG_PREC_FP64) {
+        const size_t ncells = (size_t)(r.geom.dim[0] - 1) * (r.geom.dim[1] - 1) * (r.geom.dim[2] - 1);
         for (int t : need) {
-            r.map32[t].alloc(npts * sizeof(float));
-            if (e->precision == SG_PREC_FP32_H16) r.map16[t].alloc(npts * sizeof(__half));
-            cuda_check(launch_grid_narrow(r.map64[t].as<double>(), r.map32[t].as<float>(), r.map16[t].as<__half>(), npts,
-                                          e->stream),
-                       "narrow maps");
+            r.map32[t].alloc(ncells * 2 * sizeof(float4));
+            if (e->precision == SG_PREC_FP32_H16) r.map16[t].alloc(ncells * sizeof(uint4));
+            cuda_check(launch_grid_pack(r.geom, r.map64[t].as<double>(), r.map32[t].as<float4>(), r.map16[t].as<uint4>(),
+                                        e->stream),
+                       "pack maps");
             if (charged) {
-                r.cmap32[t].alloc(npts * sizeof(float));
-                cuda_check(launch_grid_narrow(r.cmap64[t].as<double>(), r.cmap32[t].as<float>(), nullptr, npts, e->stream),
-                           "narrow charge maps");
+                r.cmap32[t].alloc(ncells * 2 * sizeof(float4));
+                cuda_check(launch_grid_pack(r.geom, r.cmap64[t].as<double>(), r.cmap32[t].as<float4>(), nullptr, e->stream),
+                           "pack charge maps");
             }
         }
     }
@@ -399,8 +367,8 @@ namespace sg {
 
 // Validates one model descriptor on the host so that no device index can
 // leave its array, then appends its packed arrays.
-static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<double>& D, std::vector<size_t>& ioff,
-                     std::vector<size_t>& doff, DModel& hm) {
+static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<double>& D, std::vector<float>& Fl,
+                     std::vector<size_t>& ioff, std::vector<size_t>& doff, std::vector<size_t>& foff, DModel& hm) {
     const int N = d.num_atoms, M = d.num_movable, F = d.num_frames, P = d.num_pairs;
     require(N > 0 && N <= 4096 && M > 0 && M <= N, "model: atom counts out of range");
     require(F > 0 && F <= 1024 && d.num_ligands >= 0 && d.num_flex >= 0 && d.num_ligands + d.num_flex > 0,
@@ -473,10 +441,13 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
     }
     child_start[F] = (int)child_list.size();
     // pairs, groups, per-atom ordered pair lists
-    std::vector<int> group(P, 0);
+    std::vector<int> group(P, 0), pair_tp(P, 0);
     for (int k = 0; k < P; k++) {
         const int a = d.pairs[2 * k], b = d.pairs[2 * k + 1];
         require(a >= 0 && a < N && b >= 0 && b < N && a != b, "model: pair atom out of range");
+        const int ta = d.atom_type[a], tb = d.atom_type[b];
+        require(ta < kNumTypes && tb < kNumTypes, "model: a pair atom has no type");
+        pair_tp[k] = (ta <= tb ? tri_index(ta, tb) : tri_index(tb, ta)) | (ta > tb ? (1 << 30) : 0);
         if (k >= d.num_other_pairs)
             for (int l = 0; l < d.num_ligands; l++)
                 if (k < d.lig_pair_end[l]) { group[k] = l + 1; break; }
@@ -532,6 +503,7 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
     pi(d.atom_type, N); pi(d.frame_kind, F); pi(d.frame_parent, F); pi(d.frame_begin, F); pi(d.frame_end, F);
     pi(d.frame_conf, F); pi(d.frame_dof, F);
     pv(atom_frame); pv(level_start); pv(level_frames); pv(child_start); pv(child_list);
+    if (I.size() & 1) I.push_back(0);  // pairs are read as int2
     if (P) pi(d.pairs, 2 * (size_t)P); else pv({});
     pv(group); pv(csr_start); pv(csr); pv(heavy);
     std::vector<int> lb(d.ligand_atom_begin, d.ligand_atom_begin + d.num_ligands),
@@ -539,6 +511,54 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
         lp(d.lig_pair_end, d.lig_pair_end + d.num_ligands);
     pv(lb); pv(le); pv(lr); pv(lp);
     pv(blk_rigid); pv(blk_conf); pv(blk_dof); pv(blk_ntors); pv(tor_conf); pv(tor_dof); pv(tor_frame);
+    pv(pair_tp);
+    {   // subtree atom ranges: a frame's descendants follow its own atoms
+        std::vector<int> sub_end(F);
+        for (int f = F - 1; f >= 0; f--) {
+            sub_end[f] = d.frame_end[f];
+            for (int c = f + 1; c < F; c++)
+                if (d.frame_parent[c] == f) sub_end[f] = std::max(sub_end[f], sub_end[c]);
+        }
+        for (int c = 0; c < F; c++)
+            for (int a = d.frame_parent[c]; a >= 0; a = d.frame_parent[a])
+                require(d.frame_begin[c] >= d.frame_end[a] && d.frame_end[c] <= sub_end[a],
+                        "model: a subtree's atoms must follow its root frame's atoms contiguously");
+        pv(sub_end);
+    }
+    {   // mixed-precision pair order: round robin over first-atom groups, curl group in bit 29
+        std::vector<std::vector<int>> groups;
+        std::vector<int> gid(N, -1);
+        for (int k = 0; k < P; k++) {
+            const int a = d.pairs[2 * k];
+            if (gid[a] < 0) { gid[a] = (int)groups.size(); groups.emplace_back(); }
+            groups[gid[a]].push_back(k);
+        }
+        std::vector<int> p32, t32;
+        size_t maxg = 0;
+        for (auto& g : groups) maxg = std::max(maxg, g.size());
+        for (size_t r = 0; r < maxg; r++)
+            for (auto& g : groups)
+                if (r < g.size()) {
+                    const int k = g[r];
+                    p32.push_back(d.pairs[2 * k]);
+                    p32.push_back(d.pairs[2 * k + 1]);
+                    t32.push_back(pair_tp[k] | (k >= d.num_other_pairs ? (1 << 29) : 0));
+                }
+        if (I.size() & 1) I.push_back(0);  // read as int2
+        pv(p32);
+        pv(t32);
+    }
+    auto pf4 = [&](const double* xyz, const double* w4, size_t n) {
+        foff.push_back(Fl.size());
+        for (size_t i = 0; i < n; i++) {
+            Fl.push_back((float)xyz[3 * i]); Fl.push_back((float)xyz[3 * i + 1]); Fl.push_back((float)xyz[3 * i + 2]);
+            Fl.push_back(w4 ? (float)w4[i] : 0.f);
+        }
+    };
+    foff.clear();
+    pf4(d.atom_local, d.atom_charge, N); pf4(d.atom_lab, nullptr, N);
+    pf4(d.frame_origin, nullptr, F); pf4(d.frame_axis, nullptr, F); pf4(d.frame_init_origin, nullptr, F);
+    hm.cost = M + P + 8 * F;
     pd(d.atom_charge, N); pd(d.atom_local, 3 * (size_t)N); pd(d.atom_lab, 3 * (size_t)N);
     pd(d.frame_origin, 3 * (size_t)F); pd(d.frame_axis, 3 * (size_t)F); pd(d.frame_init_origin, 3 * (size_t)F);
     hm.natoms = N; hm.nmov = M; hm.nframes = F; hm.nlig = d.num_ligands; hm.nflex = d.num_flex;
@@ -552,13 +572,16 @@ void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedM
     require(models && nmodels > 0 && nmodels <= (1 << 20), "models: bad array");
     std::vector<int> I;
     std::vector<double> D;
-    std::vector<std::vector<size_t>> ioffs(nmodels), doffs(nmodels);
+    std::vector<float> Fl;
+    std::vector<std::vector<size_t>> ioffs(nmodels), doffs(nmodels), foffs(nmodels);
     out.host.assign(nmodels, DModel{});
-    for (int k = 0; k < nmodels; k++) pack_one(models[k], I, D, ioffs[k], doffs[k], out.host[k]);
+    for (int k = 0; k < nmodels; k++) pack_one(models[k], I, D, Fl, ioffs[k], doffs[k], foffs[k], out.host[k]);
     out.ints.upload(I.data(), std::max<size_t>(1, I.size()) * sizeof(int), e->stream);
     out.dbls.upload(D.data(), std::max<size_t>(1, D.size()) * sizeof(double), e->stream);
+    out.flts.upload(Fl.data(), std::max<size_t>(4, Fl.size()) * sizeof(float), e->stream);
     const int* ib = out.ints.as<int>();
     const double* db = out.dbls.as<double>();
+    const float* fb = out.flts.as<float>();
     out.max_ws64 = 0;
     for (int k = 0; k < nmodels; k++) {
         DModel& h = out.host[k];
@@ -573,6 +596,14 @@ void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedM
         h.lig_begin = ib + io[j++]; h.lig_end = ib + io[j++]; h.lig_root = ib + io[j++]; h.lig_pair_end = ib + io[j++];
         h.blk_rigid = ib + io[j++]; h.blk_conf = ib + io[j++]; h.blk_dof = ib + io[j++]; h.blk_ntors = ib + io[j++];
         h.tor_conf = ib + io[j++]; h.tor_dof = ib + io[j++]; h.tor_frame = ib + io[j++];
+        h.pair_tp = ib + io[j++];
+        h.fsub_end = ib + io[j++];
+        h.pairs32 = (const int2*)(ib + io[j++]);
+        h.tp32 = ib + io[j++];
+        const std::vector<size_t>& fo = foffs[k];
+        h.local32 = (const float4*)(fb + fo[0]); h.lab32 = (const float4*)(fb + fo[1]);
+        h.forigin32 = (const float4*)(fb + fo[2]); h.faxis32 = (const float4*)(fb + fo[3]);
+        h.finit32 = (const float4*)(fb + fo[4]);
         int q = 0;
         h.charge = db + dd[q++]; h.local = db + dd[q++]; h.lab = db + dd[q++];
         h.forigin = db + dd[q++]; h.faxis = db + dd[q++]; h.finit = db + dd[q++];
@@ -635,6 +666,18 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
         de.make(nconfs, e->stream);
         dg.make((size_t)nconfs * h.dof, e->stream);
         if (out_coords) dx.make((size_t)nconfs * h.nmov * 3, e->stream);
+        if (!direct && e->precision != SG_PREC_FP64) {  // the mixed-precision evaluation
+            const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
+            require(ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
+            cuda_check(launch_eval32(pm.dmodels.as<DModel>(), ws, tables32(e), maps32(e, r), nconfs, dc.p(), v, slope,
+                                     de.p(), dg.p(), out_coords ? dx.p() : nullptr, e->stream),
+                       "eval launch");
+            de.fetch(out_e, e->stream);
+            dg.fetch(out_g, e->stream);
+            if (out_coords) dx.fetch(out_coords, e->stream);
+            e->check_device_errors();
+            return;
+        }
         cuda_check(launch_eval64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), nconfs, dc.p(), v,
                                  slope, direct, de.p(), dg.p(), out_coords ? dx.p() : nullptr, e->d_err.as<int>(), e->stream),
                    "eval launch");
@@ -795,7 +838,7 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
         dx.make((size_t)nposes * hs * 3, e->stream);
         dpm.make(nposes, e->stream, pose_model);
         cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(), nposes,
-                                   dc.p(), cs, cap, maxiters, accurate_line, early_term, de.p(), dx.p(), hs,
+                                   dc.p(), cs, cap, maxiters, nullptr, accurate_line, early_term, de.p(), dx.p(), hs,
                                    e->d_err.as<int>(), e->stream),
                    "refine launch");
         dc.fetch(confs, e->stream);

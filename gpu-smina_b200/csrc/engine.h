@@ -1,7 +1,9 @@
 // Engine state behind the C ABI.
 #pragma once
+#include <new>
 #include <stdexcept>
 #include <string>
+#include <cstdint>
 #include <vector>
 #include "sg_dev.cuh"
 
@@ -13,6 +15,10 @@ struct EngineError : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+
+inline void require(bool ok, const std::string& msg) {
+    if (!ok) throw EngineError(SG_ERR_ARG, msg);
+}
 
 // owning device allocation
 struct DevBuf {
@@ -58,7 +64,7 @@ struct RecState {
 // a batch of models packed for the device
 struct PackedModels {
     std::vector<DModel> host;  // host copies with device pointers
-    DevBuf ints, dbls, dmodels;
+    DevBuf ints, dbls, flts, dmodels;
     size_t max_ws64 = 0;
     int max_conf = 0, max_dof = 0, max_heavy = 0, max_atoms = 0, max_pairs = 0, max_frames = 0;
 };
@@ -73,7 +79,10 @@ struct sg_engine {
     cudaStream_t stream = nullptr;
     std::string err;
     bool has_tables = false;
-    sg::DevBuf tab_smooth, tab_fast, tab_smooth32;
+    sg::DevBuf tab_smooth, tab_fast, tab32;
+    int force_wpb = 0, last_wpb = 0, last_blocks = 0;
+    double last_mc_ms = 0, last_refine_ms = 0;
+    uint64_t last_evals = 0, last_grid_hits = 0, last_pair_hits = 0, last_h2d = 0, last_d2h = 0;
     sg::DTables tables{};
     sg::RecState rec[SG_MAX_RECEPTORS];
     sg::DevBuf d_err;
@@ -82,6 +91,53 @@ struct sg_engine {
 };
 
 namespace sg {
+
+// Runs f() on the engine's device and turns exceptions into status codes
+// (the message goes to sg_last_error).
+template <typename F>
+int guarded(sg_engine* e, F f) {
+    try {
+        if (!e) return SG_ERR_ARG;
+        cuda_check(cudaSetDevice(e->device), "cudaSetDevice");
+        f();
+        return SG_OK;
+    } catch (EngineError& x) {
+        e->err = x.what();
+        return x.code;
+    } catch (std::bad_alloc&) {
+        e->err = "host allocation failed";
+        return SG_ERR_NOMEM;
+    } catch (std::exception& x) {
+        e->err = x.what();
+        return SG_ERR_ARG;
+    }
+}
+
+// ---- launchers defined in the kernel files ---------------------------------------------------
+cudaError_t launch_cell_lists(int, const double*, const int*, const DGeom&, double, const double*, const double*, int*,
+                              const int*, int*, int, cudaStream_t);
+cudaError_t launch_grid_map64(const DGeom&, int, const double*, const int*, const double*, const int*, const int*,
+                              const DTables&, const int*, int, double**, double**, cudaStream_t);
+cudaError_t launch_grid_pack(const DGeom&, const double*, float4*, uint4*, cudaStream_t);
+size_t ws64_bytes(const DModel& hm);
+cudaError_t launch_eval64(const DModel*, size_t, const DTables&, const DReceptor*, int, const double*, const double[3],
+                          double, int, double*, double*, double*, int*, cudaStream_t);
+cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor*, int, double*, const double[3], double,
+                          int, int, int, double*, int*, cudaStream_t);
+cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
+                        const MCParams64&, int*, cudaStream_t);
+cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
+                            const double[3], int, const int*, int, int, double*, double*, int, int*, cudaStream_t);
+size_t ws32_bytes(const DModel& hm);
+int mc32_occupancy(int wpb, size_t ws_stride);
+cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const Chain32*, int, const MCParams32&, unsigned*,
+                        int blocks, int wpb, size_t ws_stride, cudaStream_t);
+cudaError_t launch_eval32(const DModel*, size_t, const DTables32&, const DMaps32&, int, const double*, const double[3],
+                          double, double*, double*, double*, cudaStream_t);
+
+// FP32 views of the engine's tables and of a receptor's packed maps
+DTables32 tables32(const sg_engine* e);
+DMaps32 maps32(const sg_engine* e, const RecState& r);
 void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedModels& out);
 RecState& receptor_for(sg_engine* e, int rid);
 void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes);

@@ -1,0 +1,357 @@
+// Batched mixed-precision docking behind the C ABI (sg_dock_batch32):
+// every ligand job's chains run in one persistent search launch (k_mc32),
+// the chains of a ligand are merged like merge_output_containers with
+// min_rmsd 2, and every merged pose is refined in FP64 on the direct
+// receptor sum (k_refine64).  Reference: gpu_docking.cpp:560-625
+// (GpuDocking::dock_batch), parallel_mc.cpp:64-98, main.cpp:165-200.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include "engine.h"
+
+namespace sg {
+
+DTables32 tables32(const sg_engine* e) {
+    DTables32 T{};
+    T.nc = e->tables.nc;
+    T.n = e->tables.n;
+    T.factor = (float)e->tables.factor;
+    T.cutoff_sqr = (float)e->tables.cutoff_sqr;
+    T.tab = e->tab32.as<float4>();
+    return T;
+}
+
+DMaps32 maps32(const sg_engine* e, const RecState& r) {
+    DMaps32 G{};
+    for (int i = 0; i < 3; i++) {
+        require(r.geom.dim[i] >= 2, "mixed-precision path: the box needs at least one grid cell per axis");
+        G.cdim[i] = r.geom.dim[i] - 1;
+        G.init[i] = (float)r.geom.init[i];
+        G.factor[i] = (float)r.geom.factor[i];
+        G.factor_inv[i] = (float)r.geom.factor_inv[i];
+        G.dim_fl_minus_1[i] = (float)r.geom.dim_fl_minus_1[i];
+    }
+    for (int t = 0; t < kNumTypes; t++) {
+        G.m32[t] = r.map32[t].as<float4>();
+        G.c32[t] = r.cmap32[t].as<float4>();
+        G.m16[t] = r.map16[t].as<uint4>();
+    }
+    G.half = e->precision == SG_PREC_FP32_H16;
+    return G;
+}
+
+// every grid type the models look up has its packed maps
+static void check_packed(const sg_engine* e, const RecState& r, const sg_model_desc* models, int nmodels) {
+    for (int k = 0; k < nmodels; k++)
+        for (int i = 0; i < models[k].num_movable; i++) {
+            const int t = models[k].atom_type[i];
+            if (t >= kNumTypes || is_h(t)) continue;
+            require(r.map32[t].p && (e->precision != SG_PREC_FP32_H16 || r.map16[t].p) &&
+                        (e->tables.nc == 1 || r.cmap32[t].p),
+                    "mixed-precision maps missing for a ligand type");
+        }
+}
+
+// add_to_output_container (coords.cpp:25-58) on the host, for the merge
+struct HostPose {
+    double e;
+    std::vector<double> conf, xyz;
+};
+static void add_pose(std::vector<HostPose>& out, HostPose&& t, double min_rmsd, int max_size) {
+    size_t ci = out.size();
+    double cr = DBL_MAX;
+    const size_t H3 = t.xyz.size();
+    for (size_t i = 0; i < out.size(); i++) {
+        double acc = 0;
+        for (size_t a = 0; a < H3; a++) {
+            const double d = t.xyz[a] - out[i].xyz[a];
+            acc += d * d;
+        }
+        const double r = H3 ? std::sqrt(acc / (double)(H3 / 3)) : 0.0;
+        if (i == 0 || r < cr) { ci = i; cr = r; }
+    }
+    if (ci < out.size() && cr < min_rmsd) {
+        if (t.e < out[ci].e) out[ci] = std::move(t);
+    } else if ((int)out.size() < max_size) {
+        out.push_back(std::move(t));
+    } else if (!out.empty() && t.e < out.back().e) {
+        out.back() = std::move(t);
+    }
+    std::stable_sort(out.begin(), out.end(), [](const HostPose& a, const HostPose& b) { return a.e < b.e; });
+}
+
+// launch shape: chains (warps) per block with the most resident chains per SM
+static void choose_launch(sg_engine* e, size_t ws_stride, int nchains, int& wpb, int& blocks) {
+    const int cands[3] = {4, 2, 1};
+    int best_w = 0, best_occ = 0, best_res = 0;
+    for (int c : cands) {
+        if (e->force_wpb && c != e->force_wpb) continue;
+        const int occ = mc32_occupancy(c, ws_stride);
+        if (occ * c > best_res) { best_res = occ * c; best_w = c; best_occ = occ; }
+    }
+    require(best_res > 0, "model too large for the mixed-precision path's shared memory");
+    wpb = best_w;
+    const long long need = (nchains + wpb - 1) / wpb;
+    blocks = (int)std::min<long long>((long long)best_occ * e->num_sms, need);
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+extern "C" {
+
+int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const sg_ligand_job* jobs, int njobs,
+                    const sg_mc_params* p, int refine, sg_ligand_result* out) {
+    return guarded(e, [&] {
+        require(jobs && p && out && njobs > 0 && njobs <= (1 << 22), "dock_batch32: bad arguments");
+        require(e->precision != SG_PREC_FP64, "dock_batch32 needs an engine created with SG_PREC_FP32 or SG_PREC_FP32_H16");
+        require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->maxiters >= 0 && p->temperature > 0,
+                "dock_batch32: bad search parameters");
+        require(e->has_tables, "no tables set");
+        RecState& r = receptor_for(e, rid);
+        PackedModels pm;
+        pack_models(e, models, nmodels, pm);
+        ensure_model_maps(e, r, pm, models, nmodels);
+        check_packed(e, r, models, nmodels);
+        uint64_t h2d = pm.ints.bytes + pm.flts.bytes + pm.dbls.bytes + pm.dmodels.bytes, d2h = 0;
+        size_t ws_stride = 0;
+        for (const DModel& h : pm.host) ws_stride = std::max(ws_stride, ws32_bytes(h));
+        ws_stride = (ws_stride + 15) & ~(size_t)15;
+        const int S = p->num_saved_mins;
+        // chains of every job, with their result slots
+        std::vector<Chain32> hc;
+        std::vector<int> chain_job;
+        std::vector<size_t> cres_off, xres_off;
+        size_t nconf_res = 0, nxyz_res = 0;
+        for (int j = 0; j < njobs; j++) {
+            const sg_ligand_job& J = jobs[j];
+            require(J.model >= 0 && J.model < nmodels && J.num_chains >= 1 && J.num_chains <= (1 << 16) && J.maxiters >= 0,
+                    "dock_batch32: bad ligand job");
+            require(out[j].e && out[j].conf && out[j].coords, "dock_batch32: null result arrays");
+            const DModel& h = pm.host[J.model];
+            for (int c = 0; c < J.num_chains; c++) {
+                Chain32 ch{};
+                ch.model = J.model;
+                ch.steps = J.num_steps;
+                ch.maxiters = J.maxiters > 0 ? J.maxiters : p->maxiters;
+                ch.key0 = (uint32_t)J.seed;
+                ch.key1 = (uint32_t)(J.seed >> 32) ^ (uint32_t)(J.ligand_key >> 32);
+                ch.lig = (uint32_t)J.ligand_key;
+                ch.chain = (uint32_t)c;
+                hc.push_back(ch);
+                chain_job.push_back(j);
+                cres_off.push_back(nconf_res);
+                xres_off.push_back(nxyz_res);
+                nconf_res += (size_t)S * h.conf_size;
+                nxyz_res += (size_t)S * h.nheavy * 3;
+            }
+        }
+        const int nchains = (int)hc.size();
+        require(nchains <= (1 << 24), "dock_batch32: too many chains");
+        DevBuf d_e, d_conf, d_xyz, d_order, d_count, d_evals, d_hits, d_queue;
+        d_e.alloc((size_t)nchains * S * sizeof(double));
+        d_conf.alloc(std::max<size_t>(1, nconf_res) * sizeof(double));
+        d_xyz.alloc(std::max<size_t>(1, nxyz_res) * sizeof(float));
+        d_order.alloc((size_t)nchains * S * sizeof(int));
+        d_count.alloc((size_t)nchains * sizeof(int));
+        d_evals.alloc((size_t)nchains * sizeof(unsigned long long));
+        d_hits.alloc((size_t)nchains * 2 * sizeof(unsigned long long));
+        d_queue.alloc(sizeof(unsigned));
+        cuda_check(cudaMemsetAsync(d_queue.p, 0, sizeof(unsigned), e->stream), "queue reset");
+        for (int k = 0; k < nchains; k++) {
+            Chain32& ch = hc[k];
+            ch.out_e = d_e.as<double>() + (size_t)k * S;
+            ch.out_conf = d_conf.as<double>() + cres_off[k];
+            ch.out_coords = d_xyz.as<float>() + xres_off[k];
+            ch.out_order = d_order.as<int>() + (size_t)k * S;
+            ch.out_count = d_count.as<int>() + k;
+            ch.evals = d_evals.as<unsigned long long>() + k;
+            ch.hits = d_hits.as<unsigned long long>() + 2 * k;
+        }
+        // longest first, so the persistent kernel's queue ends evenly
+        std::vector<int> order(nchains);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return (double)hc[a].steps * pm.host[hc[a].model].cost * std::max(1, hc[a].maxiters) >
+                   (double)hc[b].steps * pm.host[hc[b].model].cost * std::max(1, hc[b].maxiters);
+        });
+        std::vector<Chain32> queue(nchains);
+        for (int k = 0; k < nchains; k++) queue[k] = hc[order[k]];
+        DevBuf d_chains;
+        d_chains.upload(queue.data(), queue.size() * sizeof(Chain32), e->stream);
+        h2d += d_chains.bytes;
+        MCParams32 P{};
+        for (int i = 0; i < 3; i++) {
+            P.hunt[i] = (float)p->hunt_cap[i];
+            P.auth[i] = (float)p->authentic_v[i];
+            P.box_lo[i] = r.gd.begin[i];
+            P.box_hi[i] = r.gd.end[i];
+        }
+        P.slope = (float)p->cache_slope;
+        P.temperature = p->temperature;
+        P.amplitude = p->mutation_amplitude;
+        P.min_rmsd = p->min_rmsd;
+        P.num_saved = S;
+        P.maxiters = p->maxiters;
+        P.accurate_line = p->accurate_line;
+        P.early_term = p->early_term;
+        int wpb = 1, blocks = 1;
+        choose_launch(e, ws_stride, nchains, wpb, blocks);
+        cudaEvent_t ev[4];
+        for (auto& x : ev) cuda_check(cudaEventCreate(&x), "event");
+        struct EvGuard {
+            cudaEvent_t* v;
+            ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(v[i]); }
+        } evg{ev};
+        cuda_check(cudaEventRecord(ev[0], e->stream), "event");
+        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), d_chains.as<Chain32>(), nchains, P,
+                               d_queue.as<unsigned>(), blocks, wpb, ws_stride, e->stream),
+                   "search launch");
+        cuda_check(cudaEventRecord(ev[1], e->stream), "event");
+        std::vector<double> he((size_t)nchains * S), hconf(nconf_res);
+        std::vector<float> hxyz(nxyz_res);
+        std::vector<int> horder((size_t)nchains * S), hcount(nchains);
+        std::vector<unsigned long long> hev(nchains), hhits(2 * (size_t)nchains);
+        auto fetch = [&](void* dst, const DevBuf& src, size_t bytes) {
+            if (!bytes) return;
+            cuda_check(cudaMemcpyAsync(dst, src.p, bytes, cudaMemcpyDeviceToHost, e->stream), "fetch results");
+            d2h += bytes;
+        };
+        fetch(he.data(), d_e, he.size() * sizeof(double));
+        fetch(hconf.data(), d_conf, hconf.size() * sizeof(double));
+        fetch(hxyz.data(), d_xyz, hxyz.size() * sizeof(float));
+        fetch(horder.data(), d_order, horder.size() * sizeof(int));
+        fetch(hcount.data(), d_count, hcount.size() * sizeof(int));
+        fetch(hev.data(), d_evals, hev.size() * sizeof(unsigned long long));
+        fetch(hhits.data(), d_hits, hhits.size() * sizeof(unsigned long long));
+        cuda_check(cudaStreamSynchronize(e->stream), "search");
+        float mc_ms = 0;
+        cuda_check(cudaEventElapsedTime(&mc_ms, ev[0], ev[1]), "event time");
+        // merge_output_containers per ligand (chains in job order)
+        std::vector<std::vector<HostPose>> merged(njobs);
+        std::vector<uint64_t> job_evals(njobs, 0);
+        uint64_t tot_evals = 0, tot_grid = 0, tot_pair = 0;
+        for (int k = 0; k < nchains; k++) {
+            const int j = chain_job[k];
+            const DModel& h = pm.host[hc[k].model];
+            job_evals[j] += hev[k];
+            tot_evals += hev[k];
+            tot_grid += hhits[2 * k];
+            tot_pair += hhits[2 * k + 1];
+            const int cnt = std::min(std::max(hcount[k], 0), S);
+            for (int i = 0; i < cnt; i++) {
+                const int slot = horder[(size_t)k * S + i];
+                require(slot >= 0 && slot < S, "dock_batch32: corrupt result order");
+                HostPose t;
+                t.e = he[(size_t)k * S + slot];
+                const double* c = &hconf[cres_off[k] + (size_t)slot * h.conf_size];
+                t.conf.assign(c, c + h.conf_size);
+                const float* x = &hxyz[xres_off[k] + (size_t)slot * h.nheavy * 3];
+                t.xyz.assign(x, x + (size_t)h.nheavy * 3);
+                add_pose(merged[j], std::move(t), 2.0, S);
+            }
+        }
+        // refine_structure of every merged pose, FP64 on the direct sum
+        float ref_ms = 0;
+        if (refine) {
+            int nposes = 0;
+            for (auto& v : merged) nposes += (int)v.size();
+            if (nposes > 0) {
+                require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+                const int cs = pm.max_conf, hs = std::max(1, pm.max_heavy);
+                std::vector<double> confs((size_t)nposes * cs, 0.0);
+                std::vector<int> pmodel(nposes), pmaxit(nposes);
+                int q = 0;
+                for (int j = 0; j < njobs; j++)
+                    for (auto& t : merged[j]) {
+                        std::memcpy(&confs[(size_t)q * cs], t.conf.data(), t.conf.size() * sizeof(double));
+                        pmodel[q] = jobs[j].model;
+                        pmaxit[q] = jobs[j].maxiters > 0 ? jobs[j].maxiters : p->maxiters;
+                        q++;
+                    }
+                DevBuf dc, de, dx, dpm, dmi;
+                dc.upload(confs.data(), confs.size() * sizeof(double), e->stream);
+                dpm.upload(pmodel.data(), pmodel.size() * sizeof(int), e->stream);
+                dmi.upload(pmaxit.data(), pmaxit.size() * sizeof(int), e->stream);
+                h2d += dc.bytes + dpm.bytes + dmi.bytes;
+                de.alloc((size_t)nposes * sizeof(double));
+                dx.alloc((size_t)nposes * hs * 3 * sizeof(double));
+                cuda_check(cudaEventRecord(ev[2], e->stream), "event");
+                cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(),
+                                           dpm.as<int>(), nposes, dc.as<double>(), cs, p->authentic_v, p->maxiters,
+                                           dmi.as<int>(), p->accurate_line, p->early_term, de.as<double>(),
+                                           dx.as<double>(), hs, e->d_err.as<int>(), e->stream),
+                           "refine launch");
+                cuda_check(cudaEventRecord(ev[3], e->stream), "event");
+                std::vector<double> re(nposes), rx((size_t)nposes * hs * 3);
+                fetch(confs.data(), dc, confs.size() * sizeof(double));
+                fetch(re.data(), de, re.size() * sizeof(double));
+                fetch(rx.data(), dx, rx.size() * sizeof(double));
+                e->check_device_errors();
+                cuda_check(cudaEventElapsedTime(&ref_ms, ev[2], ev[3]), "event time");
+                q = 0;
+                for (int j = 0; j < njobs; j++) {
+                    const DModel& h = pm.host[jobs[j].model];
+                    for (auto& t : merged[j]) {
+                        std::memcpy(t.conf.data(), &confs[(size_t)q * cs], t.conf.size() * sizeof(double));
+                        t.e = re[q];
+                        t.xyz.assign(&rx[(size_t)q * hs * 3], &rx[(size_t)q * hs * 3] + (size_t)h.nheavy * 3);
+                        q++;
+                    }
+                    std::stable_sort(merged[j].begin(), merged[j].end(),
+                                     [](const HostPose& a, const HostPose& b) { return a.e < b.e; });
+                }
+            }
+        }
+        for (int j = 0; j < njobs; j++) {
+            const DModel& h = pm.host[jobs[j].model];
+            out[j].count = (int)merged[j].size();
+            out[j].evals = job_evals[j];
+            for (size_t i = 0; i < merged[j].size(); i++) {
+                out[j].e[i] = merged[j][i].e;
+                std::memcpy(out[j].conf + i * h.conf_size, merged[j][i].conf.data(), h.conf_size * sizeof(double));
+                std::memcpy(out[j].coords + i * h.nheavy * 3, merged[j][i].xyz.data(), (size_t)h.nheavy * 3 * sizeof(double));
+            }
+        }
+        e->last_wpb = wpb;
+        e->last_blocks = blocks;
+        e->last_mc_ms = mc_ms;
+        e->last_refine_ms = ref_ms;
+        e->last_evals = tot_evals;
+        e->last_grid_hits = tot_grid;
+        e->last_pair_hits = tot_pair;
+        e->last_h2d = h2d;
+        e->last_d2h = d2h;
+    });
+}
+
+int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms, int* chains_per_block, int* blocks) {
+    if (!e) return SG_ERR_ARG;
+    if (mc_ms) *mc_ms = e->last_mc_ms;
+    if (refine_ms) *refine_ms = e->last_refine_ms;
+    if (chains_per_block) *chains_per_block = e->last_wpb;
+    if (blocks) *blocks = e->last_blocks;
+    return SG_OK;
+}
+
+int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookups, uint64_t* pair_lookups,
+                      uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+    if (!e) return SG_ERR_ARG;
+    if (evals) *evals = e->last_evals;
+    if (grid_lookups) *grid_lookups = e->last_grid_hits;
+    if (pair_lookups) *pair_lookups = e->last_pair_hits;
+    if (h2d_bytes) *h2d_bytes = e->last_h2d;
+    if (d2h_bytes) *d2h_bytes = e->last_d2h;
+    return SG_OK;
+}
+
+int sg_set_chains_per_block(sg_engine* e, int n) {
+    if (!e || !(n == 0 || n == 1 || n == 2 || n == 4)) return SG_ERR_ARG;
+    e->force_wpb = n;
+    return SG_OK;
+}
+
+}  // extern "C"

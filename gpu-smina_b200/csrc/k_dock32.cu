@@ -1,0 +1,555 @@
+// Mixed-precision path, part 2: the batched Monte Carlo search.
+//
+// A persistent kernel: every warp takes chains from a global queue (ordered
+// longest first on the host) until the queue is empty, so ligands of very
+// different sizes and step counts share the GPU without a tail.  One warp
+// runs one chain: mutate, BFGS on the hunt-capped energy, Metropolis test,
+// BFGS on the authentic energy for accepted poses, and the chain's output
+// container in global memory.  Confs, the inverse Hessian, the Armijo test
+// and the orientation increment stay in FP64; energies and gradients come
+// from the FP32 evaluation.  Random numbers: Philox4x32-10 keyed by the
+// request seed, counter (draw, ligand key, chain) -- independent of the
+// batch composition and of the launch shape.
+// Reference semantics: monte_carlo.cpp:95-130; mutate.cpp:35-63;
+// bfgs.h:30-282; conf.h:98-404; coords.cpp:25-58 (add_to_output_container).
+#include "dock32_eval.cuh"
+
+namespace sg {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    // butterfly: every lane ends with the same bits (each step adds the
+    // same two operands on both partners)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull32, v, o);
+    return v;
+}
+__device__ __forceinline__ double dotd(const W32& w, const double* a, const double* b, int n) {
+    double t = 0;
+    for (int i = w.lane; i < n; i += 32) t += a[i] * b[i];
+    return warp_sum_d(t);
+}
+__device__ __forceinline__ void copyd(const W32& w, double* d, const double* s, int n) {
+    for (int i = w.lane; i < n; i += 32) d[i] = s[i];
+    __syncwarp();
+}
+
+// quaternion_increment (quaternion.cpp:118-126) with an FP32 sine/cosine of
+// the half angle, composed and re-normalised in FP64
+__device__ void q_increment32(double* c, double rx, double ry, double rz) {
+    const double ang = sqrt(rx * rx + ry * ry + rz * rz);
+    double s = 0, co = 1;
+    if (ang > kEps) {
+        double a = ang;
+        normalize_angle(a);
+        float sf, cf;
+        sincosf((float)(0.5 * a), &sf, &cf);
+        s = (double)sf / ang;
+        co = (double)cf;
+    }
+    Quat<double> q{c[0], c[1], c[2], c[3]};
+    q = qmul(Quat<double>{co, s * rx, s * ry, s * rz}, q);
+    q_normalize_approx(q);
+    c[0] = q.a; c[1] = q.b; c[2] = q.c; c[3] = q.d;
+}
+
+// conf::increment
+__device__ void increment32(const W32& w, double* x, const double* p, double alpha) {
+    const DModel& m = *w.m;
+    for (int l = w.lane; l < m.nlig; l += 32) {
+        const int f = __ldg(m.lig_root + l);
+        double* c = x + __ldg(m.fconf + f);
+        const double* d = p + __ldg(m.fdof + f);
+        c[0] += alpha * d[0]; c[1] += alpha * d[1]; c[2] += alpha * d[2];
+        q_increment32(c + 3, alpha * d[3], alpha * d[4], alpha * d[5]);
+    }
+    for (int k = w.lane; k < m.ntors; k += 32) {
+        double& t = x[__ldg(m.tor_conf + k)];
+        t += normalized_angle(alpha * p[__ldg(m.tor_dof + k)]);
+        normalize_angle(t);
+    }
+    __syncwarp();
+}
+
+// conf::operator()(index): value of change coordinate i (accurate line search)
+__device__ double conf_value32(const DModel& m, const double* x, int i) {
+    for (int l = 0; l < m.nlig; l++) {
+        const int f = __ldg(m.lig_root + l);
+        const int d0 = __ldg(m.fdof + f);
+        if (i >= d0 && i < d0 + 3) return x[__ldg(m.fconf + f) + (i - d0)];
+        if (i >= d0 + 3 && i < d0 + 6) {
+            const double* c = x + __ldg(m.fconf + f);
+            const V3<double> a = q_to_angle(Quat<double>{c[3], c[4], c[5], c[6]});
+            const int j = i - d0 - 3;
+            return j == 0 ? a.x : j == 1 ? a.y : a.z;
+        }
+    }
+    for (int k = 0; k < m.ntors; k++)
+        if (__ldg(m.tor_dof + k) == i) return x[__ldg(m.tor_conf + k)];
+    return 0;
+}
+
+struct Mode32 {
+    float v[3];
+    float slope;
+};
+
+__device__ __forceinline__ double feval32(W32& w, const double* x, double* g, const Mode32& em) {
+    return (double)eval_deriv32(w, x, em.v, em.slope, g);
+}
+
+// ---- line searches (bfgs.h:30-200) ------------------------------------------------------
+__device__ double line_fast32(W32& w, const double* x, const double* g, double f0, const double* p, double* x_new,
+                              double* g_new, double& f1, const Mode32& em) {
+    const DModel& m = *w.m;
+    double alpha = 1;
+    const double pg = dotd(w, p, g, m.dof);
+    for (unsigned trial = 0; trial < 10; trial++) {
+        copyd(w, x_new, x, m.conf_size);
+        increment32(w, x_new, p, alpha);
+        f1 = feval32(w, x_new, g_new, em);
+        if (f1 - f0 < 0.0001 * alpha * pg) break;
+        alpha *= 0.5;
+    }
+    return alpha;
+}
+
+__device__ double line_accurate32(W32& w, const double* x, const double* g, double f0, const double* p, double* x_new,
+                                  double* g_new, double& f1, const Mode32& em) {
+    const DModel& m = *w.m;
+    const int n = m.dof;
+    double a, alpha, alpha2 = 0, alamin, b, disc, f2 = 0, rhs1, rhs2, tmplam = 0;
+    const double ALF = 1.0e-4, FIRST = 1.0;
+    const double slope = dotd(w, g, p, n);
+    auto give_up = [&]() {
+        copyd(w, x_new, x, m.conf_size);
+        for (int i = w.lane; i < n; i += 32) g_new[i] = 0;
+        __syncwarp();
+        return 0.0;
+    };
+    if (slope >= 0) return give_up();
+    double test = 0;
+    for (int i = w.lane; i < n; i += 32) test = fmax(test, fabs(p[i]) / fmax(fabs(conf_value32(m, x, i)), 1.0));
+    for (int o = 16; o > 0; o >>= 1) test = fmax(test, __shfl_xor_sync(kFull32, test, o));
+    alamin = kEps / test;
+    alpha = FIRST;
+    // alpha at least halves every round, so 128 rounds reach any alamin > 0
+    for (int it = 0; it < 128; it++) {
+        copyd(w, x_new, x, m.conf_size);
+        increment32(w, x_new, p, alpha);
+        f1 = feval32(w, x_new, g_new, em);
+        if (alpha < alamin) return give_up();
+        if (f1 <= f0 + ALF * alpha * slope) return alpha;
+        if (alpha == FIRST) {
+            tmplam = -slope / (2.0 * (f1 - f0 - slope));
+        } else {
+            rhs1 = f1 - f0 - alpha * slope;
+            rhs2 = f2 - f0 - alpha2 * slope;
+            a = (rhs1 / (alpha * alpha) - rhs2 / (alpha2 * alpha2)) / (alpha - alpha2);
+            b = (-alpha2 * rhs1 / (alpha * alpha) + alpha * rhs2 / (alpha2 * alpha2)) / (alpha - alpha2);
+            if (a == 0.0) {
+                tmplam = -slope / (2.0 * b);
+            } else {
+                disc = b * b - 3.0 * a * slope;
+                if (disc < 0) tmplam = 0.5 * alpha;
+                else if (b <= 0) tmplam = (-b + sqrt(disc)) / (3.0 * a);
+                else tmplam = -slope / (b + sqrt(disc));
+            }
+            if (tmplam > .5 * alpha) tmplam = .5 * alpha;
+        }
+        alpha2 = alpha;
+        f2 = f1;
+        alpha = fmax(tmplam, 0.1 * alpha);
+    }
+    return give_up();
+}
+
+// ---- BFGS (bfgs.h:202-282) on a full symmetric n x n inverse Hessian ------------------------
+// Lane i owns row i, stored as column i of h (h[j * n + i]) so the lanes of
+// a row sweep read consecutive words.  Every entry (i, j) is computed from
+// (min(i, j), max(i, j)) operands in one fixed order, so h stays exactly
+// symmetric.
+__device__ __noinline__ double bfgs32(W32& w, double* x, int maxiters, int accurate, int early, const Mode32& em) {
+    const DModel& m = *w.m;
+    const int n = m.dof, cs = m.conf_size;
+    double* h = w.d(w.L.h);
+    double *g = w.d(w.L.g), *g_new = w.d(w.L.g_new), *g_orig = w.d(w.L.g_orig), *p = w.d(w.L.p), *y = w.d(w.L.y);
+    double *x_new = w.d(w.L.x_new), *x_orig = w.d(w.L.x_orig), *mhy = w.d(w.L.mhy);
+    for (int i = w.lane; i < n; i += 32)
+        for (int j = 0; j < n; j++) h[j * n + i] = (i == j) ? 1.0 : 0.0;
+    __syncwarp();
+    double f0 = feval32(w, x, g, em);
+    const double f_orig = f0;
+    copyd(w, g_orig, g, n);
+    copyd(w, x_orig, x, cs);
+    for (int step = 0; step < maxiters; step++) {
+        SG_T0(t_alg);
+        for (int i = w.lane; i < n; i += 32) {
+            double sum = 0;
+            for (int j = 0; j < n; j++) sum += h[j * n + i] * g[j];
+            p[i] = -sum;
+        }
+        __syncwarp();
+        SG_T1(t_alg, 5);
+        double f1 = 0;
+        const double alpha = accurate ? line_accurate32(w, x, g, f0, p, x_new, g_new, f1, em)
+                                      : line_fast32(w, x, g, f0, p, x_new, g_new, f1, em);
+        if (alpha == 0) break;
+        SG_T0(t_alg2);
+        for (int i = w.lane; i < n; i += 32) y[i] = g_new[i] - g[i];
+        __syncwarp();
+        const double prevf0 = f0;
+        f0 = f1;
+        copyd(w, x, x_new, cs);
+        if (early && fabs(prevf0 - f0) < 1e-5) break;
+        copyd(w, g, g_new, n);
+        if (!(dotd(w, g, g, n) >= 1e-4)) break;
+        if (step == 0) {
+            const double yy = dotd(w, y, y, n);
+            if (fabs(yy) > kEps) {
+                const double dg = alpha * dotd(w, y, p, n) / yy;
+                for (int i = w.lane; i < n; i += 32) h[i * n + i] = dg;
+                __syncwarp();
+            }
+        }
+        // bfgs_update
+        const double yp = dotd(w, y, p, n);
+        if (alpha * yp >= kEps) {
+            for (int i = w.lane; i < n; i += 32) {
+                double sum = 0;
+                for (int j = 0; j < n; j++) sum += h[j * n + i] * y[j];
+                mhy[i] = -sum;
+            }
+            __syncwarp();
+            const double yhy = -dotd(w, y, mhy, n);
+            const double r = 1 / (alpha * yp);
+            const double c1 = alpha * r, c2 = alpha * alpha * (r * r * yhy + r);
+            for (int i = w.lane; i < n; i += 32)
+                for (int j = 0; j < n; j++) {
+                    const int lo = min(i, j), hi = max(i, j);
+                    h[j * n + i] += c1 * (mhy[lo] * p[hi] + mhy[hi] * p[lo]) + c2 * p[lo] * p[hi];
+                }
+            __syncwarp();
+        }
+        SG_T1(t_alg2, 5);
+    }
+    if (!(f0 <= f_orig)) {
+        f0 = f_orig;
+        copyd(w, x, x_orig, cs);
+        copyd(w, g, g_orig, n);
+    }
+    return f0;
+}
+
+// ---- Monte Carlo pieces -------------------------------------------------------------------
+__device__ V3<double> sphere32(Philox& rng) {  // random_inside_sphere, bounded rejection
+    for (int k = 0; k < 64; k++) {
+        const double a = ph_range(rng, -1, 1), b = ph_range(rng, -1, 1), c = ph_range(rng, -1, 1);
+        if (a * a + b * b + c * c < 1) return V3<double>{a, b, c};
+    }
+    return V3<double>{0, 0, 0};
+}
+
+// gyration radius of ligand l's heavy atoms about its root origin (current coords)
+__device__ double gyration32(const W32& w, int l) {
+    const DModel& m = *w.m;
+    const float3 o = f3(w.origin()[__ldg(m.lig_root + l)]);
+    float acc = 0;
+    int cnt = 0;
+    for (int i = __ldg(m.lig_begin + l) + w.lane; i < __ldg(m.lig_end + l); i += 32)
+        if (!is_h(__ldg(m.type + i))) {
+            const float3 d = f3(w.coords()[i]) - o;
+            acc += dot3(d, d);
+            cnt++;
+        }
+    acc = warp_sum(acc);
+    for (int s = 16; s > 0; s >>= 1) cnt += __shfl_xor_sync(kFull32, cnt, s);
+    return cnt > 0 ? sqrt((double)acc / cnt) : 0.0;
+}
+
+__device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude) {
+    const DModel& m = *w.m;
+    int num = 0;
+    for (int b = 0; b < m.nblocks; b++) num += (__ldg(m.blk_rigid + b) ? 2 : 0) + __ldg(m.blk_ntors + b);
+    if (num == 0) return;
+    int which = ph_int(rng, num);
+    int lig = 0;
+    for (int b = 0; b < m.nblocks; b++) {
+        double* c = x + __ldg(m.blk_conf + b);
+        if (__ldg(m.blk_rigid + b)) {
+            if (which == 0) {
+                const V3<double> d = amplitude * sphere32(rng);
+                if (w.lane == 0) { c[0] += d.x; c[1] += d.y; c[2] += d.z; }
+                __syncwarp();
+                return;
+            }
+            --which;
+            if (which == 0) {
+                const double gr = gyration32(w, lig);
+                if (gr > kEps) {
+                    const V3<double> rot = (amplitude / gr) * sphere32(rng);
+                    if (w.lane == 0) q_increment32(c + 3, rot.x, rot.y, rot.z);
+                    __syncwarp();
+                }
+                return;
+            }
+            --which;
+            c += 7;
+            lig++;
+        }
+        const int nt = __ldg(m.blk_ntors + b);
+        if (which < nt) {
+            const double t = ph_range(rng, -kPi, kPi);
+            if (w.lane == 0) c[which] = t;
+            __syncwarp();
+            return;
+        }
+        which -= nt;
+    }
+}
+
+// conf::randomize: position uniform in the box, orientation from four
+// normal deviates, torsions uniform in [-pi, pi)
+__device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams32& P) {
+    const DModel& m = *w.m;
+    for (int b = 0; b < m.nblocks; b++) {
+        double* c = x + __ldg(m.blk_conf + b);
+        if (__ldg(m.blk_rigid + b)) {
+            double v[7];
+            for (int k = 0; k < 3; k++) v[k] = ph_range(rng, P.box_lo[k], P.box_hi[k]);
+            double q[4], nq = 0;
+            for (int k = 0; k < 4; k++) { q[k] = ph_normal(rng); nq += q[k] * q[k]; }
+            nq = sqrt(nq);
+            if (nq > kEps) for (int k = 0; k < 4; k++) v[3 + k] = q[k] / nq;
+            else { v[3] = 1; v[4] = v[5] = v[6] = 0; }
+            if (w.lane == 0) for (int k = 0; k < 7; k++) c[k] = v[k];
+            c += 7;
+        }
+        const int nt = __ldg(m.blk_ntors + b);
+        for (int t = 0; t < nt; t++) {
+            const double a = ph_range(rng, -kPi, kPi);
+            if (w.lane == 0) c[t] = a;
+        }
+    }
+    __syncwarp();
+}
+
+// add_to_output_container with the chain's container in global memory;
+// returns the new size
+__device__ int add_output32(const W32& w, const Chain32& ch, const double* x, double e, double min_rmsd, int max_size,
+                            int count) {
+    const DModel& m = *w.m;
+    const int H = m.nheavy, cs = m.conf_size;
+    const float4* X = w.coords();
+    // RMSD to every saved pose: lanes over atoms, one pose at a time
+    float best = 3.4e38f;
+    int bj = count;
+    for (int j = 0; j < count; j++) {
+        const float* oc = ch.out_coords + (size_t)ch.out_order[j] * H * 3;
+        float acc = 0;
+        for (int a = w.lane; a < H; a += 32) {
+            const float3 c = f3(X[__ldg(m.heavy + a)]);
+            const float dx = c.x - oc[3 * a], dy = c.y - oc[3 * a + 1], dz = c.z - oc[3 * a + 2];
+            acc += dx * dx + dy * dy + dz * dz;
+        }
+        acc = warp_sum(acc);
+        const float r = H > 0 ? sqrtf(acc / H) : 0.f;
+        if (j == 0 || r < best) { bj = j; best = r; }
+    }
+    int target = -1;
+    if (bj < count && best < min_rmsd) {
+        if (e < ch.out_e[ch.out_order[bj]]) target = ch.out_order[bj];
+    } else if (count < max_size) {
+        target = count;
+        if (w.lane == 0) ch.out_order[count] = count;
+        count++;
+    } else if (count > 0 && e < ch.out_e[ch.out_order[count - 1]]) {
+        target = ch.out_order[count - 1];
+    }
+    __syncwarp();
+    if (target >= 0) {
+        for (int i = w.lane; i < cs; i += 32) ch.out_conf[(size_t)target * cs + i] = x[i];
+        for (int a = w.lane; a < H; a += 32) {
+            const float3 c = f3(X[__ldg(m.heavy + a)]);
+            float* o = ch.out_coords + ((size_t)target * H + a) * 3;
+            o[0] = c.x; o[1] = c.y; o[2] = c.z;
+        }
+        if (w.lane == 0) ch.out_e[target] = e;
+    }
+    __syncwarp();
+    if (w.lane == 0) {
+        *ch.out_count = count;
+        for (int i = 1; i < count; i++) {  // stable insertion sort by energy
+            const int key = ch.out_order[i];
+            const double ek = ch.out_e[key];
+            int j = i - 1;
+            while (j >= 0 && ch.out_e[ch.out_order[j]] > ek) { ch.out_order[j + 1] = ch.out_order[j]; j--; }
+            ch.out_order[j + 1] = key;
+        }
+    }
+    __syncwarp();
+    return count;
+}
+
+// monte_carlo::operator() for one chain
+__device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCParams32& P) {
+    SG_T0(t_chain);
+    const DModel& m = *w.m;
+    const int cs = m.conf_size;
+    // model state as read (mutation may read it before the first set)
+    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);
+    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
+    __syncwarp();
+    Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
+    double* tmp = w.d(w.L.x_tmp);
+    double* cand = w.d(w.L.x_cand);
+    randomize32(w, rng, tmp, P);
+    const Mode32 hunt{{P.hunt[0], P.hunt[1], P.hunt[2]}, P.slope};
+    const Mode32 auth{{P.auth[0], P.auth[1], P.auth[2]}, P.slope};
+    double tmp_e = 0, best_e = kMaxFl;
+    int count = 0;
+    if (w.lane == 0) *ch.out_count = 0;
+    for (unsigned step = 0; step < ch.steps; step++) {
+        copyd(w, cand, tmp, cs);
+        mutate32(w, rng, cand, P.amplitude);
+        const double cand_e = bfgs32(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt);
+        bool accept = step == 0 || cand_e < tmp_e;
+        if (!accept) accept = ph_u01(rng) < exp((tmp_e - cand_e) / P.temperature);
+        if (accept) {
+            copyd(w, tmp, cand, cs);
+            tmp_e = cand_e;
+            set_conf32(w, tmp);
+            if (tmp_e < best_e || count < P.num_saved) {
+                tmp_e = bfgs32(w, tmp, ch.maxiters, P.accurate_line, P.early_term, auth);
+                set_conf32(w, tmp);
+                count = add_output32(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved, count);
+                if (tmp_e < best_e) best_e = tmp_e;
+            }
+        }
+    }
+    unsigned long long gh = w.grid_hits, ph = w.pair_hits;
+    for (int o = 16; o > 0; o >>= 1) {
+        gh += __shfl_xor_sync(kFull32, gh, o);
+        ph += __shfl_xor_sync(kFull32, ph, o);
+    }
+    if (w.lane == 0) {
+        *ch.evals = w.evals;
+        ch.hits[0] = gh;
+        ch.hits[1] = ph;
+    }
+    __syncwarp();
+    SG_T1(t_chain, 7);
+}
+
+// Persistent search kernel: warps pull chains from *queue until it runs out.
+__global__ void __launch_bounds__(128, 4) k_mc32(const DModel* models, DTables32 T, DMaps32 G, const Chain32* chains,
+                                                 int nchains, MCParams32 P, unsigned* queue, int ws_stride) {
+    __shared__ DTables32 sT;
+    __shared__ DMaps32 sG;
+    extern __shared__ __align__(16) char smem32[];
+    if (threadIdx.x == 0) { sT = T; sG = G; }
+    __syncthreads();
+    W32 w;
+    w.s = smem32 + (size_t)(threadIdx.x >> 5) * ws_stride;
+    w.T = &sT;
+    w.G = &sG;
+    w.lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned c = 0;
+        if (w.lane == 0) c = atomicAdd(queue, 1u);
+        c = __shfl_sync(kFull32, c, 0);
+        if (c >= (unsigned)nchains) break;
+        const Chain32 ch = chains[c];
+        const DModel* gm = models + ch.model;
+        w.L = ws32_layout(gm->natoms, gm->nframes, gm->conf_size, gm->dof);
+        w.bind_model(gm);
+        w.evals = 0;
+        w.grid_hits = 0;
+        w.pair_hits = 0;
+        run_chain32(w, ch, P);
+    }
+}
+
+// model::eval_deriv in FP32 for a batch of confs of one model (one warp per conf)
+__global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T, DMaps32 G, int n, const double* confs,
+                                               float v0, float v1, float v2, float slope, double* out_e, double* out_g,
+                                               double* out_coords) {
+    __shared__ DTables32 sT;
+    __shared__ DMaps32 sG;
+    extern __shared__ __align__(16) char smem32[];
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    if (threadIdx.x == 0) { sT = T; sG = G; }
+    __syncthreads();
+    W32 w;
+    w.s = smem32;
+    w.T = &sT;
+    w.G = &sG;
+    w.lane = threadIdx.x & 31;
+    w.evals = 0;
+    w.grid_hits = 0;
+    w.pair_hits = 0;
+    w.L = ws32_layout(model->natoms, model->nframes, model->conf_size, model->dof);
+    w.bind_model(model);
+    const DModel& m = *w.m;
+    double* x = w.d(w.L.x_tmp);
+    copyd(w, x, confs + (size_t)k * m.conf_size, m.conf_size);
+    double* g = w.d(w.L.g);
+    const float v[3] = {v0, v1, v2};
+    const float e = eval_deriv32(w, x, v, slope, g);
+    if (w.lane == 0) out_e[k] = e;
+    for (int i = w.lane; i < m.dof; i += 32) out_g[(size_t)k * m.dof + i] = g[i];
+    if (out_coords)
+        for (int i = w.lane; i < m.nmov; i += 32) {
+            const float4 c = w.coords()[i];
+            double* o = out_coords + ((size_t)k * m.nmov + i) * 3;
+            o[0] = c.x; o[1] = c.y; o[2] = c.z;
+        }
+}
+
+// ---- host launchers -----------------------------------------------------------------------
+size_t ws32_bytes(const DModel& hm) {
+    return (size_t)ws32_layout(hm.natoms, hm.nframes, hm.conf_size, hm.dof).total;
+}
+
+static cudaError_t prep32(const void* fn, size_t smem) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// resident blocks per SM of k_mc32 with `wpb` chains (warps) per block
+int mc32_occupancy(int wpb, size_t ws_stride) {
+    const size_t smem = (size_t)wpb * ws_stride;
+    if (prep32((const void*)k_mc32, smem) != cudaSuccess) return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_mc32, 32 * wpb, smem) != cudaSuccess) return 0;
+    return blocks;
+}
+
+cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const Chain32* chains, int n,
+                        const MCParams32& P, unsigned* queue, int blocks, int wpb, size_t ws_stride, cudaStream_t s) {
+    const size_t smem = (size_t)wpb * ws_stride;
+    cudaError_t rc = prep32((const void*)k_mc32, smem);
+    if (rc != cudaSuccess) return rc;
+    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, chains, n, P, queue, (int)ws_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval32(const DModel* dm, size_t ws, const DTables32& T, const DMaps32& G, int n, const double* confs,
+                          const double v[3], double slope, double* e, double* g, double* coords, cudaStream_t s) {
+    cudaError_t rc = prep32((const void*)k_eval32, ws);
+    if (rc != cudaSuccess) return rc;
+    k_eval32<<<n, 32, ws, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, e, g, coords);
+    return cudaGetLastError();
+}
+
+#ifdef SG_PROFILE
+cudaError_t profile_read32(unsigned long long* out16, bool clear) {
+    cudaError_t rc = cudaMemcpyFromSymbol(out16, g_prof, sizeof(unsigned long long) * 16);
+    if (rc == cudaSuccess && clear) {
+        static const unsigned long long zero[16] = {};
+        rc = cudaMemcpyToSymbol(g_prof, zero, sizeof(zero));
+    }
+    return rc;
+}
+#endif
+
+}  // namespace sg

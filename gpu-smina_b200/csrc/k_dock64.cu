@@ -127,8 +127,9 @@ __device__ bool within64(W64& w, double margin) {
 // refine_structure for one pose per block
 __global__ void __launch_bounds__(32) k_refine64(const DModel* models, DTables T, const DReceptor* R,
                                                  const int* pose_model, int nposes, double* confs, int conf_stride,
-                                                 double c0, double c1, double c2, int maxiters, int accurate, int early,
-                                                 double* out_e, double* out_coords, int coord_stride, int* err) {
+                                                 double c0, double c1, double c2, int maxiters, const int* pose_maxiters,
+                                                 int accurate, int early, double* out_e, double* out_coords,
+                                                 int coord_stride, int* err) {
     const int k = blockIdx.x;
     if (k >= nposes) return;
     const DModel* mp = models + pose_model[k];
@@ -137,6 +138,7 @@ __global__ void __launch_bounds__(32) k_refine64(const DModel* models, DTables T
     const DModel& m = *mp;
     double* x = w.s + w.L.x_tmp;
     vcopy(w, x, confs + (size_t)k * conf_stride, m.conf_size);
+    if (pose_maxiters) maxiters = pose_maxiters[k];  // per-ligand iteration limit
     double slope = 10;
     double e = 0;
     for (int p = 0; p < 5; p++) {
@@ -191,12 +193,13 @@ cudaError_t launch_mc64(const DModel* dms, size_t smem, const DTables& T, const 
 }
 
 cudaError_t launch_refine64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const int* pose_model,
-                            int n, double* confs, int conf_stride, const double cap[3], int maxiters, int accurate,
-                            int early, double* e, double* coords, int coord_stride, int* err, cudaStream_t s) {
+                            int n, double* confs, int conf_stride, const double cap[3], int maxiters,
+                            const int* pose_maxiters, int accurate, int early, double* e, double* coords,
+                            int coord_stride, int* err, cudaStream_t s) {
     cudaError_t rc = prep((const void*)k_refine64, smem);
     if (rc != cudaSuccess) return rc;
     k_refine64<<<n, 32, smem, s>>>(dms, T, R, pose_model, n, confs, conf_stride, cap[0], cap[1], cap[2], maxiters,
-                                   accurate, early, e, coords, coord_stride, err);
+                                   pose_maxiters, accurate, early, e, coords, coord_stride, err);
     return cudaGetLastError();
 }
 

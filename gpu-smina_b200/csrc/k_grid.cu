@@ -11,7 +11,7 @@
 // 2. k_grid_map64: one thread per grid point, FP64 sums over the point's
 //    cell list in receptor order for a chunk of ligand types; identical
 //    rounding to the CPU's loop (each type's sum is independent).
-// 3. k_grid_narrow: FP32 / FP16 copies for the mixed-precision path.
+// 3. k_grid_pack: packed-corner FP32 / FP16 copies for the mixed-precision path.
 #include "sg_dev.cuh"
 
 namespace sg {
@@ -115,11 +115,28 @@ __global__ void __launch_bounds__(256) k_grid_map64(DGeom g, int natoms, const d
     }
 }
 
-__global__ void k_grid_narrow(const double* src, float* dst32, __half* dst16, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const double v = src[i];
-        if (dst32) dst32[i] = (float)v;
-        if (dst16) dst16[i] = __double2half(v);
+// Packed-corner copies for the mixed-precision path: cell (x, y, z) of the
+// (dim-1)^3 cells stores its 8 corners contiguously, so one trilinear lookup
+// is one 32 B (FP32) or 16 B (FP16) load instead of four row segments.
+__global__ void k_grid_pack(DGeom g, const double* src, float4* dst32, uint4* dst16) {
+    const int cx = g.dim[0] - 1, cy = g.dim[1] - 1, cz = g.dim[2] - 1;
+    const size_t ncells = (size_t)cx * cy * cz;
+    const size_t d0 = g.dim[0], d01 = (size_t)g.dim[0] * g.dim[1];
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncells; c += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = c % cx, y = (c / cx) % cy, z = c / ((size_t)cx * cy);
+        const double* b = src + x + d0 * y + d01 * z;
+        const double v[8] = {b[0], b[1], b[d0], b[d0 + 1], b[d01], b[d01 + 1], b[d01 + d0], b[d01 + d0 + 1]};
+        if (dst32) {
+            dst32[2 * c] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+            dst32[2 * c + 1] = make_float4((float)v[4], (float)v[5], (float)v[6], (float)v[7]);
+        }
+        if (dst16) {
+            uint32_t w[4];
+            for (int k = 0; k < 4; k++)
+                w[k] = (uint32_t)__half_as_ushort(__double2half(v[2 * k])) |
+                       ((uint32_t)__half_as_ushort(__double2half(v[2 * k + 1])) << 16);
+            dst16[c] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 }
 
@@ -141,8 +158,8 @@ cudaError_t launch_grid_map64(const DGeom& g, int natoms, const double* xyz, con
     return cudaGetLastError();
 }
 
-cudaError_t launch_grid_narrow(const double* src, float* d32, __half* d16, size_t n, cudaStream_t s) {
-    k_grid_narrow<<<148 * 8, 256, 0, s>>>(src, d32, d16, n);
+cudaError_t launch_grid_pack(const DGeom& g, const double* src, float4* d32, uint4* d16, cudaStream_t s) {
+    k_grid_pack<<<148 * 8, 256, 0, s>>>(g, src, d32, d16);
     return cudaGetLastError();
 }
 

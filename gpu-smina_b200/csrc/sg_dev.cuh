@@ -21,7 +21,6 @@ struct DTables {
     double factor, cutoff_sqr;
     const double* smooth;  // [pair][n][nc][2]
     const double* fast;    // [pair][n][nc]
-    const float2* smooth32;  // [pair][n] (e, dor) for nc == 1, FP32 path
 };
 
 // grid_dims + grid::init geometry
@@ -48,14 +47,14 @@ struct DReceptor {
     DGeom g;
     const double* map[kNumTypes];        // FP64 maps or null
     const double* cmap[kNumTypes];       // FP64 charge maps or null
-    const float* map32[kNumTypes];       // FP32 copies
-    const float* cmap32[kNumTypes];
-    const __half* map16[kNumTypes];      // FP16 copies
+    const float4* map32[kNumTypes];      // packed-corner FP32 copies
+    const float4* cmap32[kNumTypes];
+    const uint4* map16[kNumTypes];       // packed-corner FP16 copies
 };
 
-// A docking model packed for the device.  Arrays index into two pools
-// (ints, doubles); see pack_model() in engine.cu for the layout.
-struct DModel {
+// A docking model packed for the device.  Arrays index into three pools
+// (ints, doubles, floats); see pack_one() in engine.cu for the layout.
+struct __align__(16) DModel {
     int natoms, nmov, nframes, nlig, nflex, conf_size, dof, npairs, nother, nheavy, nlevels, nblocks;
     const int* type;
     const double* charge;
@@ -92,6 +91,63 @@ struct DModel {
     const int* tor_conf;      // [ntors] conf index of each torsion (block order)
     const int* tor_dof;       // [ntors] change index
     const int* tor_frame;     // [ntors] frame of each torsion
+    // mixed-precision copies
+    const float4* local32;    // [natoms] (x, y, z, charge); lab coords for inflex
+    const float4* lab32;      // [natoms] coords as read
+    const float4* forigin32;  // [F]
+    const float4* faxis32;    // [F]
+    const float4* finit32;    // [F]
+    const int* pair_tp;       // [P] type-pair index, bit 30 set when the pair's types are swapped
+    const int* fsub_end;      // [F] end of the atom range of the frame's subtree (depth-first layout)
+    // mixed-precision pair order: round robin over first-atom groups so the
+    // 32 pairs a warp handles at once touch different atoms
+    const int2* pairs32;      // [P] (a, b)
+    const int* tp32;          // [P] type pair | swapped << 30 | intramolecular (v[0]) << 29
+    int cost;                 // relative cost of one evaluation (atoms + pairs + frames)
+    int pad_[3];
+};
+
+// FP32 pair table: per (type pair, sample i, component) the float4
+// (e_i, dor_i, e_i+1, dor_i+1), so one interpolation is one 16 B load
+struct DTables32 {
+    int nc, n;
+    float factor, cutoff_sqr;
+    const float4* tab;  // [pair][n][nc]
+};
+
+// packed-corner grid maps: each cell's 8 corner values contiguous
+// FP32: 2 x float4 = (f000 f100 f010 f110)(f001 f101 f011 f111); FP16: 1 x uint4
+struct DMaps32 {
+    int cdim[3];  // cells per axis (dim - 1)
+    float init[3], factor[3], factor_inv[3], dim_fl_minus_1[3];
+    const float4* m32[kNumTypes];
+    const float4* c32[kNumTypes];
+    const uint4* m16[kNumTypes];
+    int half;
+};
+
+// Chain bookkeeping of the batched mixed-precision path
+struct Chain32 {
+    int model;
+    unsigned steps;
+    int maxiters;            // BFGS iterations of this ligand's search
+    uint32_t key0, key1;     // request seed (Philox key)
+    uint32_t lig, chain;     // Philox counter words
+    double* out_e;           // [S]
+    double* out_conf;        // [S][conf_size]
+    float* out_coords;       // [S][nheavy][3]
+    int* out_order;          // [S]
+    int* out_count;
+    unsigned long long* evals;
+    unsigned long long* hits;  // [2]: grid lookups, in-cutoff pair lookups
+};
+
+struct MCParams32 {
+    float hunt[3], auth[3];
+    float slope;
+    double temperature, amplitude, min_rmsd;
+    int num_saved, maxiters, accurate_line, early_term;
+    double box_lo[3], box_hi[3];
 };
 
 // Per-warp FP64 workspace layout in shared memory (offsets in doubles)

@@ -8,6 +8,7 @@ There is no CPU fallback: :func:`load` raises if the library is missing.
 Reference interfaces mirrored (paths inside the reference project):
   Engine.eval        model::eval_deriv                 src/lib/model.cpp:969-985
   Engine.dock        monte_carlo::operator() per chain  src/lib/monte_carlo.cpp:95-130
+  Engine.dock_batch  GpuDocking::dock_batch            src/gpu/gpu_docking.cpp:756
   Engine.refine      refine_structure                  src/main/main.cpp:165-190
   Engine.grid        cache::populate                   src/lib/cache.cpp:116-206
   GpuDocking         gpusmina::GpuDocking              src/gpu/gpu_docking.h:51-114
@@ -71,6 +72,15 @@ class ChainResult(C.Structure):
     _fields_ = [("count", C.c_int), ("e", _dp), ("conf", _dp), ("coords", _dp), ("evals", C.c_uint64)]
 
 
+class LigandJob(C.Structure):
+    _fields_ = [("model", C.c_int), ("num_chains", C.c_int), ("num_steps", C.c_uint), ("maxiters", C.c_int),
+                ("seed", C.c_uint64), ("ligand_key", C.c_uint64)]
+
+
+class LigandResult(C.Structure):
+    _fields_ = [("count", C.c_int), ("e", _dp), ("conf", _dp), ("coords", _dp), ("evals", C.c_uint64)]
+
+
 _lib = None
 
 
@@ -117,6 +127,11 @@ def _declare(L):
                       C.c_int, C.c_int, C.c_int, _dp, _dp],
         "sg_bfgs": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, C.c_int, C.c_int,
                     C.c_int, _dp],
+        "sg_dock_batch32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
+                            C.POINTER(MCParams), C.c_int, C.POINTER(LigandResult)],
+        "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
+        "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
+        "sg_set_chains_per_block": [vp, C.c_int],
     }.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -383,6 +398,44 @@ class Engine:
         self._check(load().sg_refine(self._h, rid, descs, len(models), iptr(pm), n, dptr(confs), vec3(cap), maxiters,
                                      accurate_line, early_term, dptr(e), dptr(xyz)))
         return confs, e, xyz
+
+    def dock_batch(self, rid, models, jobs, params: MCParams, refine=True):
+        """Batched mixed-precision docking (sg_dock_batch32).  ``jobs`` is a list
+        of :class:`LigandJob`; returns one dict per job with ``e`` [count],
+        ``conf`` [count][conf_size], ``coords`` [count][heavy][3], ``evals``."""
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        J = (LigandJob * len(jobs))(*jobs)
+        S = params.num_saved_mins
+        bufs = []
+        outs = (LigandResult * len(jobs))()
+        for k, j in enumerate(jobs):
+            m = models[j.model]
+            e = np.zeros(S)
+            conf = np.zeros((S, m.conf_size))
+            xyz = np.zeros((S, m.heavy, 3))
+            bufs.append((e, conf, xyz))
+            outs[k].e, outs[k].conf, outs[k].coords = dptr(e), dptr(conf), dptr(xyz)
+        self._check(load().sg_dock_batch32(self._h, rid, descs, len(models), J, len(jobs), C.byref(params),
+                                           1 if refine else 0, outs))
+        res = []
+        for k, (e, conf, xyz) in enumerate(bufs):
+            n = outs[k].count
+            res.append({"e": e[:n].copy(), "conf": conf[:n].copy(), "coords": xyz[:n].copy(), "evals": int(outs[k].evals)})
+        return res
+
+    def batch_stats(self):
+        """Timing and counters of the last dock_batch call."""
+        mc, rf = C.c_double(), C.c_double()
+        wpb, blocks = C.c_int(), C.c_int()
+        self._check(load().sg_batch_stats(self._h, C.byref(mc), C.byref(rf), C.byref(wpb), C.byref(blocks)))
+        ctr = [C.c_uint64() for _ in range(5)]
+        self._check(load().sg_batch_counters(self._h, *[C.byref(c) for c in ctr]))
+        return {"mc_ms": mc.value, "refine_ms": rf.value, "chains_per_block": wpb.value, "blocks": blocks.value,
+                "evals": ctr[0].value, "grid_lookups": ctr[1].value, "pair_lookups": ctr[2].value,
+                "h2d_bytes": ctr[3].value, "d2h_bytes": ctr[4].value}
+
+    def set_chains_per_block(self, n: int):
+        self._check(load().sg_set_chains_per_block(self._h, n))
 
     def close(self):
         if getattr(self, "_h", None):

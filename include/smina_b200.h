@@ -197,7 +197,8 @@ int sg_drop_receptor(sg_engine* e, int receptor_id);
 
 /* model::eval_deriv for nconfs confs of one model against receptor maps
  * (cache) of `receptor_id`.  out_e [nconfs], out_g [nconfs][dof],
- * out_coords [nconfs][num_movable][3] (may be NULL). */
+ * out_coords [nconfs][num_movable][3] (may be NULL).  FP32 engines run the
+ * mixed-precision evaluation the batched search uses. */
 int sg_eval(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs,
             const double* confs, const double v[3], double slope,
             double* out_e, double* out_g, double* out_coords);
@@ -228,6 +229,50 @@ int sg_refine(sg_engine* e, int receptor_id, const sg_model_desc* models, int nm
               const int* pose_model, int nposes, double* confs, const double cap[3],
               int maxiters, int accurate_line, int early_term,
               double* out_e, double* out_coords);
+
+/* ---- batched mixed-precision docking (virtual screening) ---------------
+ * Replaces GpuDocking::dock_batch (src/gpu/gpu_docking.h:91-94,
+ * gpu_docking.cpp:756): for every ligand job, its Monte Carlo chains,
+ * merge_output_containers with min_rmsd 2 (gpu_docking.cpp:576-599), then
+ * refine_structure of every pose in FP64 (main.cpp:165-200).  Needs an
+ * engine created with SG_PREC_FP32 or SG_PREC_FP32_H16. */
+typedef struct sg_ligand_job {
+    int model;           /* index into the models array                    */
+    int num_chains;      /* independent chains (exhaustiveness)            */
+    unsigned num_steps;  /* Monte Carlo steps per chain                    */
+    int maxiters;        /* BFGS iterations; 0: sg_mc_params.maxiters      */
+    uint64_t seed;       /* request seed (Philox key)                      */
+    uint64_t ligand_key; /* names the ligand's random streams: the same
+                            (seed, ligand_key) docks the same way alone or
+                            inside any batch                              */
+} sg_ligand_job;
+
+typedef struct sg_ligand_result {
+    int count;           /* poses written, <= num_saved_mins, by energy    */
+    double* e;           /* [num_saved_mins]                               */
+    double* conf;        /* [num_saved_mins][conf_size]                    */
+    double* coords;      /* [num_saved_mins][num_heavy_movable][3]         */
+    uint64_t evals;      /* eval_deriv calls of the search (all chains)    */
+} sg_ligand_result;
+
+/* refine: 0 skips refine_structure (poses come straight from the merge). */
+int sg_dock_batch32(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+                    const sg_ligand_job* jobs, int njobs, const sg_mc_params* p, int refine,
+                    sg_ligand_result* out);
+
+/* Timing and launch shape of the last sg_dock_batch32 call. */
+int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
+                   int* chains_per_block, int* blocks);
+
+/* Work counters of the last sg_dock_batch32 call: eval_deriv calls, grid
+ * map lookups (one packed cell each), in-cutoff pair table lookups, and
+ * bytes copied host to device and device to host. */
+int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookups,
+                      uint64_t* pair_lookups, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
+/* Chains (warps) per block of the search kernel: 1, 2 or 4, or 0 to pick
+ * the shape with the most resident chains per SM (the default). */
+int sg_set_chains_per_block(sg_engine* e, int n);
 
 #ifdef __cplusplus
 }
