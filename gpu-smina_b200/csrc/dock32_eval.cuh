@@ -16,7 +16,7 @@ constexpr unsigned kFull32 = 0xffffffffu;
 // Section timers (compile with -DSG_PROFILE): lane 0 of every warp adds
 // clock64() spans per section; sg_profile_read() copies them out.
 // Sections: 0 set_conf, 1 grid, 2 pairs, 3 derivative, 4 line-search
-// bookkeeping, 5 BFGS algebra, 7 whole chain.
+// bookkeeping, 5 BFGS algebra, 6 mutation, 7 whole chain.
 #ifdef SG_PROFILE
 __device__ unsigned long long g_prof[16];
 #define SG_T0(name) const long long name = clock64()
@@ -29,7 +29,6 @@ __device__ unsigned long long g_prof[16];
 
 // per-warp workspace (bytes, 16 B aligned)
 struct Ws32 {
-    int model;                                                   // DModel copy
     int coords, force, origin, axis, quat, rot;                  // float4 arrays (rot: 3 rows per frame)
     int x_tmp, x_cand, x_new, x_orig, g, g_new, g_orig, p, y, mhy, h;  // double arrays (h: n x n)
     int pf, pc;                                                  // prefix sums over atoms (float4)
@@ -40,7 +39,6 @@ SG_HD Ws32 ws32_layout(int natoms, int nframes, int conf, int dof) {
     Ws32 w;
     int o = 0;
     auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
-    w.model = take((int)sizeof(DModel));
     w.coords = take(16 * natoms);
     w.force = take(16 * natoms);
     w.origin = take(16 * nframes);
@@ -115,23 +113,8 @@ struct W32 {
     __device__ float4* rot() const { return (float4*)(s + L.rot); }
     __device__ double* d(int off) const { return (double*)(s + off); }
     __device__ float* scratch() const { return (float*)(s + L.scratch); }
-    // stage the chain's model descriptor in this warp's shared memory
-    __device__ void bind_model(const DModel* gm) {
-        const int4* src = (const int4*)gm;
-        int4* dst = (int4*)(s + L.model);
-        for (int i = lane; i < (int)(sizeof(DModel) / 16); i += 32) dst[i] = src[i];
-        __syncwarp();
-        m = (const DModel*)(s + L.model);
-    }
 };
 static_assert(sizeof(DModel) % 16 == 0, "DModel is copied in 16 byte pieces");
-
-// fire-and-forget add into this warp's shared workspace (shared state
-// space: no generic-address round trip, no return value)
-__device__ __forceinline__ void red_shared(float* p, float v) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
-}
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -204,16 +187,16 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
         float3 t = make_float3(0, 0, 0);
         int anc = -1, parent = -1, kind = 0;
         if (act) {
-            kind = __ldg(m.fkind + f);
-            const int ci = __ldg(m.fconf + f);
+            kind = m.fkind[f];
+            const int ci = m.fconf[f];
             if (kind == SG_FRAME_RIGID) {
                 const double* c = conf + ci;
                 t = make_float3((float)c[0], (float)c[1], (float)c[2]);
                 q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
             } else {
-                if (kind == SG_FRAME_SEGMENT) parent = anc = __ldg(m.fparent + f);
-                t = f3(__ldg(m.forigin32 + f));
-                q = axis_angle32(f3(__ldg(m.faxis32 + f)), (float)conf[ci]);
+                if (kind == SG_FRAME_SEGMENT) parent = anc = m.fparent[f];
+                t = f3(m.forigin32[f]);
+                q = axis_angle32(f3(m.faxis32[f]), (float)conf[ci]);
             }
         }
         for (int it = 0; it < 6 && __any_sync(kFull32, anc >= 0); it++) {
@@ -240,10 +223,10 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
             Q[f] = q;
             quat_rows(q, R + 3 * f);
             if (kind == SG_FRAME_SEGMENT) {
-                const float3 ax = qrot(pq, f3(__ldg(m.faxis32 + f)));
+                const float3 ax = qrot(pq, f3(m.faxis32[f]));
                 A[f] = make_float4(ax.x, ax.y, ax.z, 0);
             } else if (kind == SG_FRAME_FIRST_SEGMENT) {
-                A[f] = __ldg(m.faxis32 + f);
+                A[f] = m.faxis32[f];
             }
         }
         __syncwarp();
@@ -251,24 +234,24 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
         for (int lv = 0; lv < m.nlevels; lv++) {
             for (int idx = m.level_start[lv] + w.lane; idx < m.level_start[lv + 1]; idx += 32) {
                 const int f = __ldg(m.level_frames + idx);
-                const int kind = __ldg(m.fkind + f);
+                const int kind = m.fkind[f];
                 float4 q;
                 if (kind == SG_FRAME_RIGID) {
-                    const double* c = conf + __ldg(m.fconf + f);
+                    const double* c = conf + m.fconf[f];
                     O[f] = make_float4((float)c[0], (float)c[1], (float)c[2], 0);
                     q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
                 } else if (kind == SG_FRAME_SEGMENT) {
-                    const int p = __ldg(m.fparent + f);
-                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(__ldg(m.forigin32 + f)));
-                    const float3 ax = rot_apply(R + 3 * p, f3(__ldg(m.faxis32 + f)));
+                    const int p = m.fparent[f];
+                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(m.forigin32[f]));
+                    const float3 ax = rot_apply(R + 3 * p, f3(m.faxis32[f]));
                     O[f] = make_float4(o.x, o.y, o.z, 0);
                     A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[__ldg(m.fconf + f)]), Q[p]));
+                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[m.fconf[f]]), Q[p]));
                 } else {
-                    const float3 ax = f3(__ldg(m.faxis32 + f));
-                    O[f] = __ldg(m.forigin32 + f);
+                    const float3 ax = f3(m.faxis32[f]);
+                    O[f] = m.forigin32[f];
                     A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = axis_angle32(ax, (float)conf[__ldg(m.fconf + f)]);
+                    q = axis_angle32(ax, (float)conf[m.fconf[f]]);
                 }
                 Q[f] = q;
                 quat_rows(q, R + 3 * f);
@@ -278,8 +261,8 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
     }
     float4* X = w.coords();
     for (int i = w.lane; i < m.nmov; i += 32) {
-        const int f = __ldg(m.atom_frame + i);
-        const float3 c = f3(O[f]) + rot_apply(R + 3 * f, f3(__ldg(m.local32 + i)));
+        const int f = m.atom_frame[i];
+        const float3 c = f3(O[f]) + rot_apply(R + 3 * f, f3(m.local32[i]));
         X[i] = make_float4(c.x, c.y, c.z, 0);
     }
     __syncwarp();
@@ -333,9 +316,9 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
 }
 
 // table lookup with charge-weighted components (precalculate_linear element eval_deriv)
-__device__ __forceinline__ void table32_nc(const DTables32& T, int tp, float qa, float qb, float r2, float& e, float& dor) {
-    const int p = tp & 0x1fffffff;
-    if (tp & (1 << 30)) { const float t = qa; qa = qb; qb = t; }
+__device__ __forceinline__ void table32_nc(const DTables32& T, int p, bool swap, float qa, float qb, float r2, float& e,
+                                           float& dor) {
+    if (swap) { const float t = qa; qa = qb; qb = t; }
     const float rf = T.factor * r2;
     const int i1 = (int)rf;
     const float rem = rf - (float)i1;
@@ -359,14 +342,16 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     float4* Fz = w.force();
     float e = 0;
     // grid part; every movable atom gets its force reset (hydrogens: zero)
-    for (int i = w.lane; i < m.nmov; i += 32) {
-        const int t = __ldg(m.type + i);
+    const int nmov = m.nmov;
+    const int* __restrict__ TYPE = m.type;
+    for (int i = w.lane; i < nmov; i += 32) {
+        const int t = TYPE[i];
         float3 d = make_float3(0, 0, 0);
         if (t < kNumTypes && !is_h(t)) {
             const float3 loc = f3(X[i]);
             e += grid_aux32(*w.G, t, false, loc, slope, v[1], d);
             w.grid_hits++;
-            const float q = __ldg(m.local32 + i).w;
+            const float q = m.local32[i].w;
             if (q != 0.f && w.G->c32[t]) {
                 float3 cd;
                 e += q * grid_aux32(*w.G, t, true, loc, slope, v[1], cd);
@@ -379,59 +364,83 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     __syncwarp();
     SG_T1(t_grid, 1);
     SG_T0(t_pairs);
-    // pairs: intramolecular (v[0]) and other (v[2]); two pairs per lane in flight
-    const int P = m.npairs;
-    const float cut2 = w.T->cutoff_sqr;
-    for (int base = 0; base < P; base += 64) {
-        int2 ab[2];
-        int tp[2];
+    // Pairs: intramolecular (v[0]) and other (v[2]), two chunks of 32 in
+    // flight.  Within a chunk no atom is twice a first atom or twice a
+    // second atom, so the force updates are plain read-add-writes: first
+    // atoms, sync, second atoms, sync.
+    const int nch = m.npchunks;
+    const uint32_t* PS = m.pslot;
+    const float4* LQ = m.local32;
+    const DTables32 T = *w.T;
+    const int lane = w.lane;
+    unsigned long long hits = 0;
+    for (int c = 0; c < nch; c += 2) {
+        const bool two = c + 1 < nch;
+        uint32_t sl[2];
+        int ia[2], ib[2];
         float3 r[2];
         float r2[2];
         bool ok[2];
 #pragma unroll
         for (int u = 0; u < 2; u++) {
-            const int k = base + 32 * u + w.lane;
-            ok[u] = k < P;
-            ab[u] = ok[u] ? __ldg(m.pairs32 + k) : make_int2(0, 0);
-            tp[u] = ok[u] ? __ldg(m.tp32 + k) : 0;
-            r[u] = f3(X[ab[u].y]) - f3(X[ab[u].x]);
+            sl[u] = (u == 0 || two) ? PS[(c + u) * 32 + lane] : kSlotEmpty;
+            ia[u] = sl[u] & 0xff;
+            ib[u] = (sl[u] >> 8) & 0xff;
+            r[u] = f3(X[ib[u]]) - f3(X[ia[u]]);
             r2[u] = dot3(r[u], r[u]);
-            ok[u] = ok[u] && r2[u] < cut2;
+            ok[u] = sl[u] != kSlotEmpty && r2[u] < T.cutoff_sqr;
         }
         float4 tv[2];
         float rem[2];
-        if (w.T->nc == 1) {  // issue both table loads before using either
+        if (T.nc == 1) {  // issue both table loads before using either
 #pragma unroll
             for (int u = 0; u < 2; u++) {
-                const float rf = w.T->factor * r2[u];
+                const float rf = T.factor * r2[u];
                 const int i1 = ok[u] ? (int)rf : 0;
                 rem[u] = rf - (float)i1;
-                tv[u] = ok[u] ? __ldg(w.T->tab + ((size_t)(tp[u] & 0x1fffffff) * w.T->n + i1)) : make_float4(0, 0, 0, 0);
+                tv[u] = ok[u] ? __ldg(T.tab + ((size_t)((sl[u] >> 16) & 0x1ff) * T.n + i1)) : make_float4(0, 0, 0, 0);
             }
         }
+        float3 f[2];
 #pragma unroll
         for (int u = 0; u < 2; u++) {
+            f[u] = make_float3(0, 0, 0);
             if (!ok[u]) continue;
             float pe, dor;
-            if (w.T->nc == 1) {
+            if (T.nc == 1) {
                 pe = tv[u].x + rem[u] * (tv[u].z - tv[u].x);
                 dor = tv[u].y + rem[u] * (tv[u].w - tv[u].y);
             } else {
-                table32_nc(*w.T, tp[u], __ldg(m.local32 + ab[u].x).w, __ldg(m.local32 + ab[u].y).w, r2[u], pe, dor);
+                table32_nc(T, (sl[u] >> 16) & 0x1ff, (sl[u] & kSlotSwap) != 0, LQ[ia[u]].w, LQ[ib[u]].w, r2[u], pe, dor);
             }
-            float3 f = dor * r[u];
-            const float vv = (tp[u] & (1 << 29)) ? v[0] : v[2];
+            f[u] = dor * r[u];
+            const float vv = (sl[u] & kSlotIntra) ? v[0] : v[2];
             if (pe > 0) {
                 const float tt = (vv < 1.1920929e-07f) ? 0.f : (vv / (vv + pe));
                 pe *= tt;
-                f = (tt * tt) * f;
+                f[u] = (tt * tt) * f[u];
             }
             e += pe;
-            w.pair_hits++;
-            red_shared(&Fz[ab[u].x].x, -f.x); red_shared(&Fz[ab[u].x].y, -f.y); red_shared(&Fz[ab[u].x].z, -f.z);
-            red_shared(&Fz[ab[u].y].x, f.x); red_shared(&Fz[ab[u].y].y, f.y); red_shared(&Fz[ab[u].y].z, f.z);
+            hits++;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            if (u == 1 && !two) break;
+            if (ok[u]) {
+                float4 t = Fz[ia[u]];
+                t.x -= f[u].x; t.y -= f[u].y; t.z -= f[u].z;
+                Fz[ia[u]] = t;
+            }
+            __syncwarp();
+            if (ok[u]) {
+                float4 t = Fz[ib[u]];
+                t.x += f[u].x; t.y += f[u].y; t.z += f[u].z;
+                Fz[ib[u]] = t;
+            }
+            __syncwarp();
         }
     }
+    w.pair_hits += hits;
     e = warp_sum(e);
     __syncwarp();
     SG_T1(t_pairs, 2);
@@ -478,11 +487,11 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     }
     __syncwarp();
     for (int f = w.lane; f < m.nframes; f += 32) {
-        const int b = __ldg(m.fbegin + f), E = __ldg(m.fsub_end + f);
+        const int b = m.fbegin[f], E = m.fsub_end[f];
         const float3 F = f3(PF[E]) - f3(PF[b]);
         const float3 T = (f3(PC[E]) - f3(PC[b])) - cross3(f3(O[f]) - oref, F);
-        const int dof0 = __ldg(m.fdof + f);
-        if (__ldg(m.fkind + f) == SG_FRAME_RIGID) {
+        const int dof0 = m.fdof[f];
+        if (m.fkind[f] == SG_FRAME_RIGID) {
             g[dof0] = F.x; g[dof0 + 1] = F.y; g[dof0 + 2] = F.z;
             g[dof0 + 3] = T.x; g[dof0 + 4] = T.y; g[dof0 + 5] = T.z;
         } else {

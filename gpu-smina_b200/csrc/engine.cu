@@ -12,8 +12,6 @@
 
 namespace sg {
 
-
-
 void DevBuf::reset() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -525,28 +523,41 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
                         "model: a subtree's atoms must follow its root frame's atoms contiguously");
         pv(sub_end);
     }
-    {   // mixed-precision pair order: round robin over first-atom groups, curl group in bit 29
-        std::vector<std::vector<int>> groups;
-        std::vector<int> gid(N, -1);
-        for (int k = 0; k < P; k++) {
-            const int a = d.pairs[2 * k];
-            if (gid[a] < 0) { gid[a] = (int)groups.size(); groups.emplace_back(); }
-            groups[gid[a]].push_back(k);
+    {   // Mixed-precision pair schedule: chunks of 32 slots in which no atom is
+        // the first atom of two pairs and none is the second atom of two pairs,
+        // so one warp adds a chunk's forces without atomics (first atoms, then
+        // second atoms).  A pair may be stored either way round: swapping the
+        // atoms toggles the charge-role bit.
+        std::vector<std::vector<char>> out_used, in_used;
+        std::vector<std::vector<uint32_t>> slots;
+        const bool packable = M <= 255;
+        for (int k = 0; k < P && packable; k++) {
+            const int u = d.pairs[2 * k], v = d.pairs[2 * k + 1];
+            require(u >= 0 && v >= 0 && u < M && v < M && u != v, "model: pair atoms must be distinct movable atoms");
+            const uint32_t base = ((uint32_t)(pair_tp[k] & 0x1ff) << 16) | ((pair_tp[k] >> 30) & 1 ? kSlotSwap : 0) |
+                                  (k >= d.num_other_pairs ? kSlotIntra : 0);
+            size_t c = 0;
+            uint32_t slot = 0;
+            for (; c < slots.size(); c++) {
+                if (slots[c].size() >= 32) continue;
+                if (!out_used[c][u] && !in_used[c][v]) { slot = base | u | (v << 8); break; }
+                if (!out_used[c][v] && !in_used[c][u]) { slot = (base ^ kSlotSwap) | v | (u << 8); break; }
+            }
+            if (c == slots.size()) {
+                out_used.emplace_back(M, 0);
+                in_used.emplace_back(M, 0);
+                slots.emplace_back();
+                slot = base | u | (v << 8);
+            }
+            out_used[c][slot & 0xff] = 1;
+            in_used[c][(slot >> 8) & 0xff] = 1;
+            slots[c].push_back(slot);
         }
-        std::vector<int> p32, t32;
-        size_t maxg = 0;
-        for (auto& g : groups) maxg = std::max(maxg, g.size());
-        for (size_t r = 0; r < maxg; r++)
-            for (auto& g : groups)
-                if (r < g.size()) {
-                    const int k = g[r];
-                    p32.push_back(d.pairs[2 * k]);
-                    p32.push_back(d.pairs[2 * k + 1]);
-                    t32.push_back(pair_tp[k] | (k >= d.num_other_pairs ? (1 << 29) : 0));
-                }
-        if (I.size() & 1) I.push_back(0);  // read as int2
-        pv(p32);
-        pv(t32);
+        std::vector<int> ps;
+        for (auto& c : slots)
+            for (int l = 0; l < 32; l++) ps.push_back((int)(l < (int)c.size() ? c[l] : kSlotEmpty));
+        hm.npchunks = packable ? (int)slots.size() : -1;
+        pv(ps);
     }
     auto pf4 = [&](const double* xyz, const double* w4, size_t n) {
         foff.push_back(Fl.size());
@@ -598,8 +609,8 @@ void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedM
         h.tor_conf = ib + io[j++]; h.tor_dof = ib + io[j++]; h.tor_frame = ib + io[j++];
         h.pair_tp = ib + io[j++];
         h.fsub_end = ib + io[j++];
-        h.pairs32 = (const int2*)(ib + io[j++]);
-        h.tp32 = ib + io[j++];
+        h.pslot = h.npchunks >= 0 ? (const uint32_t*)(ib + io[j]) : nullptr;
+        j++;
         const std::vector<size_t>& fo = foffs[k];
         h.local32 = (const float4*)(fb + fo[0]); h.lab32 = (const float4*)(fb + fo[1]);
         h.forigin32 = (const float4*)(fb + fo[2]); h.faxis32 = (const float4*)(fb + fo[3]);
@@ -667,6 +678,7 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
         dg.make((size_t)nconfs * h.dof, e->stream);
         if (out_coords) dx.make((size_t)nconfs * h.nmov * 3, e->stream);
         if (!direct && e->precision != SG_PREC_FP64) {  // the mixed-precision evaluation
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
             const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
             require(ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
             cuda_check(launch_eval32(pm.dmodels.as<DModel>(), ws, tables32(e), maps32(e, r), nconfs, dc.p(), v, slope,

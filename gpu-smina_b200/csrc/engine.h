@@ -129,9 +129,10 @@ cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*,
 cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
                             const double[3], int, const int*, int, int, double*, double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
-int mc32_occupancy(int wpb, size_t ws_stride);
-cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const Chain32*, int, const MCParams32&, unsigned*,
-                        int blocks, int wpb, size_t ws_stride, cudaStream_t);
+int mc32_occupancy(int wpb, size_t smem);
+cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const Chain32*, const Item32*, int nitems,
+                        const MCParams32&, unsigned*, int blocks, int wpb, size_t stage_stride, size_t ws_stride,
+                        cudaStream_t);
 cudaError_t launch_eval32(const DModel*, size_t, const DTables32&, const DMaps32&, int, const double*, const double[3],
                           double, double*, double*, double*, cudaStream_t);
 

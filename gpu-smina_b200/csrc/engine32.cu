@@ -82,20 +82,27 @@ static void add_pose(std::vector<HostPose>& out, HostPose&& t, double min_rmsd, 
     std::stable_sort(out.begin(), out.end(), [](const HostPose& a, const HostPose& b) { return a.e < b.e; });
 }
 
-// launch shape: chains (warps) per block with the most resident chains per SM
-static void choose_launch(sg_engine* e, size_t ws_stride, int nchains, int& wpb, int& blocks) {
-    const int cands[3] = {4, 2, 1};
+// launch shape: chains (warps) per block with the most resident chains per
+// SM (ties: more chains per block, so fewer model copies)
+static void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ) {
+    const int cands[4] = {8, 4, 2, 1};
     int best_w = 0, best_occ = 0, best_res = 0;
     for (int c : cands) {
         if (e->force_wpb && c != e->force_wpb) continue;
-        const int occ = mc32_occupancy(c, ws_stride);
-        if (occ * c > best_res) { best_res = occ * c; best_w = c; best_occ = occ; }
+        if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;  // half the warps would idle
+        const size_t smem = stage_stride + (size_t)c * ws_stride;
+        if (smem > (size_t)e->max_smem) continue;
+        const int o = mc32_occupancy(c, smem);
+        if (o * c > best_res) { best_res = o * c; best_w = c; best_occ = o; }
     }
     require(best_res > 0, "model too large for the mixed-precision path's shared memory");
     wpb = best_w;
-    const long long need = (nchains + wpb - 1) / wpb;
-    blocks = (int)std::min<long long>((long long)best_occ * e->num_sms, need);
+    occ = best_occ;
 }
+
+#ifdef SG_PROFILE
+cudaError_t profile_read32(unsigned long long* out16, bool clear);
+#endif
 
 }  // namespace sg
 
@@ -117,8 +124,13 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         ensure_model_maps(e, r, pm, models, nmodels);
         check_packed(e, r, models, nmodels);
         uint64_t h2d = pm.ints.bytes + pm.flts.bytes + pm.dbls.bytes + pm.dmodels.bytes, d2h = 0;
-        size_t ws_stride = 0;
-        for (const DModel& h : pm.host) ws_stride = std::max(ws_stride, ws32_bytes(h));
+        size_t ws_stride = 0, stage_stride = 0;
+        for (const DModel& h : pm.host) {
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
+            ws_stride = std::max(ws_stride, ws32_bytes(h));
+            stage_stride = std::max(stage_stride, (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks,
+                                                                        h.nlig, h.nblocks, h.ntors));
+        }
         ws_stride = (ws_stride + 15) & ~(size_t)15;
         const int S = p->num_saved_mins;
         // chains of every job, with their result slots
@@ -171,18 +183,33 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             ch.evals = d_evals.as<unsigned long long>() + k;
             ch.hits = d_hits.as<unsigned long long>() + 2 * k;
         }
-        // longest first, so the persistent kernel's queue ends evenly
-        std::vector<int> order(nchains);
+        // work items: up to wpb chains of one job; longest first, so the
+        // persistent kernel's queue ends evenly
+        int max_chains = 1;
+        for (int j = 0; j < njobs; j++) max_chains = std::max(max_chains, jobs[j].num_chains);
+        int wpb = 1, occ = 1;
+        choose_launch(e, stage_stride, ws_stride, max_chains, wpb, occ);
+        std::vector<Item32> items;
+        std::vector<double> item_cost;
+        for (int k = 0; k < nchains;) {
+            const int j = chain_job[k];
+            int n = 0;
+            while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
+            items.push_back(Item32{hc[k].model, k, n});
+            item_cost.push_back((double)hc[k].steps * pm.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
+            k += n;
+        }
+        std::vector<int> order(items.size());
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-            return (double)hc[a].steps * pm.host[hc[a].model].cost * std::max(1, hc[a].maxiters) >
-                   (double)hc[b].steps * pm.host[hc[b].model].cost * std::max(1, hc[b].maxiters);
-        });
-        std::vector<Chain32> queue(nchains);
-        for (int k = 0; k < nchains; k++) queue[k] = hc[order[k]];
-        DevBuf d_chains;
-        d_chains.upload(queue.data(), queue.size() * sizeof(Chain32), e->stream);
-        h2d += d_chains.bytes;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_cost[a] > item_cost[b]; });
+        std::vector<Item32> queue(items.size());
+        for (size_t k = 0; k < items.size(); k++) queue[k] = items[order[k]];
+        const int nitems = (int)queue.size();
+        const int blocks = (int)std::min<long long>((long long)occ * e->num_sms, nitems);
+        DevBuf d_chains, d_items;
+        d_chains.upload(hc.data(), hc.size() * sizeof(Chain32), e->stream);
+        d_items.upload(queue.data(), queue.size() * sizeof(Item32), e->stream);
+        h2d += d_chains.bytes + d_items.bytes;
         MCParams32 P{};
         for (int i = 0; i < 3; i++) {
             P.hunt[i] = (float)p->hunt_cap[i];
@@ -198,8 +225,6 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         P.maxiters = p->maxiters;
         P.accurate_line = p->accurate_line;
         P.early_term = p->early_term;
-        int wpb = 1, blocks = 1;
-        choose_launch(e, ws_stride, nchains, wpb, blocks);
         cudaEvent_t ev[4];
         for (auto& x : ev) cuda_check(cudaEventCreate(&x), "event");
         struct EvGuard {
@@ -207,8 +232,9 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(v[i]); }
         } evg{ev};
         cuda_check(cudaEventRecord(ev[0], e->stream), "event");
-        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), d_chains.as<Chain32>(), nchains, P,
-                               d_queue.as<unsigned>(), blocks, wpb, ws_stride, e->stream),
+        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), d_chains.as<Chain32>(),
+                               d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb, stage_stride,
+                               ws_stride, e->stream),
                    "search launch");
         cuda_check(cudaEventRecord(ev[1], e->stream), "event");
         std::vector<double> he((size_t)nchains * S), hconf(nconf_res);
@@ -348,8 +374,15 @@ int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookup
     return SG_OK;
 }
 
+#ifdef SG_PROFILE
+// profiling builds only: clock64() cycles per section summed over warps
+int sg_profile_read(unsigned long long* out16, int clear) {
+    return profile_read32(out16, clear != 0) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
+}
+#endif
+
 int sg_set_chains_per_block(sg_engine* e, int n) {
-    if (!e || !(n == 0 || n == 1 || n == 2 || n == 4)) return SG_ERR_ARG;
+    if (!e || !(n == 0 || n == 1 || n == 2 || n == 4 || n == 8)) return SG_ERR_ARG;
     e->force_wpb = n;
     return SG_OK;
 }

@@ -56,15 +56,15 @@ __device__ void q_increment32(double* c, double rx, double ry, double rz) {
 __device__ void increment32(const W32& w, double* x, const double* p, double alpha) {
     const DModel& m = *w.m;
     for (int l = w.lane; l < m.nlig; l += 32) {
-        const int f = __ldg(m.lig_root + l);
-        double* c = x + __ldg(m.fconf + f);
-        const double* d = p + __ldg(m.fdof + f);
+        const int f = m.lig_root[l];
+        double* c = x + m.fconf[f];
+        const double* d = p + m.fdof[f];
         c[0] += alpha * d[0]; c[1] += alpha * d[1]; c[2] += alpha * d[2];
         q_increment32(c + 3, alpha * d[3], alpha * d[4], alpha * d[5]);
     }
     for (int k = w.lane; k < m.ntors; k += 32) {
-        double& t = x[__ldg(m.tor_conf + k)];
-        t += normalized_angle(alpha * p[__ldg(m.tor_dof + k)]);
+        double& t = x[m.tor_conf[k]];
+        t += normalized_angle(alpha * p[m.tor_dof[k]]);
         normalize_angle(t);
     }
     __syncwarp();
@@ -73,18 +73,18 @@ __device__ void increment32(const W32& w, double* x, const double* p, double alp
 // conf::operator()(index): value of change coordinate i (accurate line search)
 __device__ double conf_value32(const DModel& m, const double* x, int i) {
     for (int l = 0; l < m.nlig; l++) {
-        const int f = __ldg(m.lig_root + l);
-        const int d0 = __ldg(m.fdof + f);
-        if (i >= d0 && i < d0 + 3) return x[__ldg(m.fconf + f) + (i - d0)];
+        const int f = m.lig_root[l];
+        const int d0 = m.fdof[f];
+        if (i >= d0 && i < d0 + 3) return x[m.fconf[f] + (i - d0)];
         if (i >= d0 + 3 && i < d0 + 6) {
-            const double* c = x + __ldg(m.fconf + f);
+            const double* c = x + m.fconf[f];
             const V3<double> a = q_to_angle(Quat<double>{c[3], c[4], c[5], c[6]});
             const int j = i - d0 - 3;
             return j == 0 ? a.x : j == 1 ? a.y : a.z;
         }
     }
     for (int k = 0; k < m.ntors; k++)
-        if (__ldg(m.tor_dof + k) == i) return x[__ldg(m.tor_conf + k)];
+        if (m.tor_dof[k] == i) return x[m.tor_conf[k]];
     return 0;
 }
 
@@ -104,8 +104,10 @@ __device__ double line_fast32(W32& w, const double* x, const double* g, double f
     double alpha = 1;
     const double pg = dotd(w, p, g, m.dof);
     for (unsigned trial = 0; trial < 10; trial++) {
+        SG_T0(t_ls);
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
+        SG_T1(t_ls, 4);
         f1 = feval32(w, x_new, g_new, em);
         if (f1 - f0 < 0.0001 * alpha * pg) break;
         alpha *= 0.5;
@@ -252,11 +254,11 @@ __device__ V3<double> sphere32(Philox& rng) {  // random_inside_sphere, bounded 
 // gyration radius of ligand l's heavy atoms about its root origin (current coords)
 __device__ double gyration32(const W32& w, int l) {
     const DModel& m = *w.m;
-    const float3 o = f3(w.origin()[__ldg(m.lig_root + l)]);
+    const float3 o = f3(w.origin()[m.lig_root[l]]);
     float acc = 0;
     int cnt = 0;
-    for (int i = __ldg(m.lig_begin + l) + w.lane; i < __ldg(m.lig_end + l); i += 32)
-        if (!is_h(__ldg(m.type + i))) {
+    for (int i = m.lig_begin[l] + w.lane; i < m.lig_end[l]; i += 32)
+        if (!is_h(m.type[i])) {
             const float3 d = f3(w.coords()[i]) - o;
             acc += dot3(d, d);
             cnt++;
@@ -269,13 +271,13 @@ __device__ double gyration32(const W32& w, int l) {
 __device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude) {
     const DModel& m = *w.m;
     int num = 0;
-    for (int b = 0; b < m.nblocks; b++) num += (__ldg(m.blk_rigid + b) ? 2 : 0) + __ldg(m.blk_ntors + b);
+    for (int b = 0; b < m.nblocks; b++) num += (m.blk_rigid[b] ? 2 : 0) + m.blk_ntors[b];
     if (num == 0) return;
     int which = ph_int(rng, num);
     int lig = 0;
     for (int b = 0; b < m.nblocks; b++) {
-        double* c = x + __ldg(m.blk_conf + b);
-        if (__ldg(m.blk_rigid + b)) {
+        double* c = x + m.blk_conf[b];
+        if (m.blk_rigid[b]) {
             if (which == 0) {
                 const V3<double> d = amplitude * sphere32(rng);
                 if (w.lane == 0) { c[0] += d.x; c[1] += d.y; c[2] += d.z; }
@@ -296,7 +298,7 @@ __device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude)
             c += 7;
             lig++;
         }
-        const int nt = __ldg(m.blk_ntors + b);
+        const int nt = m.blk_ntors[b];
         if (which < nt) {
             const double t = ph_range(rng, -kPi, kPi);
             if (w.lane == 0) c[which] = t;
@@ -312,8 +314,8 @@ __device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude)
 __device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams32& P) {
     const DModel& m = *w.m;
     for (int b = 0; b < m.nblocks; b++) {
-        double* c = x + __ldg(m.blk_conf + b);
-        if (__ldg(m.blk_rigid + b)) {
+        double* c = x + m.blk_conf[b];
+        if (m.blk_rigid[b]) {
             double v[7];
             for (int k = 0; k < 3; k++) v[k] = ph_range(rng, P.box_lo[k], P.box_hi[k]);
             double q[4], nq = 0;
@@ -324,7 +326,7 @@ __device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams
             if (w.lane == 0) for (int k = 0; k < 7; k++) c[k] = v[k];
             c += 7;
         }
-        const int nt = __ldg(m.blk_ntors + b);
+        const int nt = m.blk_ntors[b];
         for (int t = 0; t < nt; t++) {
             const double a = ph_range(rng, -kPi, kPi);
             if (w.lane == 0) c[t] = a;
@@ -347,7 +349,7 @@ __device__ int add_output32(const W32& w, const Chain32& ch, const double* x, do
         const float* oc = ch.out_coords + (size_t)ch.out_order[j] * H * 3;
         float acc = 0;
         for (int a = w.lane; a < H; a += 32) {
-            const float3 c = f3(X[__ldg(m.heavy + a)]);
+            const float3 c = f3(X[m.heavy[a]]);
             const float dx = c.x - oc[3 * a], dy = c.y - oc[3 * a + 1], dz = c.z - oc[3 * a + 2];
             acc += dx * dx + dy * dy + dz * dz;
         }
@@ -369,7 +371,7 @@ __device__ int add_output32(const W32& w, const Chain32& ch, const double* x, do
     if (target >= 0) {
         for (int i = w.lane; i < cs; i += 32) ch.out_conf[(size_t)target * cs + i] = x[i];
         for (int a = w.lane; a < H; a += 32) {
-            const float3 c = f3(X[__ldg(m.heavy + a)]);
+            const float3 c = f3(X[m.heavy[a]]);
             float* o = ch.out_coords + ((size_t)target * H + a) * 3;
             o[0] = c.x; o[1] = c.y; o[2] = c.z;
         }
@@ -409,8 +411,10 @@ __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCPara
     int count = 0;
     if (w.lane == 0) *ch.out_count = 0;
     for (unsigned step = 0; step < ch.steps; step++) {
+        SG_T0(t_mut);
         copyd(w, cand, tmp, cs);
         mutate32(w, rng, cand, P.amplitude);
+        SG_T1(t_mut, 6);
         const double cand_e = bfgs32(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt);
         bool accept = step == 0 || cand_e < tmp_e;
         if (!accept) accept = ph_u01(rng) < exp((tmp_e - cand_e) / P.temperature);
@@ -440,32 +444,99 @@ __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCPara
     SG_T1(t_chain, 7);
 }
 
-// Persistent search kernel: warps pull chains from *queue until it runs out.
-__global__ void __launch_bounds__(128, 4) k_mc32(const DModel* models, DTables32 T, DMaps32 G, const Chain32* chains,
-                                                 int nchains, MCParams32 P, unsigned* queue, int ws_stride) {
+// Copies a model's descriptor and the arrays the search reads into the
+// block's shared memory; every thread of the block takes part.  Arrays that
+// are read once per chain (lab32, finit32) or only for trees of more than
+// 32 frames (levels) stay in global memory.
+template <typename T>
+__device__ __forceinline__ const T* stage_arr(const T* src, int n, char*& o, int tid, int nthr) {
+    T* d = reinterpret_cast<T*>(o);
+    o += (n * (int)sizeof(T) + 15) & ~15;
+    for (int i = tid; i < n; i += nthr) d[i] = src[i];
+    return d;
+}
+
+__device__ void stage_model(const DModel* gm, char* dst, int tid, int nthr) {
+    const int4* src = reinterpret_cast<const int4*>(gm);
+    for (int i = tid; i < (int)(sizeof(DModel) / 16); i += nthr) reinterpret_cast<int4*>(dst)[i] = src[i];
+    const DModel g = *gm;
+    char* o = dst + (((int)sizeof(DModel) + 15) & ~15);
+    DModel* d = reinterpret_cast<DModel*>(dst);
+    const float4* local32 = stage_arr(g.local32, g.natoms, o, tid, nthr);
+    const int* type = stage_arr(g.type, g.natoms, o, tid, nthr);
+    const int* atom_frame = stage_arr(g.atom_frame, g.natoms, o, tid, nthr);
+    const float4* forigin32 = stage_arr(g.forigin32, g.nframes, o, tid, nthr);
+    const float4* faxis32 = stage_arr(g.faxis32, g.nframes, o, tid, nthr);
+    const int* fkind = stage_arr(g.fkind, g.nframes, o, tid, nthr);
+    const int* fparent = stage_arr(g.fparent, g.nframes, o, tid, nthr);
+    const int* fbegin = stage_arr(g.fbegin, g.nframes, o, tid, nthr);
+    const int* fsub_end = stage_arr(g.fsub_end, g.nframes, o, tid, nthr);
+    const int* fconf = stage_arr(g.fconf, g.nframes, o, tid, nthr);
+    const int* fdof = stage_arr(g.fdof, g.nframes, o, tid, nthr);
+    const int* heavy = stage_arr(g.heavy, g.nheavy, o, tid, nthr);
+    const uint32_t* pslot = stage_arr(g.pslot, 32 * g.npchunks, o, tid, nthr);
+    const int* lig_root = stage_arr(g.lig_root, g.nlig, o, tid, nthr);
+    const int* lig_begin = stage_arr(g.lig_begin, g.nlig, o, tid, nthr);
+    const int* lig_end = stage_arr(g.lig_end, g.nlig, o, tid, nthr);
+    const int* blk_rigid = stage_arr(g.blk_rigid, g.nblocks, o, tid, nthr);
+    const int* blk_conf = stage_arr(g.blk_conf, g.nblocks, o, tid, nthr);
+    const int* blk_ntors = stage_arr(g.blk_ntors, g.nblocks, o, tid, nthr);
+    const int* tor_conf = stage_arr(g.tor_conf, g.ntors, o, tid, nthr);
+    const int* tor_dof = stage_arr(g.tor_dof, g.ntors, o, tid, nthr);
+    __syncthreads();  // descriptor copied
+    if (tid == 0) {
+        d->local32 = local32; d->type = type; d->atom_frame = atom_frame;
+        d->forigin32 = forigin32; d->faxis32 = faxis32;
+        d->fkind = fkind; d->fparent = fparent; d->fbegin = fbegin; d->fsub_end = fsub_end;
+        d->fconf = fconf; d->fdof = fdof; d->heavy = heavy; d->pslot = pslot;
+        d->lig_root = lig_root; d->lig_begin = lig_begin; d->lig_end = lig_end;
+        d->blk_rigid = blk_rigid; d->blk_conf = blk_conf; d->blk_ntors = blk_ntors;
+        d->tor_conf = tor_conf; d->tor_dof = tor_dof;
+    }
+    __syncthreads();
+}
+
+// Persistent search kernel.  A block takes work items (a group of chains
+// of one ligand, longest first) from *queue, stages the ligand's model in
+// shared memory once for all its warps, and runs one chain per warp.
+// SG_MC32_MINB resident 256-thread blocks per SM bound the registers
+// (2: 128 per thread).
+#ifndef SG_MC32_MINB
+#define SG_MC32_MINB 2
+#endif
+__global__ void __launch_bounds__(256, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
+                                                            const Chain32* chains, const Item32* items, int nitems,
+                                                            MCParams32 P, unsigned* queue, int stage_stride,
+                                                            int ws_stride) {
     __shared__ DTables32 sT;
     __shared__ DMaps32 sG;
+    __shared__ int s_item;
     extern __shared__ __align__(16) char smem32[];
-    if (threadIdx.x == 0) { sT = T; sG = G; }
-    __syncthreads();
+    const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
+    if (tid == 0) { sT = T; sG = G; }
     W32 w;
-    w.s = smem32 + (size_t)(threadIdx.x >> 5) * ws_stride;
+    w.s = smem32 + stage_stride + (size_t)warp * ws_stride;
     w.T = &sT;
     w.G = &sG;
-    w.lane = threadIdx.x & 31;
+    w.lane = tid & 31;
+    w.m = reinterpret_cast<const DModel*>(smem32);
     for (;;) {
-        unsigned c = 0;
-        if (w.lane == 0) c = atomicAdd(queue, 1u);
-        c = __shfl_sync(kFull32, c, 0);
-        if (c >= (unsigned)nchains) break;
-        const Chain32 ch = chains[c];
-        const DModel* gm = models + ch.model;
-        w.L = ws32_layout(gm->natoms, gm->nframes, gm->conf_size, gm->dof);
-        w.bind_model(gm);
-        w.evals = 0;
-        w.grid_hits = 0;
-        w.pair_hits = 0;
-        run_chain32(w, ch, P);
+        if (tid == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const Item32 item = items[it];
+        stage_model(models + item.model, smem32, tid, nthr);
+        if (warp < item.count) {
+            const Chain32 ch = chains[item.first + warp];
+            const DModel& m = *w.m;
+            w.L = ws32_layout(m.natoms, m.nframes, m.conf_size, m.dof);
+            w.evals = 0;
+            w.grid_hits = 0;
+            w.pair_hits = 0;
+            run_chain32(w, ch, P);
+        }
+        __syncthreads();  // the staged model is in use until every warp is done
     }
 }
 
@@ -489,7 +560,7 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
     w.grid_hits = 0;
     w.pair_hits = 0;
     w.L = ws32_layout(model->natoms, model->nframes, model->conf_size, model->dof);
-    w.bind_model(model);
+    w.m = model;
     const DModel& m = *w.m;
     double* x = w.d(w.L.x_tmp);
     copyd(w, x, confs + (size_t)k * m.conf_size, m.conf_size);
@@ -516,20 +587,21 @@ static cudaError_t prep32(const void* fn, size_t smem) {
 }
 
 // resident blocks per SM of k_mc32 with `wpb` chains (warps) per block
-int mc32_occupancy(int wpb, size_t ws_stride) {
-    const size_t smem = (size_t)wpb * ws_stride;
+int mc32_occupancy(int wpb, size_t smem) {
     if (prep32((const void*)k_mc32, smem) != cudaSuccess) return 0;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_mc32, 32 * wpb, smem) != cudaSuccess) return 0;
     return blocks;
 }
 
-cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const Chain32* chains, int n,
-                        const MCParams32& P, unsigned* queue, int blocks, int wpb, size_t ws_stride, cudaStream_t s) {
-    const size_t smem = (size_t)wpb * ws_stride;
+cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const Chain32* chains,
+                        const Item32* items, int nitems, const MCParams32& P, unsigned* queue, int blocks, int wpb,
+                        size_t stage_stride, size_t ws_stride, cudaStream_t s) {
+    const size_t smem = stage_stride + (size_t)wpb * ws_stride;
     cudaError_t rc = prep32((const void*)k_mc32, smem);
     if (rc != cudaSuccess) return rc;
-    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, chains, n, P, queue, (int)ws_stride);
+    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, chains, items, nitems, P, queue, (int)stage_stride,
+                                          (int)ws_stride);
     return cudaGetLastError();
 }
 

@@ -99,13 +99,19 @@ struct __align__(16) DModel {
     const float4* finit32;    // [F]
     const int* pair_tp;       // [P] type-pair index, bit 30 set when the pair's types are swapped
     const int* fsub_end;      // [F] end of the atom range of the frame's subtree (depth-first layout)
-    // mixed-precision pair order: round robin over first-atom groups so the
-    // 32 pairs a warp handles at once touch different atoms
-    const int2* pairs32;      // [P] (a, b)
-    const int* tp32;          // [P] type pair | swapped << 30 | intramolecular (v[0]) << 29
+    // mixed-precision pair schedule: npchunks chunks of 32 slots; within a
+    // chunk every atom is at most once the first and once the second atom.
+    // Slot: a | b << 8 | type pair << 16 | swapped << 25 | intramolecular
+    // (v[0]) << 26; unused slots kSlotEmpty.  Null when the model has more
+    // than 255 movable atoms.
+    const uint32_t* pslot;    // [npchunks * 32]
     int cost;                 // relative cost of one evaluation (atoms + pairs + frames)
-    int pad_[3];
+    int npchunks;
+    int pad_[2];
 };
+
+constexpr uint32_t kSlotEmpty = 0xffffffffu;
+constexpr uint32_t kSlotSwap = 1u << 25, kSlotIntra = 1u << 26;
 
 // FP32 pair table: per (type pair, sample i, component) the float4
 // (e_i, dor_i, e_i+1, dor_i+1), so one interpolation is one 16 B load
@@ -141,6 +147,19 @@ struct Chain32 {
     unsigned long long* evals;
     unsigned long long* hits;  // [2]: grid lookups, in-cutoff pair lookups
 };
+
+// A block's unit of work: chains [first, first + count) of one model
+struct Item32 {
+    int model, first, count;
+};
+
+// Bytes of the block-shared copy of a model (descriptor + the arrays the
+// mixed-precision search reads), 16 B aligned pieces
+SG_HD int stage32_bytes(int natoms, int nframes, int nheavy, int npchunks, int nlig, int nblocks, int ntors) {
+    auto r = [](int b) { return (b + 15) & ~15; };
+    return r((int)sizeof(DModel)) + r(16 * natoms) + 2 * r(4 * natoms) + 2 * r(16 * nframes) + 6 * r(4 * nframes) +
+           r(4 * nheavy) + r(128 * npchunks) + 3 * r(4 * nlig) + 3 * r(4 * nblocks) + 2 * r(4 * ntors);
+}
 
 struct MCParams32 {
     float hunt[3], auth[3];

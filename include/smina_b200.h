@@ -270,8 +270,9 @@ int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
 int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookups,
                       uint64_t* pair_lookups, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
-/* Chains (warps) per block of the search kernel: 1, 2 or 4, or 0 to pick
- * the shape with the most resident chains per SM (the default). */
+/* Chains (warps) per block of the search kernel: 1, 2, 4 or 8, or 0 to
+ * pick the shape with the most resident chains per SM (the default).  The
+ * chains of one block share one copy of their ligand's model. */
 int sg_set_chains_per_block(sg_engine* e, int n);
 
 #ifdef __cplusplus
