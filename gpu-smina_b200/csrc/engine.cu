@@ -630,6 +630,51 @@ void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedM
     cuda_check(cudaStreamSynchronize(e->stream), "model upload");
 }
 
+// Host image of the packed models for a caller that places them in device
+// memory it already owns: the int, double and float pools and then the
+// descriptors, each 16 B aligned, with every descriptor pointer aimed at
+// dev_base + its offset in the image.
+void pack_models_image(const sg_model_desc* models, int nmodels, char* dev_base, ModelImage& img) {
+    require(models && nmodels > 0 && nmodels <= (1 << 20), "models: bad array");
+    std::vector<int> I;
+    std::vector<double> D;
+    std::vector<float> Fl;
+    std::vector<std::vector<size_t>> ioffs(nmodels), doffs(nmodels), foffs(nmodels);
+    img.host.assign(nmodels, DModel{});
+    for (int k = 0; k < nmodels; k++) pack_one(models[k], I, D, Fl, ioffs[k], doffs[k], foffs[k], img.host[k]);
+    auto r16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t oi = 0, od = r16(I.size() * sizeof(int)), of = od + r16(D.size() * sizeof(double));
+    img.dmodel_off = of + r16(Fl.size() * sizeof(float));
+    img.bytes.assign(img.dmodel_off + nmodels * sizeof(DModel), 0);
+    std::memcpy(img.bytes.data() + oi, I.data(), I.size() * sizeof(int));
+    std::memcpy(img.bytes.data() + od, D.data(), D.size() * sizeof(double));
+    std::memcpy(img.bytes.data() + of, Fl.data(), Fl.size() * sizeof(float));
+    const int* ib = reinterpret_cast<const int*>(dev_base + oi);
+    const double* db = reinterpret_cast<const double*>(dev_base + od);
+    const float* fb = reinterpret_cast<const float*>(dev_base + of);
+    for (int k = 0; k < nmodels; k++) {
+        DModel& h = img.host[k];
+        const std::vector<size_t>& io = ioffs[k];
+        const std::vector<size_t>& dd = doffs[k];
+        const std::vector<size_t>& fo = foffs[k];
+        const int** ip[] = {&h.type, &h.fkind, &h.fparent, &h.fbegin, &h.fend, &h.fconf, &h.fdof, &h.atom_frame,
+                            &h.level_start, &h.level_frames, &h.child_start, &h.child_list, &h.pairs, &h.pair_group,
+                            &h.csr_start, &h.csr, &h.heavy, &h.lig_begin, &h.lig_end, &h.lig_root, &h.lig_pair_end,
+                            &h.blk_rigid, &h.blk_conf, &h.blk_dof, &h.blk_ntors, &h.tor_conf, &h.tor_dof,
+                            &h.tor_frame, &h.pair_tp, &h.fsub_end};
+        size_t j = 0;
+        for (const int** q : ip) *q = ib + io[j++];
+        h.pslot = h.npchunks >= 0 ? reinterpret_cast<const uint32_t*>(ib + io[j]) : nullptr;
+        const float4** fp[] = {&h.local32, &h.lab32, &h.forigin32, &h.faxis32, &h.finit32};
+        j = 0;
+        for (const float4** q : fp) *q = reinterpret_cast<const float4*>(fb + fo[j++]);
+        const double** dp[] = {&h.charge, &h.local, &h.lab, &h.forigin, &h.faxis, &h.finit};
+        j = 0;
+        for (const double** q : dp) *q = db + dd[j++];
+    }
+    std::memcpy(img.bytes.data() + img.dmodel_off, img.host.data(), nmodels * sizeof(DModel));
+}
+
 void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels) {
     std::vector<int> types;
     for (int k = 0; k < nmodels; k++)

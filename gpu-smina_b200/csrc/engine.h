@@ -140,6 +140,12 @@ cudaError_t launch_eval32(const DModel*, size_t, const DTables32&, const DMaps32
 DTables32 tables32(const sg_engine* e);
 DMaps32 maps32(const sg_engine* e, const RecState& r);
 void pack_models(sg_engine* e, const sg_model_desc* models, int nmodels, PackedModels& out);
+struct ModelImage {
+    std::vector<char> bytes;   // pools then descriptors, ready to copy to the device
+    size_t dmodel_off = 0;     // byte offset of the descriptor array
+    std::vector<DModel> host;  // the descriptors (device addresses)
+};
+void pack_models_image(const sg_model_desc* models, int nmodels, char* dev_base, ModelImage& img);
 RecState& receptor_for(sg_engine* e, int rid);
 void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes);
 void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels);

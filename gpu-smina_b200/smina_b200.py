@@ -129,6 +129,8 @@ def _declare(L):
                     C.c_int, _dp],
         "sg_dock_batch32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
                             C.POINTER(MCParams), C.c_int, C.POINTER(LigandResult)],
+        "sg_dock_batch32_noalloc": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
+                                    C.POINTER(MCParams), C.POINTER(LigandResult)],
         "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
         "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
         "sg_set_chains_per_block": [vp, C.c_int],
@@ -422,6 +424,28 @@ class Engine:
             n = outs[k].count
             res.append({"e": e[:n].copy(), "conf": conf[:n].copy(), "coords": xyz[:n].copy(), "evals": int(outs[k].evals)})
         return res
+
+    def dock_batch_noalloc(self, rid, models, jobs, params: MCParams):
+        """The batched search and merge without device allocation inside the
+        call (sg_dock_batch32_noalloc); same results as
+        ``dock_batch(..., refine=False)``.  For callers that must not have
+        memory allocated or freed mid-request; the batch must fit the fixed
+        8 MiB scratch array and overlapping calls on one GPU must be avoided."""
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        J = (LigandJob * len(jobs))(*jobs)
+        S = params.num_saved_mins
+        bufs = []
+        outs = (LigandResult * len(jobs))()
+        for k, j in enumerate(jobs):
+            m = models[j.model]
+            e, conf, xyz = np.zeros(S), np.zeros((S, m.conf_size)), np.zeros((S, m.heavy, 3))
+            bufs.append((e, conf, xyz))
+            outs[k].e, outs[k].conf, outs[k].coords = dptr(e), dptr(conf), dptr(xyz)
+        self._check(load().sg_dock_batch32_noalloc(self._h, rid, descs, len(models), J, len(jobs), C.byref(params),
+                                                   outs))
+        return [{"e": e[:outs[k].count].copy(), "conf": conf[:outs[k].count].copy(),
+                 "coords": xyz[:outs[k].count].copy(), "evals": int(outs[k].evals)}
+                for k, (e, conf, xyz) in enumerate(bufs)]
 
     def batch_stats(self):
         """Timing and counters of the last dock_batch call."""

@@ -260,6 +260,28 @@ int sg_dock_batch32(sg_engine* e, int receptor_id, const sg_model_desc* models, 
                     const sg_ligand_job* jobs, int njobs, const sg_mc_params* p, int refine,
                     sg_ligand_result* out);
 
+/* sg_dock_batch32 with refine = 0, for callers that must not have device
+ * memory allocated or freed while the call runs.  No counterpart in the
+ * reference.  A serving loop may have promised the rest of the GPU's memory
+ * to requests in flight or to a caching allocator, so an allocation here
+ * could fail or fragment it; and cudaFree waits for the whole device to go
+ * idle, stalling the caller's other streams.  This call places everything
+ * the search kernel writes (its copy of the models, chain and work tables,
+ * the queue counter, the chains' result slots) in one fixed 8 MiB array per
+ * device that is part of the library's image.  Limits and rules:
+ *   - a batch that needs more than the 8 MiB is refused with SG_ERR_ARG
+ *     (for example 16 ligands of 50 heavy atoms x 8 chains fit);
+ *   - the receptor's maps for the ligands' atom types must already be
+ *     built (sg_build_grids), since building them allocates;
+ *   - the first call on a device looks up the array's device address;
+ *   - every call reuses the same array, so calls that overlap on one GPU
+ *     (two engines, or two host threads) corrupt each other: keep them
+ *     apart.
+ * Results are the same as sg_dock_batch32's with refine = 0. */
+int sg_dock_batch32_noalloc(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+                            const sg_ligand_job* jobs, int njobs, const sg_mc_params* p,
+                            sg_ligand_result* out);
+
 /* Timing and launch shape of the last sg_dock_batch32 call. */
 int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
                    int* chains_per_block, int* blocks);
