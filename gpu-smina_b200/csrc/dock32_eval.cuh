@@ -27,6 +27,20 @@ __device__ unsigned long long g_prof[16];
 #define SG_T1(name, k)
 #endif
 
+// Dynamic shared memory of the mixed-precision kernels: the block's staged
+// model (SModel + arrays) at offset 0, then one workspace per warp.  Every
+// access is this symbol plus a 32-bit offset, so it compiles to shared-space
+// loads and stores with 32-bit addresses.
+extern __shared__ __align__(16) char smem32[];
+__shared__ DTables32 sT32;  // the pair table descriptor of the running kernel
+__shared__ DMaps32 sG32;    // the grid maps of the running kernel
+
+template <typename T>
+__device__ __forceinline__ T* sp(int off) {
+    return reinterpret_cast<T*>(smem32 + off);
+}
+__device__ __forceinline__ const SModel& smodel() { return *reinterpret_cast<const SModel*>(smem32); }
+
 // per-warp workspace (bytes, 16 B aligned)
 struct Ws32 {
     int coords, force, origin, axis, quat, rot;                  // float4 arrays (rot: 3 rows per frame)
@@ -96,25 +110,23 @@ __device__ __forceinline__ double ph_normal(Philox& r) {  // Box-Muller
     return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
 }
 
+// One warp's view of its chain: its workspace offset and layout, its lane,
+// and its work counters.
 struct W32 {
-    char* s;  // this warp's workspace
+    int ws;  // byte offset of this warp's workspace in smem32
     Ws32 L;
-    const DModel* m;  // staged copy in shared memory
-    const DTables32* T;
-    const DMaps32* G;
     int lane;
     unsigned long long evals;
     unsigned long long grid_hits, pair_hits;  // per-lane gather counts (algorithmic bytes)
-    __device__ float4* coords() const { return (float4*)(s + L.coords); }
-    __device__ float4* force() const { return (float4*)(s + L.force); }
-    __device__ float4* origin() const { return (float4*)(s + L.origin); }
-    __device__ float4* axis() const { return (float4*)(s + L.axis); }
-    __device__ float4* quat() const { return (float4*)(s + L.quat); }
-    __device__ float4* rot() const { return (float4*)(s + L.rot); }
-    __device__ double* d(int off) const { return (double*)(s + off); }
-    __device__ float* scratch() const { return (float*)(s + L.scratch); }
+    __device__ int at(int field) const { return ws + field; }  // smem32 offset of a workspace array
+    __device__ float4* coords() const { return sp<float4>(ws + L.coords); }
+    __device__ float4* force() const { return sp<float4>(ws + L.force); }
+    __device__ float4* origin() const { return sp<float4>(ws + L.origin); }
+    __device__ float4* axis() const { return sp<float4>(ws + L.axis); }
+    __device__ float4* quat() const { return sp<float4>(ws + L.quat); }
+    __device__ float4* rot() const { return sp<float4>(ws + L.rot); }
+    __device__ double* d(int field) const { return sp<double>(ws + field); }
 };
-static_assert(sizeof(DModel) % 16 == 0, "DModel is copied in 16 byte pieces");
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -174,29 +186,36 @@ __device__ __forceinline__ float warp_sum(float v) {
 // need no parent data; the lab transforms are their ordered compositions
 // along the path to the root, done by pointer jumping in log2(depth) warp
 // shuffles.  Trees of more than 32 frames go level by level.
-__device__ __noinline__ void set_conf32(W32& w, const double* conf) {
-    const DModel& m = *w.m;
+__device__ __noinline__ void set_conf32(W32& w, int conf_at) {
+    const SModel& m = smodel();
+    const double* conf = sp<const double>(conf_at);
+    const int nframes = m.nframes, nmov = m.nmov;
+    const int* fkind = sp<const int>(m.fkind);
+    const int* fconf = sp<const int>(m.fconf);
+    const int* fparent = sp<const int>(m.fparent);
+    const float4* forigin = sp<const float4>(m.forigin32);
+    const float4* faxis = sp<const float4>(m.faxis32);
     float4* O = w.origin();
     float4* A = w.axis();
     float4* Q = w.quat();
     float4* R = w.rot();
-    if (m.nframes <= 32) {
+    if (nframes <= 32) {
         const int f = w.lane;
-        const bool act = f < m.nframes;
+        const bool act = f < nframes;
         float4 q = make_float4(1, 0, 0, 0);
         float3 t = make_float3(0, 0, 0);
         int anc = -1, parent = -1, kind = 0;
         if (act) {
-            kind = m.fkind[f];
-            const int ci = m.fconf[f];
+            kind = fkind[f];
+            const int ci = fconf[f];
             if (kind == SG_FRAME_RIGID) {
                 const double* c = conf + ci;
                 t = make_float3((float)c[0], (float)c[1], (float)c[2]);
                 q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
             } else {
-                if (kind == SG_FRAME_SEGMENT) parent = anc = m.fparent[f];
-                t = f3(m.forigin32[f]);
-                q = axis_angle32(f3(m.faxis32[f]), (float)conf[ci]);
+                if (kind == SG_FRAME_SEGMENT) parent = anc = fparent[f];
+                t = f3(forigin[f]);
+                q = axis_angle32(f3(faxis[f]), (float)conf[ci]);
             }
         }
         for (int it = 0; it < 6 && __any_sync(kFull32, anc >= 0); it++) {
@@ -223,35 +242,35 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
             Q[f] = q;
             quat_rows(q, R + 3 * f);
             if (kind == SG_FRAME_SEGMENT) {
-                const float3 ax = qrot(pq, f3(m.faxis32[f]));
+                const float3 ax = qrot(pq, f3(faxis[f]));
                 A[f] = make_float4(ax.x, ax.y, ax.z, 0);
             } else if (kind == SG_FRAME_FIRST_SEGMENT) {
-                A[f] = m.faxis32[f];
+                A[f] = faxis[f];
             }
         }
         __syncwarp();
     } else {
         for (int lv = 0; lv < m.nlevels; lv++) {
-            for (int idx = m.level_start[lv] + w.lane; idx < m.level_start[lv + 1]; idx += 32) {
+            for (int idx = __ldg(m.level_start + lv) + w.lane; idx < __ldg(m.level_start + lv + 1); idx += 32) {
                 const int f = __ldg(m.level_frames + idx);
-                const int kind = m.fkind[f];
+                const int kind = fkind[f];
                 float4 q;
                 if (kind == SG_FRAME_RIGID) {
-                    const double* c = conf + m.fconf[f];
+                    const double* c = conf + fconf[f];
                     O[f] = make_float4((float)c[0], (float)c[1], (float)c[2], 0);
                     q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
                 } else if (kind == SG_FRAME_SEGMENT) {
-                    const int p = m.fparent[f];
-                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(m.forigin32[f]));
-                    const float3 ax = rot_apply(R + 3 * p, f3(m.faxis32[f]));
+                    const int p = fparent[f];
+                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(forigin[f]));
+                    const float3 ax = rot_apply(R + 3 * p, f3(faxis[f]));
                     O[f] = make_float4(o.x, o.y, o.z, 0);
                     A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[m.fconf[f]]), Q[p]));
+                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[fconf[f]]), Q[p]));
                 } else {
-                    const float3 ax = f3(m.faxis32[f]);
-                    O[f] = m.forigin32[f];
+                    const float3 ax = f3(faxis[f]);
+                    O[f] = forigin[f];
                     A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = axis_angle32(ax, (float)conf[m.fconf[f]]);
+                    q = axis_angle32(ax, (float)conf[fconf[f]]);
                 }
                 Q[f] = q;
                 quat_rows(q, R + 3 * f);
@@ -260,9 +279,11 @@ __device__ __noinline__ void set_conf32(W32& w, const double* conf) {
         }
     }
     float4* X = w.coords();
-    for (int i = w.lane; i < m.nmov; i += 32) {
-        const int f = m.atom_frame[i];
-        const float3 c = f3(O[f]) + rot_apply(R + 3 * f, f3(m.local32[i]));
+    const int* atom_frame = sp<const int>(m.atom_frame);
+    const float4* local = sp<const float4>(m.local32);
+    for (int i = w.lane; i < nmov; i += 32) {
+        const int f = atom_frame[i];
+        const float3 c = f3(O[f]) + rot_apply(R + 3 * f, f3(local[i]));
         X[i] = make_float4(c.x, c.y, c.z, 0);
     }
     __syncwarp();
@@ -332,10 +353,11 @@ __device__ __forceinline__ void table32_nc(const DTables32& T, int p, bool swap,
 }
 
 // model::eval_deriv in FP32; returns the energy (same on every lane), writes g (FP64)
-__device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const float v[3], float slope, double* g) {
-    const DModel& m = *w.m;
+__device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float slope, int g_at) {
+    const SModel& m = smodel();
+    double* g = sp<double>(g_at);
     SG_T0(t_set);
-    set_conf32(w, conf);
+    set_conf32(w, conf_at);
     SG_T1(t_set, 0);
     SG_T0(t_grid);
     float4* X = w.coords();
@@ -343,18 +365,19 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     float e = 0;
     // grid part; every movable atom gets its force reset (hydrogens: zero)
     const int nmov = m.nmov;
-    const int* __restrict__ TYPE = m.type;
+    const int* TYPE = sp<const int>(m.type);
+    const float4* LQ = sp<const float4>(m.local32);
     for (int i = w.lane; i < nmov; i += 32) {
         const int t = TYPE[i];
         float3 d = make_float3(0, 0, 0);
         if (t < kNumTypes && !is_h(t)) {
             const float3 loc = f3(X[i]);
-            e += grid_aux32(*w.G, t, false, loc, slope, v[1], d);
+            e += grid_aux32(sG32, t, false, loc, slope, v.y, d);
             w.grid_hits++;
-            const float q = m.local32[i].w;
-            if (q != 0.f && w.G->c32[t]) {
+            const float q = LQ[i].w;
+            if (q != 0.f && sG32.c32[t]) {
                 float3 cd;
-                e += q * grid_aux32(*w.G, t, true, loc, slope, v[1], cd);
+                e += q * grid_aux32(sG32, t, true, loc, slope, v.y, cd);
                 d = d + q * cd;
                 w.grid_hits++;
             }
@@ -369,9 +392,8 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     // second atom, so the force updates are plain read-add-writes: first
     // atoms, sync, second atoms, sync.
     const int nch = m.npchunks;
-    const uint32_t* PS = m.pslot;
-    const float4* LQ = m.local32;
-    const DTables32 T = *w.T;
+    const uint32_t* PS = sp<const uint32_t>(m.pslot);
+    const DTables32 T = sT32;
     const int lane = w.lane;
     unsigned long long hits = 0;
     for (int c = 0; c < nch; c += 2) {
@@ -414,7 +436,7 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
                 table32_nc(T, (sl[u] >> 16) & 0x1ff, (sl[u] & kSlotSwap) != 0, LQ[ia[u]].w, LQ[ib[u]].w, r2[u], pe, dor);
             }
             f[u] = dor * r[u];
-            const float vv = (sl[u] & kSlotIntra) ? v[0] : v[2];
+            const float vv = (sl[u] & kSlotIntra) ? v.x : v.z;
             if (pe > 0) {
                 const float tt = (vv < 1.1920929e-07f) ? 0.f : (vv / (vv + pe));
                 pe *= tt;
@@ -451,14 +473,14 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
     // c_i = (x_i - o_ref) x F_i, T_sub = PC[E] - PC[b] - (o_f - o_ref) x F_sub.
     // Torques are taken about the first root's origin to keep them small.
     float4* O = w.origin();
-    float4* PF = (float4*)(w.s + w.L.pf);
-    float4* PC = (float4*)(w.s + w.L.pc);
+    float4* PF = sp<float4>(w.at(w.L.pf));
+    float4* PC = sp<float4>(w.at(w.L.pc));
     const float3 oref = f3(O[0]);
     float3 cf = make_float3(0, 0, 0), cc = make_float3(0, 0, 0);
-    for (int base = 0; base < m.nmov; base += 32) {
+    for (int base = 0; base < nmov; base += 32) {
         const int i = base + w.lane;
         float3 F = make_float3(0, 0, 0), Cq = make_float3(0, 0, 0);
-        if (i < m.nmov) {
+        if (i < nmov) {
             F = f3(Fz[i]);
             Cq = cross3(f3(X[i]) - oref, F);
         }
@@ -473,7 +495,7 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
                 iC = iC + make_float3(b0, b1, b2);
             }
         }
-        if (i < m.nmov) {  // exclusive prefix at i
+        if (i < nmov) {  // exclusive prefix at i
             const float3 eF = cf + (iF - F), eC = cc + (iC - Cq);
             PF[i] = make_float4(eF.x, eF.y, eF.z, 0);
             PC[i] = make_float4(eC.x, eC.y, eC.z, 0);
@@ -482,16 +504,20 @@ __device__ __noinline__ float eval_deriv32(W32& w, const double* conf, const flo
         cc = cc + make_float3(__shfl_sync(kFull32, iC.x, 31), __shfl_sync(kFull32, iC.y, 31), __shfl_sync(kFull32, iC.z, 31));
     }
     if (w.lane == 0) {
-        PF[m.nmov] = make_float4(cf.x, cf.y, cf.z, 0);
-        PC[m.nmov] = make_float4(cc.x, cc.y, cc.z, 0);
+        PF[nmov] = make_float4(cf.x, cf.y, cf.z, 0);
+        PC[nmov] = make_float4(cc.x, cc.y, cc.z, 0);
     }
     __syncwarp();
+    const int* fbegin = sp<const int>(m.fbegin);
+    const int* fsub_end = sp<const int>(m.fsub_end);
+    const int* fdof = sp<const int>(m.fdof);
+    const int* fkind = sp<const int>(m.fkind);
     for (int f = w.lane; f < m.nframes; f += 32) {
-        const int b = m.fbegin[f], E = m.fsub_end[f];
+        const int b = fbegin[f], E = fsub_end[f];
         const float3 F = f3(PF[E]) - f3(PF[b]);
         const float3 T = (f3(PC[E]) - f3(PC[b])) - cross3(f3(O[f]) - oref, F);
-        const int dof0 = m.fdof[f];
-        if (m.fkind[f] == SG_FRAME_RIGID) {
+        const int dof0 = fdof[f];
+        if (fkind[f] == SG_FRAME_RIGID) {
             g[dof0] = F.x; g[dof0 + 1] = F.y; g[dof0 + 2] = F.z;
             g[dof0 + 3] = T.x; g[dof0 + 4] = T.y; g[dof0 + 5] = T.z;
         } else {

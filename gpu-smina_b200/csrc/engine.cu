@@ -725,8 +725,10 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
         if (!direct && e->precision != SG_PREC_FP64) {  // the mixed-precision evaluation
             require(h.npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
             const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
-            require(ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
-            cuda_check(launch_eval32(pm.dmodels.as<DModel>(), ws, tables32(e), maps32(e, r), nconfs, dc.p(), v, slope,
+            const size_t stage =
+                (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
+            require(stage + ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
+            cuda_check(launch_eval32(pm.dmodels.as<DModel>(), stage, ws, tables32(e), maps32(e, r), nconfs, dc.p(), v, slope,
                                      de.p(), dg.p(), out_coords ? dx.p() : nullptr, e->stream),
                        "eval launch");
             de.fetch(out_e, e->stream);

@@ -133,8 +133,8 @@ int mc32_occupancy(int wpb, size_t smem);
 cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const Chain32*, const Item32*, int nitems,
                         const MCParams32&, unsigned*, int blocks, int wpb, size_t stage_stride, size_t ws_stride,
                         cudaStream_t);
-cudaError_t launch_eval32(const DModel*, size_t, const DTables32&, const DMaps32&, int, const double*, const double[3],
-                          double, double*, double*, double*, cudaStream_t);
+cudaError_t launch_eval32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, const double*,
+                          const double[3], double, double*, double*, double*, cudaStream_t);
 
 // FP32 views of the engine's tables and of a receptor's packed maps
 DTables32 tables32(const sg_engine* e);

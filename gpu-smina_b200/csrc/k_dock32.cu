@@ -35,7 +35,7 @@ __device__ __forceinline__ void copyd(const W32& w, double* d, const double* s, 
 
 // quaternion_increment (quaternion.cpp:118-126) with an FP32 sine/cosine of
 // the half angle, composed and re-normalised in FP64
-__device__ void q_increment32(double* c, double rx, double ry, double rz) {
+__device__ __forceinline__ void q_increment32(double* c, double rx, double ry, double rz) {
     const double ang = sqrt(rx * rx + ry * ry + rz * rz);
     double s = 0, co = 1;
     if (ang > kEps) {
@@ -53,75 +53,95 @@ __device__ void q_increment32(double* c, double rx, double ry, double rz) {
 }
 
 // conf::increment
-__device__ void increment32(const W32& w, double* x, const double* p, double alpha) {
-    const DModel& m = *w.m;
+__device__ __forceinline__ void increment32(const W32& w, double* x, const double* p, double alpha) {
+    const SModel& m = smodel();
+    const int* lig_root = sp<const int>(m.lig_root);
+    const int* fconf = sp<const int>(m.fconf);
+    const int* fdof = sp<const int>(m.fdof);
+    const int* tor_conf = sp<const int>(m.tor_conf);
+    const int* tor_dof = sp<const int>(m.tor_dof);
     for (int l = w.lane; l < m.nlig; l += 32) {
-        const int f = m.lig_root[l];
-        double* c = x + m.fconf[f];
-        const double* d = p + m.fdof[f];
+        const int f = lig_root[l];
+        double* c = x + fconf[f];
+        const double* d = p + fdof[f];
         c[0] += alpha * d[0]; c[1] += alpha * d[1]; c[2] += alpha * d[2];
         q_increment32(c + 3, alpha * d[3], alpha * d[4], alpha * d[5]);
     }
     for (int k = w.lane; k < m.ntors; k += 32) {
-        double& t = x[m.tor_conf[k]];
-        t += normalized_angle(alpha * p[m.tor_dof[k]]);
+        double& t = x[tor_conf[k]];
+        t += normalized_angle(alpha * p[tor_dof[k]]);
         normalize_angle(t);
     }
     __syncwarp();
 }
 
 // conf::operator()(index): value of change coordinate i (accurate line search)
-__device__ double conf_value32(const DModel& m, const double* x, int i) {
+__device__ double conf_value32(const double* x, int i) {
+    const SModel& m = smodel();
+    const int* lig_root = sp<const int>(m.lig_root);
+    const int* fconf = sp<const int>(m.fconf);
+    const int* fdof = sp<const int>(m.fdof);
+    const int* tor_conf = sp<const int>(m.tor_conf);
+    const int* tor_dof = sp<const int>(m.tor_dof);
     for (int l = 0; l < m.nlig; l++) {
-        const int f = m.lig_root[l];
-        const int d0 = m.fdof[f];
-        if (i >= d0 && i < d0 + 3) return x[m.fconf[f] + (i - d0)];
+        const int f = lig_root[l];
+        const int d0 = fdof[f];
+        if (i >= d0 && i < d0 + 3) return x[fconf[f] + (i - d0)];
         if (i >= d0 + 3 && i < d0 + 6) {
-            const double* c = x + m.fconf[f];
+            const double* c = x + fconf[f];
             const V3<double> a = q_to_angle(Quat<double>{c[3], c[4], c[5], c[6]});
             const int j = i - d0 - 3;
             return j == 0 ? a.x : j == 1 ? a.y : a.z;
         }
     }
     for (int k = 0; k < m.ntors; k++)
-        if (m.tor_dof[k] == i) return x[m.tor_conf[k]];
+        if (tor_dof[k] == i) return x[tor_conf[k]];
     return 0;
 }
 
 struct Mode32 {
-    float v[3];
+    float3 v;
     float slope;
 };
 
-__device__ __forceinline__ double feval32(W32& w, const double* x, double* g, const Mode32& em) {
-    return (double)eval_deriv32(w, x, em.v, em.slope, g);
+// energy and gradient of the conf at smem32 offset x_at (gradient to g_at)
+__device__ __forceinline__ double feval32(W32& w, int x_at, int g_at, const Mode32& em) {
+    return (double)eval_deriv32(w, x_at, em.v, em.slope, g_at);
 }
 
 // ---- line searches (bfgs.h:30-200) ------------------------------------------------------
-__device__ double line_fast32(W32& w, const double* x, const double* g, double f0, const double* p, double* x_new,
-                              double* g_new, double& f1, const Mode32& em) {
-    const DModel& m = *w.m;
+// x, g, p, x_new, g_new: offsets of this warp's workspace arrays in smem32
+__device__ __forceinline__ double line_fast32(W32& w, int x_at, int g_at, double f0, int p_at, int xn_at, int gn_at,
+                                              double& f1, const Mode32& em) {
+    const SModel& m = smodel();
+    const double* x = sp<const double>(x_at);
+    const double* p = sp<const double>(p_at);
+    double* x_new = sp<double>(xn_at);
     double alpha = 1;
-    const double pg = dotd(w, p, g, m.dof);
+    const double pg = dotd(w, p, sp<const double>(g_at), m.dof);
     for (unsigned trial = 0; trial < 10; trial++) {
         SG_T0(t_ls);
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
         SG_T1(t_ls, 4);
-        f1 = feval32(w, x_new, g_new, em);
+        f1 = feval32(w, xn_at, gn_at, em);
         if (f1 - f0 < 0.0001 * alpha * pg) break;
         alpha *= 0.5;
     }
     return alpha;
 }
 
-__device__ double line_accurate32(W32& w, const double* x, const double* g, double f0, const double* p, double* x_new,
-                                  double* g_new, double& f1, const Mode32& em) {
-    const DModel& m = *w.m;
+__device__ __forceinline__ double line_accurate32(W32& w, int x_at, int g_at, double f0, int p_at, int xn_at,
+                                                  int gn_at, double& f1, const Mode32& em) {
+    const SModel& m = smodel();
     const int n = m.dof;
+    const double* x = sp<const double>(x_at);
+    const double* p = sp<const double>(p_at);
+    double* x_new = sp<double>(xn_at);
+    double* g_new = sp<double>(gn_at);
     double a, alpha, alpha2 = 0, alamin, b, disc, f2 = 0, rhs1, rhs2, tmplam = 0;
     const double ALF = 1.0e-4, FIRST = 1.0;
-    const double slope = dotd(w, g, p, n);
+    const double slope = dotd(w, sp<const double>(g_at), p, n);
     auto give_up = [&]() {
         copyd(w, x_new, x, m.conf_size);
         for (int i = w.lane; i < n; i += 32) g_new[i] = 0;
@@ -130,7 +150,7 @@ __device__ double line_accurate32(W32& w, const double* x, const double* g, doub
     };
     if (slope >= 0) return give_up();
     double test = 0;
-    for (int i = w.lane; i < n; i += 32) test = fmax(test, fabs(p[i]) / fmax(fabs(conf_value32(m, x, i)), 1.0));
+    for (int i = w.lane; i < n; i += 32) test = fmax(test, fabs(p[i]) / fmax(fabs(conf_value32(x, i)), 1.0));
     for (int o = 16; o > 0; o >>= 1) test = fmax(test, __shfl_xor_sync(kFull32, test, o));
     alamin = kEps / test;
     alpha = FIRST;
@@ -138,7 +158,7 @@ __device__ double line_accurate32(W32& w, const double* x, const double* g, doub
     for (int it = 0; it < 128; it++) {
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
-        f1 = feval32(w, x_new, g_new, em);
+        f1 = feval32(w, xn_at, gn_at, em);
         if (alpha < alamin) return give_up();
         if (f1 <= f0 + ALF * alpha * slope) return alpha;
         if (alpha == FIRST) {
@@ -169,17 +189,19 @@ __device__ double line_accurate32(W32& w, const double* x, const double* g, doub
 // Lane i owns row i, stored as column i of h (h[j * n + i]) so the lanes of
 // a row sweep read consecutive words.  Every entry (i, j) is computed from
 // (min(i, j), max(i, j)) operands in one fixed order, so h stays exactly
-// symmetric.
-__device__ __noinline__ double bfgs32(W32& w, double* x, int maxiters, int accurate, int early, const Mode32& em) {
-    const DModel& m = *w.m;
+// symmetric.  x_at: smem32 offset of the conf, optimised in place.
+__device__ __noinline__ double bfgs32(W32& w, int x_at, int maxiters, int accurate, int early, const Mode32& em) {
+    const SModel& m = smodel();
     const int n = m.dof, cs = m.conf_size;
+    const int g_at = w.at(w.L.g), gn_at = w.at(w.L.g_new), p_at = w.at(w.L.p), xn_at = w.at(w.L.x_new);
+    double* x = sp<double>(x_at);
     double* h = w.d(w.L.h);
-    double *g = w.d(w.L.g), *g_new = w.d(w.L.g_new), *g_orig = w.d(w.L.g_orig), *p = w.d(w.L.p), *y = w.d(w.L.y);
-    double *x_new = w.d(w.L.x_new), *x_orig = w.d(w.L.x_orig), *mhy = w.d(w.L.mhy);
+    double *g = sp<double>(g_at), *g_new = sp<double>(gn_at), *g_orig = w.d(w.L.g_orig), *p = sp<double>(p_at);
+    double *y = w.d(w.L.y), *x_new = sp<double>(xn_at), *x_orig = w.d(w.L.x_orig), *mhy = w.d(w.L.mhy);
     for (int i = w.lane; i < n; i += 32)
         for (int j = 0; j < n; j++) h[j * n + i] = (i == j) ? 1.0 : 0.0;
     __syncwarp();
-    double f0 = feval32(w, x, g, em);
+    double f0 = feval32(w, x_at, g_at, em);
     const double f_orig = f0;
     copyd(w, g_orig, g, n);
     copyd(w, x_orig, x, cs);
@@ -193,8 +215,8 @@ __device__ __noinline__ double bfgs32(W32& w, double* x, int maxiters, int accur
         __syncwarp();
         SG_T1(t_alg, 5);
         double f1 = 0;
-        const double alpha = accurate ? line_accurate32(w, x, g, f0, p, x_new, g_new, f1, em)
-                                      : line_fast32(w, x, g, f0, p, x_new, g_new, f1, em);
+        const double alpha = accurate ? line_accurate32(w, x_at, g_at, f0, p_at, xn_at, gn_at, f1, em)
+                                      : line_fast32(w, x_at, g_at, f0, p_at, xn_at, gn_at, f1, em);
         if (alpha == 0) break;
         SG_T0(t_alg2);
         for (int i = w.lane; i < n; i += 32) y[i] = g_new[i] - g[i];
@@ -243,7 +265,7 @@ __device__ __noinline__ double bfgs32(W32& w, double* x, int maxiters, int accur
 }
 
 // ---- Monte Carlo pieces -------------------------------------------------------------------
-__device__ V3<double> sphere32(Philox& rng) {  // random_inside_sphere, bounded rejection
+__device__ __forceinline__ V3<double> sphere32(Philox& rng) {  // random_inside_sphere, bounded rejection
     for (int k = 0; k < 64; k++) {
         const double a = ph_range(rng, -1, 1), b = ph_range(rng, -1, 1), c = ph_range(rng, -1, 1);
         if (a * a + b * b + c * c < 1) return V3<double>{a, b, c};
@@ -252,13 +274,15 @@ __device__ V3<double> sphere32(Philox& rng) {  // random_inside_sphere, bounded 
 }
 
 // gyration radius of ligand l's heavy atoms about its root origin (current coords)
-__device__ double gyration32(const W32& w, int l) {
-    const DModel& m = *w.m;
-    const float3 o = f3(w.origin()[m.lig_root[l]]);
+__device__ __forceinline__ double gyration32(const W32& w, int l) {
+    const SModel& m = smodel();
+    const int* type = sp<const int>(m.type);
+    const float3 o = f3(w.origin()[sp<const int>(m.lig_root)[l]]);
     float acc = 0;
     int cnt = 0;
-    for (int i = m.lig_begin[l] + w.lane; i < m.lig_end[l]; i += 32)
-        if (!is_h(m.type[i])) {
+    const int end = sp<const int>(m.lig_end)[l];
+    for (int i = sp<const int>(m.lig_begin)[l] + w.lane; i < end; i += 32)
+        if (!is_h(type[i])) {
             const float3 d = f3(w.coords()[i]) - o;
             acc += dot3(d, d);
             cnt++;
@@ -268,16 +292,19 @@ __device__ double gyration32(const W32& w, int l) {
     return cnt > 0 ? sqrt((double)acc / cnt) : 0.0;
 }
 
-__device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude) {
-    const DModel& m = *w.m;
+__device__ __forceinline__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude) {
+    const SModel& m = smodel();
+    const int* blk_rigid = sp<const int>(m.blk_rigid);
+    const int* blk_ntors = sp<const int>(m.blk_ntors);
+    const int* blk_conf = sp<const int>(m.blk_conf);
     int num = 0;
-    for (int b = 0; b < m.nblocks; b++) num += (m.blk_rigid[b] ? 2 : 0) + m.blk_ntors[b];
+    for (int b = 0; b < m.nblocks; b++) num += (blk_rigid[b] ? 2 : 0) + blk_ntors[b];
     if (num == 0) return;
     int which = ph_int(rng, num);
     int lig = 0;
     for (int b = 0; b < m.nblocks; b++) {
-        double* c = x + m.blk_conf[b];
-        if (m.blk_rigid[b]) {
+        double* c = x + blk_conf[b];
+        if (blk_rigid[b]) {
             if (which == 0) {
                 const V3<double> d = amplitude * sphere32(rng);
                 if (w.lane == 0) { c[0] += d.x; c[1] += d.y; c[2] += d.z; }
@@ -298,7 +325,7 @@ __device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude)
             c += 7;
             lig++;
         }
-        const int nt = m.blk_ntors[b];
+        const int nt = blk_ntors[b];
         if (which < nt) {
             const double t = ph_range(rng, -kPi, kPi);
             if (w.lane == 0) c[which] = t;
@@ -311,11 +338,14 @@ __device__ void mutate32(const W32& w, Philox& rng, double* x, double amplitude)
 
 // conf::randomize: position uniform in the box, orientation from four
 // normal deviates, torsions uniform in [-pi, pi)
-__device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams32& P) {
-    const DModel& m = *w.m;
+__device__ __forceinline__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams32& P) {
+    const SModel& m = smodel();
+    const int* blk_rigid = sp<const int>(m.blk_rigid);
+    const int* blk_ntors = sp<const int>(m.blk_ntors);
+    const int* blk_conf = sp<const int>(m.blk_conf);
     for (int b = 0; b < m.nblocks; b++) {
-        double* c = x + m.blk_conf[b];
-        if (m.blk_rigid[b]) {
+        double* c = x + blk_conf[b];
+        if (blk_rigid[b]) {
             double v[7];
             for (int k = 0; k < 3; k++) v[k] = ph_range(rng, P.box_lo[k], P.box_hi[k]);
             double q[4], nq = 0;
@@ -326,7 +356,7 @@ __device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams
             if (w.lane == 0) for (int k = 0; k < 7; k++) c[k] = v[k];
             c += 7;
         }
-        const int nt = m.blk_ntors[b];
+        const int nt = blk_ntors[b];
         for (int t = 0; t < nt; t++) {
             const double a = ph_range(rng, -kPi, kPi);
             if (w.lane == 0) c[t] = a;
@@ -337,10 +367,11 @@ __device__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams
 
 // add_to_output_container with the chain's container in global memory;
 // returns the new size
-__device__ int add_output32(const W32& w, const Chain32& ch, const double* x, double e, double min_rmsd, int max_size,
-                            int count) {
-    const DModel& m = *w.m;
+__device__ __forceinline__ int add_output32(const W32& w, const Chain32& ch, const double* x, double e,
+                                            double min_rmsd, int max_size, int count) {
+    const SModel& m = smodel();
     const int H = m.nheavy, cs = m.conf_size;
+    const int* heavy = sp<const int>(m.heavy);
     const float4* X = w.coords();
     // RMSD to every saved pose: lanes over atoms, one pose at a time
     float best = 3.4e38f;
@@ -349,7 +380,7 @@ __device__ int add_output32(const W32& w, const Chain32& ch, const double* x, do
         const float* oc = ch.out_coords + (size_t)ch.out_order[j] * H * 3;
         float acc = 0;
         for (int a = w.lane; a < H; a += 32) {
-            const float3 c = f3(X[m.heavy[a]]);
+            const float3 c = f3(X[heavy[a]]);
             const float dx = c.x - oc[3 * a], dy = c.y - oc[3 * a + 1], dz = c.z - oc[3 * a + 2];
             acc += dx * dx + dy * dy + dz * dz;
         }
@@ -371,7 +402,7 @@ __device__ int add_output32(const W32& w, const Chain32& ch, const double* x, do
     if (target >= 0) {
         for (int i = w.lane; i < cs; i += 32) ch.out_conf[(size_t)target * cs + i] = x[i];
         for (int a = w.lane; a < H; a += 32) {
-            const float3 c = f3(X[m.heavy[a]]);
+            const float3 c = f3(X[heavy[a]]);
             float* o = ch.out_coords + ((size_t)target * H + a) * 3;
             o[0] = c.x; o[1] = c.y; o[2] = c.z;
         }
@@ -395,18 +426,19 @@ __device__ int add_output32(const W32& w, const Chain32& ch, const double* x, do
 // monte_carlo::operator() for one chain
 __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCParams32& P) {
     SG_T0(t_chain);
-    const DModel& m = *w.m;
+    const SModel& m = smodel();
     const int cs = m.conf_size;
     // model state as read (mutation may read it before the first set)
     for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);
     for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
     __syncwarp();
     Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
-    double* tmp = w.d(w.L.x_tmp);
-    double* cand = w.d(w.L.x_cand);
+    const int tmp_at = w.at(w.L.x_tmp), cand_at = w.at(w.L.x_cand);
+    double* tmp = sp<double>(tmp_at);
+    double* cand = sp<double>(cand_at);
     randomize32(w, rng, tmp, P);
-    const Mode32 hunt{{P.hunt[0], P.hunt[1], P.hunt[2]}, P.slope};
-    const Mode32 auth{{P.auth[0], P.auth[1], P.auth[2]}, P.slope};
+    const Mode32 hunt{make_float3(P.hunt[0], P.hunt[1], P.hunt[2]), P.slope};
+    const Mode32 auth{make_float3(P.auth[0], P.auth[1], P.auth[2]), P.slope};
     double tmp_e = 0, best_e = kMaxFl;
     int count = 0;
     if (w.lane == 0) *ch.out_count = 0;
@@ -415,16 +447,16 @@ __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCPara
         copyd(w, cand, tmp, cs);
         mutate32(w, rng, cand, P.amplitude);
         SG_T1(t_mut, 6);
-        const double cand_e = bfgs32(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt);
+        const double cand_e = bfgs32(w, cand_at, ch.maxiters, P.accurate_line, P.early_term, hunt);
         bool accept = step == 0 || cand_e < tmp_e;
         if (!accept) accept = ph_u01(rng) < exp((tmp_e - cand_e) / P.temperature);
         if (accept) {
             copyd(w, tmp, cand, cs);
             tmp_e = cand_e;
-            set_conf32(w, tmp);
+            set_conf32(w, tmp_at);
             if (tmp_e < best_e || count < P.num_saved) {
-                tmp_e = bfgs32(w, tmp, ch.maxiters, P.accurate_line, P.early_term, auth);
-                set_conf32(w, tmp);
+                tmp_e = bfgs32(w, tmp_at, ch.maxiters, P.accurate_line, P.early_term, auth);
+                set_conf32(w, tmp_at);
                 count = add_output32(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved, count);
                 if (tmp_e < best_e) best_e = tmp_e;
             }
@@ -444,55 +476,51 @@ __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCPara
     SG_T1(t_chain, 7);
 }
 
-// Copies a model's descriptor and the arrays the search reads into the
-// block's shared memory; every thread of the block takes part.  Arrays that
-// are read once per chain (lab32, finit32) or only for trees of more than
-// 32 frames (levels) stay in global memory.
+// Copies a model's counts and the arrays the search reads into smem32 at
+// offset 0 (an SModel, then the arrays); every thread of the block takes
+// part.  Ends with a block barrier.
 template <typename T>
-__device__ __forceinline__ const T* stage_arr(const T* src, int n, char*& o, int tid, int nthr) {
-    T* d = reinterpret_cast<T*>(o);
+__device__ __forceinline__ int stage_arr(const T* src, int n, int& o, int tid, int nthr) {
+    const int at = o;
+    T* d = sp<T>(at);
     o += (n * (int)sizeof(T) + 15) & ~15;
     for (int i = tid; i < n; i += nthr) d[i] = src[i];
-    return d;
+    return at;
 }
 
-__device__ void stage_model(const DModel* gm, char* dst, int tid, int nthr) {
-    const int4* src = reinterpret_cast<const int4*>(gm);
-    for (int i = tid; i < (int)(sizeof(DModel) / 16); i += nthr) reinterpret_cast<int4*>(dst)[i] = src[i];
-    const DModel g = *gm;
-    char* o = dst + (((int)sizeof(DModel) + 15) & ~15);
-    DModel* d = reinterpret_cast<DModel*>(dst);
-    const float4* local32 = stage_arr(g.local32, g.natoms, o, tid, nthr);
-    const int* type = stage_arr(g.type, g.natoms, o, tid, nthr);
-    const int* atom_frame = stage_arr(g.atom_frame, g.natoms, o, tid, nthr);
-    const float4* forigin32 = stage_arr(g.forigin32, g.nframes, o, tid, nthr);
-    const float4* faxis32 = stage_arr(g.faxis32, g.nframes, o, tid, nthr);
-    const int* fkind = stage_arr(g.fkind, g.nframes, o, tid, nthr);
-    const int* fparent = stage_arr(g.fparent, g.nframes, o, tid, nthr);
-    const int* fbegin = stage_arr(g.fbegin, g.nframes, o, tid, nthr);
-    const int* fsub_end = stage_arr(g.fsub_end, g.nframes, o, tid, nthr);
-    const int* fconf = stage_arr(g.fconf, g.nframes, o, tid, nthr);
-    const int* fdof = stage_arr(g.fdof, g.nframes, o, tid, nthr);
-    const int* heavy = stage_arr(g.heavy, g.nheavy, o, tid, nthr);
-    const uint32_t* pslot = stage_arr(g.pslot, 32 * g.npchunks, o, tid, nthr);
-    const int* lig_root = stage_arr(g.lig_root, g.nlig, o, tid, nthr);
-    const int* lig_begin = stage_arr(g.lig_begin, g.nlig, o, tid, nthr);
-    const int* lig_end = stage_arr(g.lig_end, g.nlig, o, tid, nthr);
-    const int* blk_rigid = stage_arr(g.blk_rigid, g.nblocks, o, tid, nthr);
-    const int* blk_conf = stage_arr(g.blk_conf, g.nblocks, o, tid, nthr);
-    const int* blk_ntors = stage_arr(g.blk_ntors, g.nblocks, o, tid, nthr);
-    const int* tor_conf = stage_arr(g.tor_conf, g.ntors, o, tid, nthr);
-    const int* tor_dof = stage_arr(g.tor_dof, g.ntors, o, tid, nthr);
-    __syncthreads();  // descriptor copied
-    if (tid == 0) {
-        d->local32 = local32; d->type = type; d->atom_frame = atom_frame;
-        d->forigin32 = forigin32; d->faxis32 = faxis32;
-        d->fkind = fkind; d->fparent = fparent; d->fbegin = fbegin; d->fsub_end = fsub_end;
-        d->fconf = fconf; d->fdof = fdof; d->heavy = heavy; d->pslot = pslot;
-        d->lig_root = lig_root; d->lig_begin = lig_begin; d->lig_end = lig_end;
-        d->blk_rigid = blk_rigid; d->blk_conf = blk_conf; d->blk_ntors = blk_ntors;
-        d->tor_conf = tor_conf; d->tor_dof = tor_dof;
-    }
+__device__ void stage_model(const DModel* gm, int tid, int nthr) {
+    const DModel& g = *gm;
+    int o = ((int)sizeof(SModel) + 15) & ~15;
+    SModel s;
+    s.natoms = g.natoms; s.nmov = g.nmov; s.nframes = g.nframes; s.nlig = g.nlig; s.conf_size = g.conf_size;
+    s.dof = g.dof; s.nheavy = g.nheavy; s.nlevels = g.nlevels; s.nblocks = g.nblocks; s.ntors = g.ntors;
+    s.npchunks = g.npchunks;
+    s.local32 = stage_arr(g.local32, g.natoms, o, tid, nthr);
+    s.type = stage_arr(g.type, g.natoms, o, tid, nthr);
+    s.atom_frame = stage_arr(g.atom_frame, g.natoms, o, tid, nthr);
+    s.forigin32 = stage_arr(g.forigin32, g.nframes, o, tid, nthr);
+    s.faxis32 = stage_arr(g.faxis32, g.nframes, o, tid, nthr);
+    s.fkind = stage_arr(g.fkind, g.nframes, o, tid, nthr);
+    s.fparent = stage_arr(g.fparent, g.nframes, o, tid, nthr);
+    s.fbegin = stage_arr(g.fbegin, g.nframes, o, tid, nthr);
+    s.fsub_end = stage_arr(g.fsub_end, g.nframes, o, tid, nthr);
+    s.fconf = stage_arr(g.fconf, g.nframes, o, tid, nthr);
+    s.fdof = stage_arr(g.fdof, g.nframes, o, tid, nthr);
+    s.heavy = stage_arr(g.heavy, g.nheavy, o, tid, nthr);
+    s.pslot = stage_arr(g.pslot, 32 * g.npchunks, o, tid, nthr);
+    s.lig_root = stage_arr(g.lig_root, g.nlig, o, tid, nthr);
+    s.lig_begin = stage_arr(g.lig_begin, g.nlig, o, tid, nthr);
+    s.lig_end = stage_arr(g.lig_end, g.nlig, o, tid, nthr);
+    s.blk_rigid = stage_arr(g.blk_rigid, g.nblocks, o, tid, nthr);
+    s.blk_conf = stage_arr(g.blk_conf, g.nblocks, o, tid, nthr);
+    s.blk_ntors = stage_arr(g.blk_ntors, g.nblocks, o, tid, nthr);
+    s.tor_conf = stage_arr(g.tor_conf, g.ntors, o, tid, nthr);
+    s.tor_dof = stage_arr(g.tor_dof, g.ntors, o, tid, nthr);
+    s.lab32 = g.lab32;
+    s.finit32 = g.finit32;
+    s.level_start = g.level_start;
+    s.level_frames = g.level_frames;
+    if (tid == 0) *sp<SModel>(0) = s;
     __syncthreads();
 }
 
@@ -508,28 +536,22 @@ __global__ void __launch_bounds__(256, SG_MC32_MINB) k_mc32(const DModel* models
                                                             const Chain32* chains, const Item32* items, int nitems,
                                                             MCParams32 P, unsigned* queue, int stage_stride,
                                                             int ws_stride) {
-    __shared__ DTables32 sT;
-    __shared__ DMaps32 sG;
     __shared__ int s_item;
-    extern __shared__ __align__(16) char smem32[];
     const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
-    if (tid == 0) { sT = T; sG = G; }
+    if (tid == 0) { sT32 = T; sG32 = G; }
     W32 w;
-    w.s = smem32 + stage_stride + (size_t)warp * ws_stride;
-    w.T = &sT;
-    w.G = &sG;
+    w.ws = stage_stride + warp * ws_stride;
     w.lane = tid & 31;
-    w.m = reinterpret_cast<const DModel*>(smem32);
     for (;;) {
         if (tid == 0) s_item = (int)atomicAdd(queue, 1u);
         __syncthreads();
         const int it = s_item;
         if (it >= nitems) break;
         const Item32 item = items[it];
-        stage_model(models + item.model, smem32, tid, nthr);
+        stage_model(models + item.model, tid, nthr);
         if (warp < item.count) {
             const Chain32 ch = chains[item.first + warp];
-            const DModel& m = *w.m;
+            const SModel& m = smodel();
             w.L = ws32_layout(m.natoms, m.nframes, m.conf_size, m.dof);
             w.evals = 0;
             w.grid_hits = 0;
@@ -540,33 +562,27 @@ __global__ void __launch_bounds__(256, SG_MC32_MINB) k_mc32(const DModel* models
     }
 }
 
-// model::eval_deriv in FP32 for a batch of confs of one model (one warp per conf)
+// model::eval_deriv in FP32 for a batch of confs of one model (one warp per
+// conf); the model is staged like the search kernel's, the workspace
+// follows it at ws_at
 __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T, DMaps32 G, int n, const double* confs,
                                                float v0, float v1, float v2, float slope, double* out_e, double* out_g,
-                                               double* out_coords) {
-    __shared__ DTables32 sT;
-    __shared__ DMaps32 sG;
-    extern __shared__ __align__(16) char smem32[];
+                                               double* out_coords, int ws_at) {
     const int k = blockIdx.x;
     if (k >= n) return;
-    if (threadIdx.x == 0) { sT = T; sG = G; }
-    __syncthreads();
+    if (threadIdx.x == 0) { sT32 = T; sG32 = G; }
+    stage_model(model, threadIdx.x, 32);
     W32 w;
-    w.s = smem32;
-    w.T = &sT;
-    w.G = &sG;
+    w.ws = ws_at;
     w.lane = threadIdx.x & 31;
     w.evals = 0;
     w.grid_hits = 0;
     w.pair_hits = 0;
-    w.L = ws32_layout(model->natoms, model->nframes, model->conf_size, model->dof);
-    w.m = model;
-    const DModel& m = *w.m;
-    double* x = w.d(w.L.x_tmp);
-    copyd(w, x, confs + (size_t)k * m.conf_size, m.conf_size);
-    double* g = w.d(w.L.g);
-    const float v[3] = {v0, v1, v2};
-    const float e = eval_deriv32(w, x, v, slope, g);
+    const SModel& m = smodel();
+    w.L = ws32_layout(m.natoms, m.nframes, m.conf_size, m.dof);
+    copyd(w, w.d(w.L.x_tmp), confs + (size_t)k * m.conf_size, m.conf_size);
+    const float e = eval_deriv32(w, w.at(w.L.x_tmp), make_float3(v0, v1, v2), slope, w.at(w.L.g));
+    const double* g = w.d(w.L.g);
     if (w.lane == 0) out_e[k] = e;
     for (int i = w.lane; i < m.dof; i += 32) out_g[(size_t)k * m.dof + i] = g[i];
     if (out_coords)
@@ -605,11 +621,14 @@ cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G,
     return cudaGetLastError();
 }
 
-cudaError_t launch_eval32(const DModel* dm, size_t ws, const DTables32& T, const DMaps32& G, int n, const double* confs,
-                          const double v[3], double slope, double* e, double* g, double* coords, cudaStream_t s) {
-    cudaError_t rc = prep32((const void*)k_eval32, ws);
+cudaError_t launch_eval32(const DModel* dm, size_t stage, size_t ws, const DTables32& T, const DMaps32& G, int n,
+                          const double* confs, const double v[3], double slope, double* e, double* g, double* coords,
+                          cudaStream_t s) {
+    const size_t smem = stage + ws;
+    cudaError_t rc = prep32((const void*)k_eval32, smem);
     if (rc != cudaSuccess) return rc;
-    k_eval32<<<n, 32, ws, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, e, g, coords);
+    k_eval32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, e, g, coords,
+                                 (int)stage);
     return cudaGetLastError();
 }
 

@@ -153,11 +153,24 @@ struct Item32 {
     int model, first, count;
 };
 
-// Bytes of the block-shared copy of a model (descriptor + the arrays the
-// mixed-precision search reads), 16 B aligned pieces
+// The block-shared copy of a model for the mixed-precision kernels: counts,
+// then the byte offsets (in the kernel's dynamic shared memory) of the
+// arrays the search reads.  Arrays read once per chain or only for trees
+// of more than 32 frames stay in global memory.
+struct SModel {
+    int natoms, nmov, nframes, nlig, conf_size, dof, nheavy, nlevels, nblocks, ntors, npchunks;
+    int local32, type, atom_frame, forigin32, faxis32, fkind, fparent, fbegin, fsub_end, fconf, fdof, heavy, pslot,
+        lig_root, lig_begin, lig_end, blk_rigid, blk_conf, blk_ntors, tor_conf, tor_dof;
+    const float4* lab32;
+    const float4* finit32;
+    const int* level_start;
+    const int* level_frames;
+};
+
+// Bytes of the staged model (SModel + arrays), 16 B aligned pieces
 SG_HD int stage32_bytes(int natoms, int nframes, int nheavy, int npchunks, int nlig, int nblocks, int ntors) {
     auto r = [](int b) { return (b + 15) & ~15; };
-    return r((int)sizeof(DModel)) + r(16 * natoms) + 2 * r(4 * natoms) + 2 * r(16 * nframes) + 6 * r(4 * nframes) +
+    return r((int)sizeof(SModel)) + r(16 * natoms) + 2 * r(4 * natoms) + 2 * r(16 * nframes) + 6 * r(4 * nframes) +
            r(4 * nheavy) + r(128 * npchunks) + 3 * r(4 * nlig) + 3 * r(4 * nblocks) + 2 * r(4 * ntors);
 }
 
