@@ -13,10 +13,15 @@ namespace sg {
 
 constexpr unsigned kFull32 = 0xffffffffu;
 
+#ifndef SG_PAIR_CHUNKS
+#define SG_PAIR_CHUNKS 2  // pair chunks (of 32) whose table loads are in flight together
+#endif
+
 // Section timers (compile with -DSG_PROFILE): lane 0 of every warp adds
 // clock64() spans per section; sg_profile_read() copies them out.
 // Sections: 0 set_conf, 1 grid, 2 pairs, 3 derivative, 4 line-search
-// bookkeeping, 5 BFGS algebra, 6 mutation, 7 whole chain.
+// bookkeeping, 5 BFGS algebra, 6 mutation, 7 whole chain, 8 wait at the
+// block barrier after a work item.
 #ifdef SG_PROFILE
 __device__ unsigned long long g_prof[16];
 #define SG_T0(name) const long long name = clock64()
@@ -40,42 +45,6 @@ __device__ __forceinline__ T* sp(int off) {
     return reinterpret_cast<T*>(smem32 + off);
 }
 __device__ __forceinline__ const SModel& smodel() { return *reinterpret_cast<const SModel*>(smem32); }
-
-// per-warp workspace (bytes, 16 B aligned)
-struct Ws32 {
-    int coords, force, origin, axis, quat, rot;                  // float4 arrays (rot: 3 rows per frame)
-    int x_tmp, x_cand, x_new, x_orig, g, g_new, g_orig, p, y, mhy, h;  // double arrays (h: n x n)
-    int pf, pc;                                                  // prefix sums over atoms (float4)
-    int scratch;                                                 // 64 floats
-    int total;
-};
-SG_HD Ws32 ws32_layout(int natoms, int nframes, int conf, int dof) {
-    Ws32 w;
-    int o = 0;
-    auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
-    w.coords = take(16 * natoms);
-    w.force = take(16 * natoms);
-    w.origin = take(16 * nframes);
-    w.axis = take(16 * nframes);
-    w.quat = take(16 * nframes);
-    w.rot = take(48 * nframes);
-    w.x_tmp = take(8 * conf);
-    w.x_cand = take(8 * conf);
-    w.x_new = take(8 * conf);
-    w.x_orig = take(8 * conf);
-    w.g = take(8 * dof);
-    w.g_new = take(8 * dof);
-    w.g_orig = take(8 * dof);
-    w.p = take(8 * dof);
-    w.y = take(8 * dof);
-    w.mhy = take(8 * dof);
-    w.h = take(8 * dof * dof);
-    w.pf = take(16 * (natoms + 1));
-    w.pc = take(16 * (natoms + 1));
-    w.scratch = take(4 * 64);
-    w.total = o;
-    return w;
-}
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw 2011) -------------------------------
 struct Philox {
@@ -110,23 +79,27 @@ __device__ __forceinline__ double ph_normal(Philox& r) {  // Box-Muller
     return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
 }
 
-// One warp's view of its chain: its workspace offset and layout, its lane,
-// and its work counters.
+// This warp's workspace: its byte offset in smem32 and the lane.  The
+// layout is the block's (SModel::L).  Every function builds it on the spot
+// from threadIdx and two block constants, so it lives in registers.
+__shared__ int sWs0, sWsStride;  // first warp's workspace offset, stride between warps
 struct W32 {
-    int ws;  // byte offset of this warp's workspace in smem32
-    Ws32 L;
-    int lane;
-    unsigned long long evals;
-    unsigned long long grid_hits, pair_hits;  // per-lane gather counts (algorithmic bytes)
+    int ws, lane;
     __device__ int at(int field) const { return ws + field; }  // smem32 offset of a workspace array
-    __device__ float4* coords() const { return sp<float4>(ws + L.coords); }
-    __device__ float4* force() const { return sp<float4>(ws + L.force); }
-    __device__ float4* origin() const { return sp<float4>(ws + L.origin); }
-    __device__ float4* axis() const { return sp<float4>(ws + L.axis); }
-    __device__ float4* quat() const { return sp<float4>(ws + L.quat); }
-    __device__ float4* rot() const { return sp<float4>(ws + L.rot); }
+    __device__ float4* coords() const { return sp<float4>(ws + smodel().L.coords); }
+    __device__ float4* force() const { return sp<float4>(ws + smodel().L.force); }
+    __device__ float4* origin() const { return sp<float4>(ws + smodel().L.origin); }
+    __device__ float4* axis() const { return sp<float4>(ws + smodel().L.axis); }
+    __device__ float4* quat() const { return sp<float4>(ws + smodel().L.quat); }
+    __device__ float4* rot() const { return sp<float4>(ws + smodel().L.rot); }
     __device__ double* d(int field) const { return sp<double>(ws + field); }
+    // work counters: grid lookups per lane [0, 32), in-cutoff pair lookups
+    // per lane [32, 64), evaluations [64]
+    __device__ unsigned* counters() const { return sp<unsigned>(ws + smodel().L.scratch); }
 };
+__device__ __forceinline__ W32 here() {
+    return W32{sWs0 + (int)(threadIdx.x >> 5) * sWsStride, (int)(threadIdx.x & 31)};
+}
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -186,7 +159,8 @@ __device__ __forceinline__ float warp_sum(float v) {
 // need no parent data; the lab transforms are their ordered compositions
 // along the path to the root, done by pointer jumping in log2(depth) warp
 // shuffles.  Trees of more than 32 frames go level by level.
-__device__ __noinline__ void set_conf32(W32& w, int conf_at) {
+__device__ __noinline__ void set_conf32(int conf_at) {
+    const W32 w = here();
     const SModel& m = smodel();
     const double* conf = sp<const double>(conf_at);
     const int nframes = m.nframes, nmov = m.nmov;
@@ -336,8 +310,9 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
     return f + penalty;
 }
 
-// table lookup with charge-weighted components (precalculate_linear element eval_deriv)
-__device__ __forceinline__ void table32_nc(const DTables32& T, int p, bool swap, float qa, float qb, float r2, float& e,
+// table lookup with charge-weighted components (precalculate_linear element
+// eval_deriv); out of line, charge-dependent scoring only
+__device__ __noinline__ void table32_nc(const DTables32& T, int p, bool swap, float qa, float qb, float r2, float& e,
                                            float& dor) {
     if (swap) { const float t = qa; qa = qb; qb = t; }
     const float rf = T.factor * r2;
@@ -353,16 +328,18 @@ __device__ __forceinline__ void table32_nc(const DTables32& T, int p, bool swap,
 }
 
 // model::eval_deriv in FP32; returns the energy (same on every lane), writes g (FP64)
-__device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float slope, int g_at) {
+__device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, int g_at) {
+    const W32 w = here();
     const SModel& m = smodel();
     double* g = sp<double>(g_at);
     SG_T0(t_set);
-    set_conf32(w, conf_at);
+    set_conf32(conf_at);
     SG_T1(t_set, 0);
     SG_T0(t_grid);
     float4* X = w.coords();
     float4* Fz = w.force();
     float e = 0;
+    unsigned ghits = 0;
     // grid part; every movable atom gets its force reset (hydrogens: zero)
     const int nmov = m.nmov;
     const int* TYPE = sp<const int>(m.type);
@@ -373,13 +350,13 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
         if (t < kNumTypes && !is_h(t)) {
             const float3 loc = f3(X[i]);
             e += grid_aux32(sG32, t, false, loc, slope, v.y, d);
-            w.grid_hits++;
+            ghits++;
             const float q = LQ[i].w;
             if (q != 0.f && sG32.c32[t]) {
                 float3 cd;
                 e += q * grid_aux32(sG32, t, true, loc, slope, v.y, cd);
                 d = d + q * cd;
-                w.grid_hits++;
+                ghits++;
             }
         }
         Fz[i] = make_float4(d.x, d.y, d.z, 0);
@@ -387,45 +364,45 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
     __syncwarp();
     SG_T1(t_grid, 1);
     SG_T0(t_pairs);
-    // Pairs: intramolecular (v[0]) and other (v[2]), two chunks of 32 in
-    // flight.  Within a chunk no atom is twice a first atom or twice a
+    // Pairs: intramolecular (v[0]) and other (v[2]), SG_PAIR_CHUNKS chunks
+    // of 32 in flight.  Within a chunk no atom is twice a first atom or twice a
     // second atom, so the force updates are plain read-add-writes: first
     // atoms, sync, second atoms, sync.
     const int nch = m.npchunks;
     const uint32_t* PS = sp<const uint32_t>(m.pslot);
     const DTables32 T = sT32;
     const int lane = w.lane;
-    unsigned long long hits = 0;
-    for (int c = 0; c < nch; c += 2) {
-        const bool two = c + 1 < nch;
-        uint32_t sl[2];
-        int ia[2], ib[2];
-        float3 r[2];
-        float r2[2];
-        bool ok[2];
+    unsigned hits = 0;
+    for (int c = 0; c < nch; c += SG_PAIR_CHUNKS) {
+        const int live = min(SG_PAIR_CHUNKS, nch - c);  // chunks this round (warp-uniform)
+        uint32_t sl[SG_PAIR_CHUNKS];
+        int ia[SG_PAIR_CHUNKS], ib[SG_PAIR_CHUNKS];
+        float3 r[SG_PAIR_CHUNKS];
+        float r2[SG_PAIR_CHUNKS];
+        bool ok[SG_PAIR_CHUNKS];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            sl[u] = (u == 0 || two) ? PS[(c + u) * 32 + lane] : kSlotEmpty;
+        for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
+            sl[u] = u < live ? PS[(c + u) * 32 + lane] : kSlotEmpty;
             ia[u] = sl[u] & 0xff;
             ib[u] = (sl[u] >> 8) & 0xff;
             r[u] = f3(X[ib[u]]) - f3(X[ia[u]]);
             r2[u] = dot3(r[u], r[u]);
             ok[u] = sl[u] != kSlotEmpty && r2[u] < T.cutoff_sqr;
         }
-        float4 tv[2];
-        float rem[2];
-        if (T.nc == 1) {  // issue both table loads before using either
+        float4 tv[SG_PAIR_CHUNKS];
+        float rem[SG_PAIR_CHUNKS];
+        if (T.nc == 1) {  // issue every table load before using any
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
                 const float rf = T.factor * r2[u];
                 const int i1 = ok[u] ? (int)rf : 0;
                 rem[u] = rf - (float)i1;
                 tv[u] = ok[u] ? __ldg(T.tab + ((size_t)((sl[u] >> 16) & 0x1ff) * T.n + i1)) : make_float4(0, 0, 0, 0);
             }
         }
-        float3 f[2];
+        float3 f[SG_PAIR_CHUNKS];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
             f[u] = make_float3(0, 0, 0);
             if (!ok[u]) continue;
             float pe, dor;
@@ -446,8 +423,8 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
             hits++;
         }
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            if (u == 1 && !two) break;
+        for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
+            if (u >= live) break;
             if (ok[u]) {
                 float4 t = Fz[ia[u]];
                 t.x -= f[u].x; t.y -= f[u].y; t.z -= f[u].z;
@@ -462,7 +439,6 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
             __syncwarp();
         }
     }
-    w.pair_hits += hits;
     e = warp_sum(e);
     __syncwarp();
     SG_T1(t_pairs, 2);
@@ -473,8 +449,8 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
     // c_i = (x_i - o_ref) x F_i, T_sub = PC[E] - PC[b] - (o_f - o_ref) x F_sub.
     // Torques are taken about the first root's origin to keep them small.
     float4* O = w.origin();
-    float4* PF = sp<float4>(w.at(w.L.pf));
-    float4* PC = sp<float4>(w.at(w.L.pc));
+    float4* PF = sp<float4>(w.at(m.L.pf));
+    float4* PC = sp<float4>(w.at(m.L.pc));
     const float3 oref = f3(O[0]);
     float3 cf = make_float3(0, 0, 0), cc = make_float3(0, 0, 0);
     for (int base = 0; base < nmov; base += 32) {
@@ -526,7 +502,10 @@ __device__ __noinline__ float eval_deriv32(W32& w, int conf_at, float3 v, float 
     }
     __syncwarp();
     SG_T1(t_der, 3);
-    w.evals++;
+    unsigned* C = w.counters();
+    C[w.lane] += ghits;
+    C[32 + w.lane] += hits;
+    if (w.lane == 0) C[64] += 1;
     return e;
 }
 

@@ -33,22 +33,32 @@ __device__ __forceinline__ void copyd(const W32& w, double* d, const double* s, 
     __syncwarp();
 }
 
+// normalize_angle for the mixed-precision path: the nearest multiple of
+// 2 pi is subtracted in one step (same interval as common.h's loop, not
+// its rounding)
+__device__ __forceinline__ double wrap_pi(double x) {
+    return x - (2 * kPi) * rint(x * (1.0 / (2 * kPi)));
+}
+
 // quaternion_increment (quaternion.cpp:118-126) with an FP32 sine/cosine of
 // the half angle, composed and re-normalised in FP64
 __device__ __forceinline__ void q_increment32(double* c, double rx, double ry, double rz) {
-    const double ang = sqrt(rx * rx + ry * ry + rz * rz);
+    const double a2 = rx * rx + ry * ry + rz * rz;
     double s = 0, co = 1;
-    if (ang > kEps) {
-        double a = ang;
-        normalize_angle(a);
+    if (a2 > kEps * kEps) {  // angle > epsilon
+        const double inv = rsqrt(a2);
         float sf, cf;
-        sincosf((float)(0.5 * a), &sf, &cf);
-        s = (double)sf / ang;
+        sincosf((float)(0.5 * wrap_pi(a2 * inv)), &sf, &cf);
+        s = (double)sf * inv;
         co = (double)cf;
     }
     Quat<double> q{c[0], c[1], c[2], c[3]};
     q = qmul(Quat<double>{co, s * rx, s * ry, s * rz}, q);
-    q_normalize_approx(q);
+    const double n2 = q.a * q.a + q.b * q.b + q.c * q.c + q.d * q.d;
+    if (fabs(n2 - 1) >= 1e-6) {  // quaternion_normalize_approx
+        const double inv = rsqrt(n2);
+        q.a *= inv; q.b *= inv; q.c *= inv; q.d *= inv;
+    }
     c[0] = q.a; c[1] = q.b; c[2] = q.c; c[3] = q.d;
 }
 
@@ -69,8 +79,7 @@ __device__ __forceinline__ void increment32(const W32& w, double* x, const doubl
     }
     for (int k = w.lane; k < m.ntors; k += 32) {
         double& t = x[tor_conf[k]];
-        t += normalized_angle(alpha * p[tor_dof[k]]);
-        normalize_angle(t);
+        t = wrap_pi(t + wrap_pi(alpha * p[tor_dof[k]]));
     }
     __syncwarp();
 }
@@ -105,13 +114,13 @@ struct Mode32 {
 };
 
 // energy and gradient of the conf at smem32 offset x_at (gradient to g_at)
-__device__ __forceinline__ double feval32(W32& w, int x_at, int g_at, const Mode32& em) {
-    return (double)eval_deriv32(w, x_at, em.v, em.slope, g_at);
+__device__ __forceinline__ double feval32(int x_at, int g_at, const Mode32& em) {
+    return (double)eval_deriv32(x_at, em.v, em.slope, g_at);
 }
 
 // ---- line searches (bfgs.h:30-200) ------------------------------------------------------
 // x, g, p, x_new, g_new: offsets of this warp's workspace arrays in smem32
-__device__ __forceinline__ double line_fast32(W32& w, int x_at, int g_at, double f0, int p_at, int xn_at, int gn_at,
+__device__ __forceinline__ double line_fast32(const W32& w, int x_at, int g_at, double f0, int p_at, int xn_at, int gn_at,
                                               double& f1, const Mode32& em) {
     const SModel& m = smodel();
     const double* x = sp<const double>(x_at);
@@ -124,14 +133,14 @@ __device__ __forceinline__ double line_fast32(W32& w, int x_at, int g_at, double
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
         SG_T1(t_ls, 4);
-        f1 = feval32(w, xn_at, gn_at, em);
+        f1 = feval32(xn_at, gn_at, em);
         if (f1 - f0 < 0.0001 * alpha * pg) break;
         alpha *= 0.5;
     }
     return alpha;
 }
 
-__device__ __forceinline__ double line_accurate32(W32& w, int x_at, int g_at, double f0, int p_at, int xn_at,
+__device__ __noinline__ double line_accurate32(const W32& w, int x_at, int g_at, double f0, int p_at, int xn_at,
                                                   int gn_at, double& f1, const Mode32& em) {
     const SModel& m = smodel();
     const int n = m.dof;
@@ -158,7 +167,7 @@ __device__ __forceinline__ double line_accurate32(W32& w, int x_at, int g_at, do
     for (int it = 0; it < 128; it++) {
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
-        f1 = feval32(w, xn_at, gn_at, em);
+        f1 = feval32(xn_at, gn_at, em);
         if (alpha < alamin) return give_up();
         if (f1 <= f0 + ALF * alpha * slope) return alpha;
         if (alpha == FIRST) {
@@ -190,18 +199,20 @@ __device__ __forceinline__ double line_accurate32(W32& w, int x_at, int g_at, do
 // a row sweep read consecutive words.  Every entry (i, j) is computed from
 // (min(i, j), max(i, j)) operands in one fixed order, so h stays exactly
 // symmetric.  x_at: smem32 offset of the conf, optimised in place.
-__device__ __noinline__ double bfgs32(W32& w, int x_at, int maxiters, int accurate, int early, const Mode32& em) {
+__device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int early, const Mode32& em) {
+    const W32 w = here();
     const SModel& m = smodel();
+    const Ws32& L = m.L;
     const int n = m.dof, cs = m.conf_size;
-    const int g_at = w.at(w.L.g), gn_at = w.at(w.L.g_new), p_at = w.at(w.L.p), xn_at = w.at(w.L.x_new);
+    const int g_at = w.at(L.g), gn_at = w.at(L.g_new), p_at = w.at(L.p), xn_at = w.at(L.x_new);
     double* x = sp<double>(x_at);
-    double* h = w.d(w.L.h);
-    double *g = sp<double>(g_at), *g_new = sp<double>(gn_at), *g_orig = w.d(w.L.g_orig), *p = sp<double>(p_at);
-    double *y = w.d(w.L.y), *x_new = sp<double>(xn_at), *x_orig = w.d(w.L.x_orig), *mhy = w.d(w.L.mhy);
+    double* h = w.d(L.h);
+    double *g = sp<double>(g_at), *g_new = sp<double>(gn_at), *g_orig = w.d(L.g_orig), *p = sp<double>(p_at);
+    double *y = w.d(L.y), *x_new = sp<double>(xn_at), *x_orig = w.d(L.x_orig), *mhy = w.d(L.mhy);
     for (int i = w.lane; i < n; i += 32)
         for (int j = 0; j < n; j++) h[j * n + i] = (i == j) ? 1.0 : 0.0;
     __syncwarp();
-    double f0 = feval32(w, x_at, g_at, em);
+    double f0 = feval32(x_at, g_at, em);
     const double f_orig = f0;
     copyd(w, g_orig, g, n);
     copyd(w, x_orig, x, cs);
@@ -424,16 +435,20 @@ __device__ __forceinline__ int add_output32(const W32& w, const Chain32& ch, con
 }
 
 // monte_carlo::operator() for one chain
-__device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCParams32& P) {
+__device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P) {
     SG_T0(t_chain);
+    const W32 w = here();
     const SModel& m = smodel();
+    const Ws32& L = m.L;
+    unsigned* C = w.counters();
+    for (int i = w.lane; i < 65; i += 32) C[i] = 0;
     const int cs = m.conf_size;
     // model state as read (mutation may read it before the first set)
     for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);
     for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
     __syncwarp();
     Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
-    const int tmp_at = w.at(w.L.x_tmp), cand_at = w.at(w.L.x_cand);
+    const int tmp_at = w.at(L.x_tmp), cand_at = w.at(L.x_cand);
     double* tmp = sp<double>(tmp_at);
     double* cand = sp<double>(cand_at);
     randomize32(w, rng, tmp, P);
@@ -447,28 +462,29 @@ __device__ __noinline__ void run_chain32(W32& w, const Chain32& ch, const MCPara
         copyd(w, cand, tmp, cs);
         mutate32(w, rng, cand, P.amplitude);
         SG_T1(t_mut, 6);
-        const double cand_e = bfgs32(w, cand_at, ch.maxiters, P.accurate_line, P.early_term, hunt);
+        const double cand_e = bfgs32(cand_at, ch.maxiters, P.accurate_line, P.early_term, hunt);
         bool accept = step == 0 || cand_e < tmp_e;
         if (!accept) accept = ph_u01(rng) < exp((tmp_e - cand_e) / P.temperature);
         if (accept) {
             copyd(w, tmp, cand, cs);
             tmp_e = cand_e;
-            set_conf32(w, tmp_at);
+            set_conf32(tmp_at);
             if (tmp_e < best_e || count < P.num_saved) {
-                tmp_e = bfgs32(w, tmp_at, ch.maxiters, P.accurate_line, P.early_term, auth);
-                set_conf32(w, tmp_at);
+                tmp_e = bfgs32(tmp_at, ch.maxiters, P.accurate_line, P.early_term, auth);
+                set_conf32(tmp_at);
                 count = add_output32(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved, count);
                 if (tmp_e < best_e) best_e = tmp_e;
             }
         }
     }
-    unsigned long long gh = w.grid_hits, ph = w.pair_hits;
+    __syncwarp();
+    unsigned long long gh = C[w.lane], ph = C[32 + w.lane];
     for (int o = 16; o > 0; o >>= 1) {
         gh += __shfl_xor_sync(kFull32, gh, o);
         ph += __shfl_xor_sync(kFull32, ph, o);
     }
     if (w.lane == 0) {
-        *ch.evals = w.evals;
+        *ch.evals = C[64];
         ch.hits[0] = gh;
         ch.hits[1] = ph;
     }
@@ -520,6 +536,7 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
     s.finit32 = g.finit32;
     s.level_start = g.level_start;
     s.level_frames = g.level_frames;
+    s.L = ws32_layout(g.natoms, g.nframes, g.conf_size, g.dof);
     if (tid == 0) *sp<SModel>(0) = s;
     __syncthreads();
 }
@@ -532,16 +549,16 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
 #ifndef SG_MC32_MINB
 #define SG_MC32_MINB 2
 #endif
-__global__ void __launch_bounds__(256, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
+#ifndef SG_MC32_THREADS
+#define SG_MC32_THREADS 256
+#endif
+__global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
                                                             const Chain32* chains, const Item32* items, int nitems,
                                                             MCParams32 P, unsigned* queue, int stage_stride,
                                                             int ws_stride) {
     __shared__ int s_item;
     const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
-    if (tid == 0) { sT32 = T; sG32 = G; }
-    W32 w;
-    w.ws = stage_stride + warp * ws_stride;
-    w.lane = tid & 31;
+    if (tid == 0) { sT32 = T; sG32 = G; sWs0 = stage_stride; sWsStride = ws_stride; }
     for (;;) {
         if (tid == 0) s_item = (int)atomicAdd(queue, 1u);
         __syncthreads();
@@ -551,14 +568,11 @@ __global__ void __launch_bounds__(256, SG_MC32_MINB) k_mc32(const DModel* models
         stage_model(models + item.model, tid, nthr);
         if (warp < item.count) {
             const Chain32 ch = chains[item.first + warp];
-            const SModel& m = smodel();
-            w.L = ws32_layout(m.natoms, m.nframes, m.conf_size, m.dof);
-            w.evals = 0;
-            w.grid_hits = 0;
-            w.pair_hits = 0;
-            run_chain32(w, ch, P);
+            run_chain32(ch, P);
         }
+        SG_T0(t_bar);
         __syncthreads();  // the staged model is in use until every warp is done
+        SG_T1(t_bar, 8);
     }
 }
 
@@ -570,19 +584,16 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
                                                double* out_coords, int ws_at) {
     const int k = blockIdx.x;
     if (k >= n) return;
-    if (threadIdx.x == 0) { sT32 = T; sG32 = G; }
+    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = 0; }
     stage_model(model, threadIdx.x, 32);
-    W32 w;
-    w.ws = ws_at;
-    w.lane = threadIdx.x & 31;
-    w.evals = 0;
-    w.grid_hits = 0;
-    w.pair_hits = 0;
+    const W32 w = here();
     const SModel& m = smodel();
-    w.L = ws32_layout(m.natoms, m.nframes, m.conf_size, m.dof);
-    copyd(w, w.d(w.L.x_tmp), confs + (size_t)k * m.conf_size, m.conf_size);
-    const float e = eval_deriv32(w, w.at(w.L.x_tmp), make_float3(v0, v1, v2), slope, w.at(w.L.g));
-    const double* g = w.d(w.L.g);
+    const Ws32& L = m.L;
+    unsigned* C = w.counters();
+    for (int i = w.lane; i < 65; i += 32) C[i] = 0;
+    copyd(w, w.d(L.x_tmp), confs + (size_t)k * m.conf_size, m.conf_size);
+    const float e = eval_deriv32(w.at(L.x_tmp), make_float3(v0, v1, v2), slope, w.at(L.g));
+    const double* g = w.d(L.g);
     if (w.lane == 0) out_e[k] = e;
     for (int i = w.lane; i < m.dof; i += 32) out_g[(size_t)k * m.dof + i] = g[i];
     if (out_coords)

@@ -153,6 +153,42 @@ struct Item32 {
     int model, first, count;
 };
 
+// per-warp workspace (bytes, 16 B aligned)
+struct Ws32 {
+    int coords, force, origin, axis, quat, rot;                  // float4 arrays (rot: 3 rows per frame)
+    int x_tmp, x_cand, x_new, x_orig, g, g_new, g_orig, p, y, mhy, h;  // double arrays (h: n x n)
+    int pf, pc;                                                  // prefix sums over atoms (float4)
+    int scratch;                                                 // counters: 32 + 32 + 1 words
+    int total;
+};
+SG_HD Ws32 ws32_layout(int natoms, int nframes, int conf, int dof) {
+    Ws32 w;
+    int o = 0;
+    auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
+    w.coords = take(16 * natoms);
+    w.force = take(16 * natoms);
+    w.origin = take(16 * nframes);
+    w.axis = take(16 * nframes);
+    w.quat = take(16 * nframes);
+    w.rot = take(48 * nframes);
+    w.x_tmp = take(8 * conf);
+    w.x_cand = take(8 * conf);
+    w.x_new = take(8 * conf);
+    w.x_orig = take(8 * conf);
+    w.g = take(8 * dof);
+    w.g_new = take(8 * dof);
+    w.g_orig = take(8 * dof);
+    w.p = take(8 * dof);
+    w.y = take(8 * dof);
+    w.mhy = take(8 * dof);
+    w.h = take(8 * dof * dof);
+    w.pf = take(16 * (natoms + 1));
+    w.pc = take(16 * (natoms + 1));
+    w.scratch = take(4 * 65);
+    w.total = o;
+    return w;
+}
+
 // The block-shared copy of a model for the mixed-precision kernels: counts,
 // then the byte offsets (in the kernel's dynamic shared memory) of the
 // arrays the search reads.  Arrays read once per chain or only for trees
@@ -165,6 +201,7 @@ struct SModel {
     const float4* finit32;
     const int* level_start;
     const int* level_frames;
+    Ws32 L;  // every warp's workspace layout (all warps of a block run this model)
 };
 
 // Bytes of the staged model (SModel + arrays), 16 B aligned pieces
