@@ -13,6 +13,15 @@ namespace sg {
 
 constexpr unsigned kFull32 = 0xffffffffu;
 
+// Loops that are run a handful of times per evaluation are kept rolled by
+// default: the evaluation is latency-bound and instruction-cache-bound, so
+// shorter code beats unrolled code there.
+#ifndef SG_UNROLL_HOT
+#define SG_ROLLED _Pragma("unroll 1")
+#else
+#define SG_ROLLED
+#endif
+
 #ifndef SG_PAIR_CHUNKS
 #define SG_PAIR_CHUNKS 2  // pair chunks (of 32) whose table loads are in flight together
 #endif
@@ -63,8 +72,9 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
     }
     return c;
 }
-// uniform double in [0, 1) with 53 random bits; every lane computes the same value
-__device__ __forceinline__ double ph_u01(Philox& r) {
+// uniform double in [0, 1) with 53 random bits; every lane computes the same
+// value.  Out of line: one copy of the ten rounds serves every draw site.
+__device__ __noinline__ double ph_u01(Philox& r) {
     const uint4 o = philox10(make_uint4(r.n++, 0u, r.c2, r.c3), r.k0, r.k1);
     const uint64_t v = ((uint64_t)(o.x >> 5) << 26) | (o.y >> 6);
     return (double)v * (1.0 / 9007199254740992.0);
@@ -152,6 +162,48 @@ __device__ __forceinline__ float warp_sum(float v) {
 }
 
 
+// model::set frame by frame, level after level (trees of more than 32
+// frames); out of line because typical ligands never need it
+__device__ __noinline__ void set_frames_by_level(const W32& w, const double* conf) {
+    const SModel& m = smodel();
+    const int* fkind = sp<const int>(m.fkind);
+    const int* fconf = sp<const int>(m.fconf);
+    const int* fparent = sp<const int>(m.fparent);
+    const float4* forigin = sp<const float4>(m.forigin32);
+    const float4* faxis = sp<const float4>(m.faxis32);
+    float4* O = w.origin();
+    float4* A = w.axis();
+    float4* Q = w.quat();
+    float4* R = w.rot();
+    for (int lv = 0; lv < m.nlevels; lv++) {
+        for (int idx = __ldg(m.level_start + lv) + w.lane; idx < __ldg(m.level_start + lv + 1); idx += 32) {
+            const int f = __ldg(m.level_frames + idx);
+            const int kind = fkind[f];
+            float4 q;
+            if (kind == SG_FRAME_RIGID) {
+                const double* c = conf + fconf[f];
+                O[f] = make_float4((float)c[0], (float)c[1], (float)c[2], 0);
+                q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
+            } else if (kind == SG_FRAME_SEGMENT) {
+                const int p = fparent[f];
+                const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(forigin[f]));
+                const float3 ax = rot_apply(R + 3 * p, f3(faxis[f]));
+                O[f] = make_float4(o.x, o.y, o.z, 0);
+                A[f] = make_float4(ax.x, ax.y, ax.z, 0);
+                q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[fconf[f]]), Q[p]));
+            } else {
+                const float3 ax = f3(faxis[f]);
+                O[f] = forigin[f];
+                A[f] = make_float4(ax.x, ax.y, ax.z, 0);
+                q = axis_angle32(ax, (float)conf[fconf[f]]);
+            }
+            Q[f] = q;
+            quat_rows(q, R + 3 * f);
+        }
+        __syncwarp();
+    }
+}
+
 // model::set in FP32.  Each frame's transform relative to its parent is a
 // rotation about its parent-frame axis plus its parent-frame origin offset:
 // turning about the lab axis R_p a equals R_p turning about a, so
@@ -192,6 +244,7 @@ __device__ __noinline__ void set_conf32(int conf_at) {
                 q = axis_angle32(f3(faxis[f]), (float)conf[ci]);
             }
         }
+        SG_ROLLED
         for (int it = 0; it < 6 && __any_sync(kFull32, anc >= 0); it++) {
             const int src = anc >= 0 ? anc : f;
             const float qa0 = __shfl_sync(kFull32, q.x, src), qa1 = __shfl_sync(kFull32, q.y, src),
@@ -224,33 +277,7 @@ __device__ __noinline__ void set_conf32(int conf_at) {
         }
         __syncwarp();
     } else {
-        for (int lv = 0; lv < m.nlevels; lv++) {
-            for (int idx = __ldg(m.level_start + lv) + w.lane; idx < __ldg(m.level_start + lv + 1); idx += 32) {
-                const int f = __ldg(m.level_frames + idx);
-                const int kind = fkind[f];
-                float4 q;
-                if (kind == SG_FRAME_RIGID) {
-                    const double* c = conf + fconf[f];
-                    O[f] = make_float4((float)c[0], (float)c[1], (float)c[2], 0);
-                    q = make_float4((float)c[3], (float)c[4], (float)c[5], (float)c[6]);
-                } else if (kind == SG_FRAME_SEGMENT) {
-                    const int p = fparent[f];
-                    const float3 o = f3(O[p]) + rot_apply(R + 3 * p, f3(forigin[f]));
-                    const float3 ax = rot_apply(R + 3 * p, f3(faxis[f]));
-                    O[f] = make_float4(o.x, o.y, o.z, 0);
-                    A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = q_norm_approx32(qmul32(axis_angle32(ax, (float)conf[fconf[f]]), Q[p]));
-                } else {
-                    const float3 ax = f3(faxis[f]);
-                    O[f] = forigin[f];
-                    A[f] = make_float4(ax.x, ax.y, ax.z, 0);
-                    q = axis_angle32(ax, (float)conf[fconf[f]]);
-                }
-                Q[f] = q;
-                quat_rows(q, R + 3 * f);
-            }
-            __syncwarp();
-        }
+        set_frames_by_level(w, conf);
     }
     float4* X = w.coords();
     const int* atom_frame = sp<const int>(m.atom_frame);
@@ -310,6 +337,11 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
     return f + penalty;
 }
 
+// charge map lookup (charge-dependent scoring only), out of line
+__device__ __noinline__ float grid_charge32(int t, float3 loc, float slope, float v, float3& deriv) {
+    return grid_aux32(sG32, t, true, loc, slope, v, deriv);
+}
+
 // table lookup with charge-weighted components (precalculate_linear element
 // eval_deriv); out of line, charge-dependent scoring only
 __device__ __noinline__ void table32_nc(const DTables32& T, int p, bool swap, float qa, float qb, float r2, float& e,
@@ -354,7 +386,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
             const float q = LQ[i].w;
             if (q != 0.f && sG32.c32[t]) {
                 float3 cd;
-                e += q * grid_aux32(sG32, t, true, loc, slope, v.y, cd);
+                e += q * grid_charge32(t, loc, slope, v.y, cd);
                 d = d + q * cd;
                 ghits++;
             }
@@ -461,7 +493,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
             Cq = cross3(f3(X[i]) - oref, F);
         }
         float3 iF = F, iC = Cq;
-#pragma unroll
+        SG_ROLLED
         for (int off = 1; off < 32; off <<= 1) {
             const float a0 = __shfl_up_sync(kFull32, iF.x, off), a1 = __shfl_up_sync(kFull32, iF.y, off),
                         a2 = __shfl_up_sync(kFull32, iF.z, off), b0 = __shfl_up_sync(kFull32, iC.x, off),

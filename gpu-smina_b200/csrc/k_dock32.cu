@@ -220,6 +220,7 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
         SG_T0(t_alg);
         for (int i = w.lane; i < n; i += 32) {
             double sum = 0;
+            SG_ROLLED
             for (int j = 0; j < n; j++) sum += h[j * n + i] * g[j];
             p[i] = -sum;
         }
@@ -251,6 +252,7 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
         if (alpha * yp >= kEps) {
             for (int i = w.lane; i < n; i += 32) {
                 double sum = 0;
+                SG_ROLLED
                 for (int j = 0; j < n; j++) sum += h[j * n + i] * y[j];
                 mhy[i] = -sum;
             }
@@ -259,6 +261,7 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
             const double r = 1 / (alpha * yp);
             const double c1 = alpha * r, c2 = alpha * alpha * (r * r * yhy + r);
             for (int i = w.lane; i < n; i += 32)
+                SG_ROLLED
                 for (int j = 0; j < n; j++) {
                     const int lo = min(i, j), hi = max(i, j);
                     h[j * n + i] += c1 * (mhy[lo] * p[hi] + mhy[hi] * p[lo]) + c2 * p[lo] * p[hi];
