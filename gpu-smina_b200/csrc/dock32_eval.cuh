@@ -327,7 +327,7 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
     const float dx0 = (lo.y - lo.x) * my + (lo.w - lo.z) * y, dx1 = (hi.y - hi.x) * my + (hi.w - hi.z) * y;
     float3 grad = make_float3(dx0 * mz + dx1 * z, (e10 - e00) * mz + (e11 - e01) * z, ez1 - ez0);
     if (f > 0) {  // soft curl
-        const float tt = (v < 1.1920929e-07f) ? 0.f : (v / (v + f));
+        const float tt = (v < 1.1920929e-07f) ? 0.f : __fdividef(v, v + f);
         f *= tt;
         grad = (tt * tt) * grad;
     }
@@ -419,7 +419,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
             ib[u] = (sl[u] >> 8) & 0xff;
             r[u] = f3(X[ib[u]]) - f3(X[ia[u]]);
             r2[u] = dot3(r[u], r[u]);
-            ok[u] = sl[u] != kSlotEmpty && r2[u] < T.cutoff_sqr;
+            ok[u] = ((sl[u] >> 16) & kSlotPairMask) != kSlotPairMask && r2[u] < T.cutoff_sqr;
         }
         float4 tv[SG_PAIR_CHUNKS];
         float rem[SG_PAIR_CHUNKS];
@@ -447,7 +447,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
             f[u] = dor * r[u];
             const float vv = (sl[u] & kSlotIntra) ? v.x : v.z;
             if (pe > 0) {
-                const float tt = (vv < 1.1920929e-07f) ? 0.f : (vv / (vv + pe));
+                const float tt = (vv < 1.1920929e-07f) ? 0.f : __fdividef(vv, vv + pe);
                 pe *= tt;
                 f[u] = (tt * tt) * f[u];
             }

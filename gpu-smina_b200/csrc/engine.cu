@@ -527,36 +527,58 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
         // the first atom of two pairs and none is the second atom of two pairs,
         // so one warp adds a chunk's forces without atomics (first atoms, then
         // second atoms).  A pair may be stored either way round: swapping the
-        // atoms toggles the charge-role bit.
-        std::vector<std::vector<char>> out_used, in_used;
-        std::vector<std::vector<uint32_t>> slots;
+        // atoms toggles the charge-role bit.  Within each quarter of a chunk
+        // (the 8 lanes that one 16-byte shared-memory access serves at a time)
+        // the first atoms are distinct modulo 8 and so are the second atoms,
+        // so the per-atom float4 loads and stores of a quarter hit 8 different
+        // bank groups.
+        struct Chunk {
+            std::vector<char> out_used, in_used;
+            uint8_t amod[4] = {}, bmod[4] = {};  // bank groups taken per quarter (bit masks)
+            uint32_t slot[32];
+            int fill[4] = {};
+        };
+        std::vector<Chunk> chunks;
         const bool packable = M <= 255;
         for (int k = 0; k < P && packable; k++) {
             const int u = d.pairs[2 * k], v = d.pairs[2 * k + 1];
             require(u >= 0 && v >= 0 && u < M && v < M && u != v, "model: pair atoms must be distinct movable atoms");
+            require((pair_tp[k] & 0x1ff) < (int)kSlotPairMask, "model: type pair index out of range");
             const uint32_t base = ((uint32_t)(pair_tp[k] & 0x1ff) << 16) | ((pair_tp[k] >> 30) & 1 ? kSlotSwap : 0) |
                                   (k >= d.num_other_pairs ? kSlotIntra : 0);
-            size_t c = 0;
-            uint32_t slot = 0;
-            for (; c < slots.size(); c++) {
-                if (slots[c].size() >= 32) continue;
-                if (!out_used[c][u] && !in_used[c][v]) { slot = base | u | (v << 8); break; }
-                if (!out_used[c][v] && !in_used[c][u]) { slot = (base ^ kSlotSwap) | v | (u << 8); break; }
+            bool placed = false;
+            for (size_t c = 0; c < chunks.size() && !placed; c++) {
+                Chunk& ch = chunks[c];
+                for (int o = 0; o < 2 && !placed; o++) {
+                    const int a = o ? v : u, b = o ? u : v;
+                    if (ch.out_used[a] || ch.in_used[b]) continue;
+                    for (int q = 0; q < 4; q++) {
+                        if (ch.fill[q] == 8 || (ch.amod[q] >> (a & 7) & 1) || (ch.bmod[q] >> (b & 7) & 1)) continue;
+                        ch.out_used[a] = ch.in_used[b] = 1;
+                        ch.amod[q] |= 1 << (a & 7);
+                        ch.bmod[q] |= 1 << (b & 7);
+                        ch.slot[8 * q + ch.fill[q]++] = (o ? base ^ kSlotSwap : base) | a | (b << 8);
+                        placed = true;
+                        break;
+                    }
+                }
             }
-            if (c == slots.size()) {
-                out_used.emplace_back(M, 0);
-                in_used.emplace_back(M, 0);
-                slots.emplace_back();
-                slot = base | u | (v << 8);
+            if (!placed) {
+                chunks.emplace_back();
+                Chunk& ch = chunks.back();
+                ch.out_used.assign(M, 0);
+                ch.in_used.assign(M, 0);
+                for (uint32_t& x : ch.slot) x = kSlotEmpty;
+                ch.out_used[u] = ch.in_used[v] = 1;
+                ch.amod[0] = 1 << (u & 7);
+                ch.bmod[0] = 1 << (v & 7);
+                ch.slot[ch.fill[0]++] = base | u | (v << 8);
             }
-            out_used[c][slot & 0xff] = 1;
-            in_used[c][(slot >> 8) & 0xff] = 1;
-            slots[c].push_back(slot);
         }
         std::vector<int> ps;
-        for (auto& c : slots)
-            for (int l = 0; l < 32; l++) ps.push_back((int)(l < (int)c.size() ? c[l] : kSlotEmpty));
-        hm.npchunks = packable ? (int)slots.size() : -1;
+        for (const Chunk& ch : chunks)
+            for (int l = 0; l < 32; l++) ps.push_back((int)ch.slot[l]);
+        hm.npchunks = packable ? (int)chunks.size() : -1;
         pv(ps);
     }
     auto pf4 = [&](const double* xyz, const double* w4, size_t n) {

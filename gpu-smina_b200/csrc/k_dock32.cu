@@ -23,6 +23,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull32, v, o);
     return v;
 }
+// three butterfly sums at once (one latency chain)
+__device__ __forceinline__ void warp_sum3_d(double& a, double& b, double& c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(kFull32, a, o);
+        b += __shfl_xor_sync(kFull32, b, o);
+        c += __shfl_xor_sync(kFull32, c, o);
+    }
+}
 __device__ __forceinline__ double dotd(const W32& w, const double* a, const double* b, int n) {
     double t = 0;
     for (int i = w.lane; i < n; i += 32) t += a[i] * b[i];
@@ -48,7 +57,7 @@ __device__ __forceinline__ void q_increment32(double* c, double rx, double ry, d
     if (a2 > kEps * kEps) {  // angle > epsilon
         const double inv = rsqrt(a2);
         float sf, cf;
-        sincosf((float)(0.5 * wrap_pi(a2 * inv)), &sf, &cf);
+        __sincosf((float)(0.5 * wrap_pi(a2 * inv)), &sf, &cf);
         s = (double)sf * inv;
         co = (double)cf;
     }
@@ -120,14 +129,14 @@ __device__ __forceinline__ double feval32(int x_at, int g_at, const Mode32& em) 
 
 // ---- line searches (bfgs.h:30-200) ------------------------------------------------------
 // x, g, p, x_new, g_new: offsets of this warp's workspace arrays in smem32
-__device__ __forceinline__ double line_fast32(const W32& w, int x_at, int g_at, double f0, int p_at, int xn_at, int gn_at,
-                                              double& f1, const Mode32& em) {
+// pg: p . g, computed by the caller with p
+__device__ __forceinline__ double line_fast32(const W32& w, int x_at, double pg, double f0, int p_at, int xn_at,
+                                              int gn_at, double& f1, const Mode32& em) {
     const SModel& m = smodel();
     const double* x = sp<const double>(x_at);
     const double* p = sp<const double>(p_at);
     double* x_new = sp<double>(xn_at);
     double alpha = 1;
-    const double pg = dotd(w, p, sp<const double>(g_at), m.dof);
     for (unsigned trial = 0; trial < 10; trial++) {
         SG_T0(t_ls);
         copyd(w, x_new, x, m.conf_size);
@@ -140,8 +149,8 @@ __device__ __forceinline__ double line_fast32(const W32& w, int x_at, int g_at, 
     return alpha;
 }
 
-__device__ __noinline__ double line_accurate32(const W32& w, int x_at, int g_at, double f0, int p_at, int xn_at,
-                                                  int gn_at, double& f1, const Mode32& em) {
+__device__ __noinline__ double line_accurate32(const W32& w, int x_at, double pg, double f0, int p_at, int xn_at,
+                                                int gn_at, double& f1, const Mode32& em) {
     const SModel& m = smodel();
     const int n = m.dof;
     const double* x = sp<const double>(x_at);
@@ -150,7 +159,7 @@ __device__ __noinline__ double line_accurate32(const W32& w, int x_at, int g_at,
     double* g_new = sp<double>(gn_at);
     double a, alpha, alpha2 = 0, alamin, b, disc, f2 = 0, rhs1, rhs2, tmplam = 0;
     const double ALF = 1.0e-4, FIRST = 1.0;
-    const double slope = dotd(w, sp<const double>(g_at), p, n);
+    const double slope = pg;
     auto give_up = [&]() {
         copyd(w, x_new, x, m.conf_size);
         for (int i = w.lane; i < n; i += 32) g_new[i] = 0;
@@ -218,54 +227,70 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
     copyd(w, x_orig, x, cs);
     for (int step = 0; step < maxiters; step++) {
         SG_T0(t_alg);
+        double pg = 0;  // p . g, for the line search
         for (int i = w.lane; i < n; i += 32) {
             double sum = 0;
             SG_ROLLED
             for (int j = 0; j < n; j++) sum += h[j * n + i] * g[j];
             p[i] = -sum;
+            pg += -sum * g[i];
         }
+        pg = warp_sum_d(pg);
         __syncwarp();
         SG_T1(t_alg, 5);
         double f1 = 0;
-        const double alpha = accurate ? line_accurate32(w, x_at, g_at, f0, p_at, xn_at, gn_at, f1, em)
-                                      : line_fast32(w, x_at, g_at, f0, p_at, xn_at, gn_at, f1, em);
+        const double alpha = accurate ? line_accurate32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em)
+                                      : line_fast32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em);
         if (alpha == 0) break;
         SG_T0(t_alg2);
-        for (int i = w.lane; i < n; i += 32) y[i] = g_new[i] - g[i];
+        // y = g_new - g, g = g_new, and the three dot products the update needs
+        double gg = 0, yy = 0, yp = 0;
+        for (int i = w.lane; i < n; i += 32) {
+            const double gi = g_new[i], yi = gi - g[i];
+            y[i] = yi;
+            g[i] = gi;
+            gg += gi * gi;
+            yy += yi * yi;
+            yp += yi * p[i];
+        }
+        warp_sum3_d(gg, yy, yp);
         __syncwarp();
         const double prevf0 = f0;
         f0 = f1;
         copyd(w, x, x_new, cs);
         if (early && fabs(prevf0 - f0) < 1e-5) break;
-        copyd(w, g, g_new, n);
-        if (!(dotd(w, g, g, n) >= 1e-4)) break;
-        if (step == 0) {
-            const double yy = dotd(w, y, y, n);
-            if (fabs(yy) > kEps) {
-                const double dg = alpha * dotd(w, y, p, n) / yy;
-                for (int i = w.lane; i < n; i += 32) h[i * n + i] = dg;
-                __syncwarp();
-            }
+        if (!(gg >= 1e-4)) break;
+        if (step == 0 && fabs(yy) > kEps) {
+            const double dg = alpha * yp / yy;
+            for (int i = w.lane; i < n; i += 32) h[i * n + i] = dg;
+            __syncwarp();
         }
         // bfgs_update
-        const double yp = dotd(w, y, p, n);
         if (alpha * yp >= kEps) {
+            double yhy = 0;
             for (int i = w.lane; i < n; i += 32) {
                 double sum = 0;
                 SG_ROLLED
                 for (int j = 0; j < n; j++) sum += h[j * n + i] * y[j];
                 mhy[i] = -sum;
+                yhy += y[i] * -sum;
             }
+            yhy = -warp_sum_d(yhy);
             __syncwarp();
-            const double yhy = -dotd(w, y, mhy, n);
             const double r = 1 / (alpha * yp);
             const double c1 = alpha * r, c2 = alpha * alpha * (r * r * yhy + r);
-            for (int i = w.lane; i < n; i += 32)
+            for (int i = w.lane; i < n; i += 32) {
+                const double mi = mhy[i], pi = p[i];
                 SG_ROLLED
                 for (int j = 0; j < n; j++) {
-                    const int lo = min(i, j), hi = max(i, j);
-                    h[j * n + i] += c1 * (mhy[lo] * p[hi] + mhy[hi] * p[lo]) + c2 * p[lo] * p[hi];
+                    // operands ordered (lower index, higher index) so h stays symmetric
+                    const double mj = mhy[j], pj = p[j];
+                    const bool own_lo = i <= j;
+                    const double ml = own_lo ? mi : mj, mh = own_lo ? mj : mi;
+                    const double pl = own_lo ? pi : pj, ph = own_lo ? pj : pi;
+                    h[j * n + i] += c1 * (ml * ph + mh * pl) + c2 * pl * ph;
                 }
+            }
             __syncwarp();
         }
         SG_T1(t_alg2, 5);

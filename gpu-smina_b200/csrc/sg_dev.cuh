@@ -102,7 +102,8 @@ struct __align__(16) DModel {
     // mixed-precision pair schedule: npchunks chunks of 32 slots; within a
     // chunk every atom is at most once the first and once the second atom.
     // Slot: a | b << 8 | type pair << 16 | swapped << 25 | intramolecular
-    // (v[0]) << 26; unused slots kSlotEmpty.  Null when the model has more
+    // (v[0]) << 26; unused slots kSlotEmpty (type pair 0x1ff, atoms 0 and 0,
+    // so their loads stay in range).  Null when the model has more
     // than 255 movable atoms.
     const uint32_t* pslot;    // [npchunks * 32]
     int cost;                 // relative cost of one evaluation (atoms + pairs + frames)
@@ -110,7 +111,8 @@ struct __align__(16) DModel {
     int pad_[2];
 };
 
-constexpr uint32_t kSlotEmpty = 0xffffffffu;
+constexpr uint32_t kSlotEmpty = 0x1ffu << 16;
+constexpr uint32_t kSlotPairMask = 0x1ffu;  // (slot >> 16) & mask: type pair, 0x1ff when empty
 constexpr uint32_t kSlotSwap = 1u << 25, kSlotIntra = 1u << 26;
 
 // FP32 pair table: per (type pair, sample i, component) the float4
