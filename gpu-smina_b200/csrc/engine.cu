@@ -103,6 +103,7 @@ int sg_create(int device, int precision, sg_engine** out) {
 void sg_destroy(sg_engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
+    serve_shutdown(e);
     cudaStreamSynchronize(e->stream);
     delete e;
 }

@@ -130,9 +130,9 @@ cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DRecept
                             const double[3], int, const int*, int, int, double*, double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
 int mc32_occupancy(int wpb, size_t smem);
-cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const Chain32*, const Item32*, int nitems,
-                        const MCParams32&, unsigned*, int blocks, int wpb, size_t stage_stride, size_t ws_stride,
-                        cudaStream_t);
+cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
+                        const Item32*, int nitems, const MCParams32&, unsigned*, int blocks, int wpb,
+                        size_t stage_stride, size_t ws_stride, cudaStream_t);
 cudaError_t launch_eval32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, const double*,
                           const double[3], double, double*, double*, double*, cudaStream_t);
 
@@ -150,4 +150,5 @@ RecState& receptor_for(sg_engine* e, int rid);
 void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes);
 void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels);
 void refresh_header(sg_engine* e, RecState& r);
+void serve_shutdown(sg_engine* e);  // stops the engine's request loop, if one runs
 }  // namespace sg

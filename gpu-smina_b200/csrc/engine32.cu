@@ -195,7 +195,7 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             const int j = chain_job[k];
             int n = 0;
             while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
-            items.push_back(Item32{hc[k].model, k, n});
+            items.push_back(Item32{hc[k].model, k, n, 0});
             item_cost.push_back((double)hc[k].steps * pm.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
             k += n;
         }
@@ -214,8 +214,8 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         for (int i = 0; i < 3; i++) {
             P.hunt[i] = (float)p->hunt_cap[i];
             P.auth[i] = (float)p->authentic_v[i];
-            P.box_lo[i] = r.gd.begin[i];
-            P.box_hi[i] = r.gd.end[i];
+            P.box[i] = r.gd.begin[i];
+            P.box[3 + i] = r.gd.end[i];
         }
         P.slope = (float)p->cache_slope;
         P.temperature = p->temperature;
@@ -232,7 +232,7 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(v[i]); }
         } evg{ev};
         cuda_check(cudaEventRecord(ev[0], e->stream), "event");
-        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), d_chains.as<Chain32>(),
+        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), nullptr, d_chains.as<Chain32>(),
                                d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb, stage_stride,
                                ws_stride, e->stream),
                    "search launch");

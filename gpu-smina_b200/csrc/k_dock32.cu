@@ -377,7 +377,8 @@ __device__ __forceinline__ void mutate32(const W32& w, Philox& rng, double* x, d
 
 // conf::randomize: position uniform in the box, orientation from four
 // normal deviates, torsions uniform in [-pi, pi)
-__device__ __forceinline__ void randomize32(const W32& w, Philox& rng, double* x, const MCParams32& P) {
+// box: 6 doubles (lo xyz, hi xyz) of the search box
+__device__ __forceinline__ void randomize32(const W32& w, Philox& rng, double* x, const double* box) {
     const SModel& m = smodel();
     const int* blk_rigid = sp<const int>(m.blk_rigid);
     const int* blk_ntors = sp<const int>(m.blk_ntors);
@@ -386,7 +387,7 @@ __device__ __forceinline__ void randomize32(const W32& w, Philox& rng, double* x
         double* c = x + blk_conf[b];
         if (blk_rigid[b]) {
             double v[7];
-            for (int k = 0; k < 3; k++) v[k] = ph_range(rng, P.box_lo[k], P.box_hi[k]);
+            for (int k = 0; k < 3; k++) v[k] = ph_range(rng, box[k], box[3 + k]);
             double q[4], nq = 0;
             for (int k = 0; k < 4; k++) { q[k] = ph_normal(rng); nq += q[k] * q[k]; }
             nq = sqrt(nq);
@@ -479,7 +480,7 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
     const int tmp_at = w.at(L.x_tmp), cand_at = w.at(L.x_cand);
     double* tmp = sp<double>(tmp_at);
     double* cand = sp<double>(cand_at);
-    randomize32(w, rng, tmp, P);
+    randomize32(w, rng, tmp, ch.box ? ch.box : P.box);
     const Mode32 hunt{make_float3(P.hunt[0], P.hunt[1], P.hunt[2]), P.slope};
     const Mode32 auth{make_float3(P.auth[0], P.auth[1], P.auth[2]), P.slope};
     double tmp_e = 0, best_e = kMaxFl;
@@ -515,6 +516,13 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
         *ch.evals = C[64];
         ch.hits[0] = gh;
         ch.hits[1] = ph;
+        if (ch.done_count) {
+            __threadfence();  // this chain's results, before its count
+            if (atomicAdd(ch.done_count, 1u) + 1 == (unsigned)ch.lig_chains) {
+                __threadfence_system();
+                *ch.host_flag = 1u;
+            }
+        }
     }
     __syncwarp();
     SG_T1(t_chain, 7);
@@ -580,10 +588,12 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
 #ifndef SG_MC32_THREADS
 #define SG_MC32_THREADS 256
 #endif
+// maps_tab: one DMaps32 per receptor (items name theirs), or null when the
+// whole launch uses G.
 __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
-                                                            const Chain32* chains, const Item32* items, int nitems,
-                                                            MCParams32 P, unsigned* queue, int stage_stride,
-                                                            int ws_stride) {
+                                                            const DMaps32* maps_tab, const Chain32* chains,
+                                                            const Item32* items, int nitems, MCParams32 P,
+                                                            unsigned* queue, int stage_stride, int ws_stride) {
     __shared__ int s_item;
     const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
     if (tid == 0) { sT32 = T; sG32 = G; sWs0 = stage_stride; sWsStride = ws_stride; }
@@ -593,6 +603,7 @@ __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DM
         const int it = s_item;
         if (it >= nitems) break;
         const Item32 item = items[it];
+        if (maps_tab && tid == 0) sG32 = maps_tab[item.rec];  // read after stage_model's barrier
         stage_model(models + item.model, tid, nthr);
         if (warp < item.count) {
             const Chain32 ch = chains[item.first + warp];
@@ -649,13 +660,13 @@ int mc32_occupancy(int wpb, size_t smem) {
     return blocks;
 }
 
-cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const Chain32* chains,
-                        const Item32* items, int nitems, const MCParams32& P, unsigned* queue, int blocks, int wpb,
-                        size_t stage_stride, size_t ws_stride, cudaStream_t s) {
+cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const DMaps32* maps_tab,
+                        const Chain32* chains, const Item32* items, int nitems, const MCParams32& P, unsigned* queue,
+                        int blocks, int wpb, size_t stage_stride, size_t ws_stride, cudaStream_t s) {
     const size_t smem = stage_stride + (size_t)wpb * ws_stride;
     cudaError_t rc = prep32((const void*)k_mc32, smem);
     if (rc != cudaSuccess) return rc;
-    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, chains, items, nitems, P, queue, (int)stage_stride,
+    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue, (int)stage_stride,
                                           (int)ws_stride);
     return cudaGetLastError();
 }

@@ -177,7 +177,7 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
             const int j = chain_job[k];
             int n = 0;
             while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
-            items.push_back(Item32{hc[k].model, (int)k, n});
+            items.push_back(Item32{hc[k].model, (int)k, n, 0});
             item_cost.push_back((double)hc[k].steps * img.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
             k += n;
         }
@@ -226,8 +226,8 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
         for (int i = 0; i < 3; i++) {
             P.hunt[i] = (float)p->hunt_cap[i];
             P.auth[i] = (float)p->authentic_v[i];
-            P.box_lo[i] = r.gd.begin[i];
-            P.box_hi[i] = r.gd.end[i];
+            P.box[i] = r.gd.begin[i];
+            P.box[3 + i] = r.gd.end[i];
         }
         P.slope = (float)p->cache_slope;
         P.temperature = p->temperature;
@@ -240,7 +240,7 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
         const int nitems = (int)queue.size();
         const int blocks = (int)std::min<long long>((long long)occ * e->num_sms, nitems);
         cuda_check(launch_mc32(reinterpret_cast<const DModel*>(base + models_at + img.dmodel_off), tables32(e),
-                               maps32(e, r), reinterpret_cast<const Chain32*>(base + chains_at),
+                               maps32(e, r), nullptr, reinterpret_cast<const Chain32*>(base + chains_at),
                                reinterpret_cast<const Item32*>(base + items_at), nitems, P,
                                reinterpret_cast<unsigned*>(base + queue_at), blocks, wpb, stage_stride, ws_stride, s),
                    "search launch");

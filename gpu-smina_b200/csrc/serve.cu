@@ -1,0 +1,826 @@
+// Serving: a request loop with continuous batching over resident receptors.
+//
+// Requests (one ligand against one resident receptor each) are queued by
+// sg_serve_submit.  A worker thread launches them in small batches: a batch
+// goes out as soon as enough requests wait or the oldest has waited
+// max_wait_ms, if the device memory the server holds for requests in flight
+// stays under its budget.  Batches run on their own streams with one block
+// per work item (a group of chains of one ligand), so a new batch's blocks
+// start as soon as earlier batches' blocks retire: the device keeps a mix of
+// requests in flight rather than a queue of whole batches.  Ligands of
+// different receptors share a batch (the kernel takes a table of map sets).
+// The last chain of a ligand to finish raises a flag in host-mapped memory;
+// the worker then copies that ligand's chain results back, merges them
+// (min_rmsd 2) and refines the merged poses in FP64 on a separate stream,
+// and the result becomes available to sg_serve_poll / sg_serve_fetch.
+// Results are the same as sg_dock_batch32's for the same (seed, ligand key)
+// whatever else is in flight.
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <thread>
+#include "engine.h"
+
+namespace sg {
+
+using Clock = std::chrono::steady_clock;
+
+// an owned copy of a caller's model description (the caller may free its
+// arrays once sg_serve_submit returns)
+struct ModelCopy {
+    sg_model_desc d{};
+    std::vector<int> lig_pair_end, lig_begin, lig_end, lig_root, type, fkind, fparent, fbegin, fend, fconf, fdof, pairs;
+    std::vector<double> charge, local, lab, forigin, faxis, finit;
+    explicit ModelCopy(const sg_model_desc& s) : d(s) {
+        auto ci = [](std::vector<int>& v, const int* p, size_t n) { if (p) v.assign(p, p + n); };
+        auto cd = [](std::vector<double>& v, const double* p, size_t n) { if (p) v.assign(p, p + n); };
+        const size_t L = s.num_ligands, N = s.num_atoms, F = s.num_frames, P = s.num_pairs;
+        ci(lig_pair_end, s.lig_pair_end, L); ci(lig_begin, s.ligand_atom_begin, L); ci(lig_end, s.ligand_atom_end, L);
+        ci(lig_root, s.ligand_root, L); ci(type, s.atom_type, N); ci(fkind, s.frame_kind, F);
+        ci(fparent, s.frame_parent, F); ci(fbegin, s.frame_begin, F); ci(fend, s.frame_end, F);
+        ci(fconf, s.frame_conf, F); ci(fdof, s.frame_dof, F); ci(pairs, s.pairs, 2 * P);
+        cd(charge, s.atom_charge, N); cd(local, s.atom_local, 3 * N); cd(lab, s.atom_lab, 3 * N);
+        cd(forigin, s.frame_origin, 3 * F); cd(faxis, s.frame_axis, 3 * F); cd(finit, s.frame_init_origin, 3 * F);
+        auto pi = [](const std::vector<int>& v) { return v.empty() ? nullptr : v.data(); };
+        auto pd = [](const std::vector<double>& v) { return v.empty() ? nullptr : v.data(); };
+        d.lig_pair_end = pi(lig_pair_end); d.ligand_atom_begin = pi(lig_begin); d.ligand_atom_end = pi(lig_end);
+        d.ligand_root = pi(lig_root); d.atom_type = pi(type); d.frame_kind = pi(fkind); d.frame_parent = pi(fparent);
+        d.frame_begin = pi(fbegin); d.frame_end = pi(fend); d.frame_conf = pi(fconf); d.frame_dof = pi(fdof);
+        d.pairs = pi(pairs); d.atom_charge = pd(charge); d.atom_local = pd(local); d.atom_lab = pd(lab);
+        d.frame_origin = pd(forigin); d.frame_axis = pd(faxis); d.frame_init_origin = pd(finit);
+    }
+};
+
+struct ServeReq {
+    uint64_t ticket = 0;
+    int rid = 0;
+    sg_ligand_job job{};
+    sg_mc_params p{};
+    std::shared_ptr<ModelCopy> m;
+    Clock::time_point t_submit;
+    size_t bytes = 0;  // device memory its share of a batch needs
+};
+
+struct ServeDone {
+    sg_serve_done info{};
+    std::vector<double> e, conf, coords;
+};
+
+// add_to_output_container (coords.cpp:25-58) for the per-ligand merge
+struct SvPose {
+    double e;
+    std::vector<double> conf, xyz;
+};
+static void sv_add_pose(std::vector<SvPose>& out, SvPose&& t, double min_rmsd, int max_size) {
+    size_t ci = out.size();
+    double cr = DBL_MAX;
+    const size_t H3 = t.xyz.size();
+    for (size_t i = 0; i < out.size(); i++) {
+        double acc = 0;
+        for (size_t a = 0; a < H3; a++) {
+            const double d = t.xyz[a] - out[i].xyz[a];
+            acc += d * d;
+        }
+        const double r = H3 ? std::sqrt(acc / (double)(H3 / 3)) : 0.0;
+        if (i == 0 || r < cr) { ci = i; cr = r; }
+    }
+    if (ci < out.size() && cr < min_rmsd) {
+        if (t.e < out[ci].e) out[ci] = std::move(t);
+    } else if ((int)out.size() < max_size) {
+        out.push_back(std::move(t));
+    } else if (!out.empty() && t.e < out.back().e) {
+        out.back() = std::move(t);
+    }
+    std::stable_sort(out.begin(), out.end(), [](const SvPose& a, const SvPose& b) { return a.e < b.e; });
+}
+
+// One ligand inside a launched batch and its post-processing state.
+struct SvLig {
+    ServeReq req;
+    int model = 0, first = 0, nchains = 0, flag = -1;
+    int state = 0;  // 0 searching, 1 refining, 2 published
+    uint64_t evals = 0;
+    std::vector<SvPose> poses;
+    size_t conf_off = 0, xyz_off = 0;
+    struct SvBatch* batch = nullptr;
+};
+
+struct SvBatch {
+    cudaStream_t stream = nullptr;
+    char* dmem = nullptr;
+    size_t bytes = 0;
+    ModelImage img;
+    std::vector<SvLig> ligs;
+    std::vector<Chain32> hc;
+    size_t e_at = 0, conf_at = 0, xyz_at = 0, order_at = 0, count_at = 0, evals_at = 0;
+    int S = 20;
+    cudaEvent_t kdone = nullptr;
+    int published = 0;
+};
+
+struct Server {
+    sg_engine* e = nullptr;
+    sg_serve_opts o{};
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv_done;
+    std::deque<ServeReq> queue;
+    std::map<uint64_t, ServeDone> done;
+    std::deque<uint64_t> done_order;  // not yet reported by poll
+    std::vector<std::unique_ptr<SvBatch>> inflight;
+    size_t inflight_bytes = 0;
+    uint64_t next_ticket = 1;
+    bool stopping = false;
+    int error = SG_OK;
+    std::string error_text;
+    std::vector<cudaStream_t> streams, free_streams;  // one launch in flight per stream
+    int inflight_ligs = 0;
+    cudaStream_t refine_stream = nullptr, copy_stream = nullptr;
+    // completion flags in host-mapped memory
+    volatile unsigned* flags = nullptr;
+    unsigned* dflags = nullptr;
+    std::vector<int> free_flags;
+    int* d_err = nullptr;
+    Clock::time_point last_err_check;
+    std::vector<std::unique_ptr<struct RefineGroup>> refining;
+    static constexpr int kFlags = 1 << 16;
+    static constexpr int kMaxStreams = 96;
+};
+
+static size_t req_bytes(const sg_model_desc& m, const sg_ligand_job& j, int S) {
+    const size_t conf = m.conf_size, heavy = m.num_movable;  // heavy <= movable: an upper bound
+    const size_t per_chain = sizeof(Chain32) + S * (8 + 8 * conf + 12 * heavy + 4) + 4 + 8 + 16;
+    const size_t model = 64 * (size_t)m.num_atoms + 96 * (size_t)m.num_frames + 24 * (size_t)m.num_pairs + 4096;
+    return model + j.num_chains * per_chain + S * (8 * conf + 24 * heavy + 8) + 4096;
+}
+
+static bool same_params(const sg_mc_params& a, const sg_mc_params& b) {
+    return a.temperature == b.temperature && a.mutation_amplitude == b.mutation_amplitude && a.min_rmsd == b.min_rmsd &&
+           a.num_saved_mins == b.num_saved_mins && a.accurate_line == b.accurate_line && a.early_term == b.early_term &&
+           a.cache_slope == b.cache_slope && std::equal(a.hunt_cap, a.hunt_cap + 3, b.hunt_cap) &&
+           std::equal(a.authentic_v, a.authentic_v + 3, b.authentic_v);
+}
+
+// Launches one batch; called by the worker with mu held.
+static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
+    sg_engine* e = s.e;
+    auto b = std::make_unique<SvBatch>();
+    const sg_mc_params& p = reqs[0].p;
+    const int S = p.num_saved_mins;
+    b->S = S;
+    if (s.free_streams.empty()) {
+        cudaStream_t st;
+        cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "serve: stream");
+        s.streams.push_back(st);
+        s.free_streams.push_back(st);
+    }
+    b->stream = s.free_streams.back();
+    s.free_streams.pop_back();
+    std::vector<sg_model_desc> descs;
+    for (auto& r : reqs) descs.push_back(r.m->d);
+    size_t need = 0;
+    for (auto& r : reqs) need += r.bytes;
+    // layout: models image, then tables and results; the image is packed
+    // once to size the allocation (against a placeholder base, never
+    // dereferenced) and again against the allocation
+    ModelImage probe;
+    pack_models_image(descs.data(), (int)descs.size(), reinterpret_cast<char*>(uintptr_t(1) << 20), probe);
+    auto r16 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t nchains = 0, nconf = 0, nxyz = 0;
+    for (size_t k = 0; k < reqs.size(); k++) {
+        const DModel& h = probe.host[k];
+        nchains += reqs[k].job.num_chains;
+        nconf += (size_t)reqs[k].job.num_chains * S * h.conf_size;
+        nxyz += (size_t)reqs[k].job.num_chains * S * h.nheavy * 3;
+    }
+    size_t at = r16(probe.bytes.size());
+    const size_t maps_at = at; at = r16(at + SG_MAX_RECEPTORS * sizeof(DMaps32));
+    const size_t boxes_at = at; at = r16(at + SG_MAX_RECEPTORS * 6 * sizeof(double));
+    const size_t chains_at = at; at = r16(at + nchains * sizeof(Chain32));
+    const size_t items_at = at; at = r16(at + nchains * sizeof(Item32));
+    const size_t queue_at = at; at = r16(at + 256);
+    const size_t cnt_at = at; at = r16(at + reqs.size() * sizeof(unsigned));
+    b->e_at = at; at = r16(at + nchains * S * sizeof(double));
+    b->conf_at = at; at = r16(at + nconf * sizeof(double));
+    b->xyz_at = at; at = r16(at + nxyz * sizeof(float));
+    b->order_at = at; at = r16(at + nchains * S * sizeof(int));
+    b->count_at = at; at = r16(at + nchains * sizeof(int));
+    b->evals_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
+    const size_t hits_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
+    b->bytes = std::max(at, need);
+    cuda_check(cudaMallocAsync((void**)&b->dmem, b->bytes, b->stream), "serve: batch memory");
+    pack_models_image(descs.data(), (int)descs.size(), b->dmem, b->img);
+    // map sets and search boxes of every receptor
+    std::vector<DMaps32> tab(SG_MAX_RECEPTORS);
+    std::vector<double> boxes(SG_MAX_RECEPTORS * 6, 0.0);
+    for (int rid = 0; rid < SG_MAX_RECEPTORS; rid++) {
+        const RecState& r = e->rec[rid];
+        bool any = false;
+        for (int t = 0; t < kNumTypes; t++) any = any || r.map32[t].p != nullptr;
+        if (!r.set || !any) continue;
+        tab[rid] = maps32(e, r);
+        for (int i = 0; i < 3; i++) {
+            boxes[rid * 6 + i] = r.gd.begin[i];
+            boxes[rid * 6 + 3 + i] = r.gd.end[i];
+        }
+    }
+    // chains, items (longest first) and the ligands' slots
+    size_t ws_stride = 0, stage_stride = 0;
+    int max_chains = 1;
+    for (const DModel& h : b->img.host) {
+        ws_stride = std::max(ws_stride, ws32_bytes(h));
+        stage_stride = std::max(stage_stride, (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig,
+                                                                    h.nblocks, h.ntors));
+    }
+    ws_stride = (ws_stride + 15) & ~(size_t)15;
+    for (auto& r : reqs) max_chains = std::max(max_chains, r.job.num_chains);
+    int wpb = 0, occ = 0;
+    for (int c : {8, 4, 2, 1}) {
+        if (e->force_wpb && c != e->force_wpb) continue;
+        if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;
+        const size_t smem = stage_stride + (size_t)c * ws_stride;
+        if (smem > (size_t)e->max_smem) continue;
+        const int o2 = mc32_occupancy(c, smem);
+        if (o2 * c > occ * wpb) { wpb = c; occ = o2; }
+    }
+    require(wpb > 0, "serve: model too large for the mixed-precision path's shared memory");
+    std::vector<Item32> items;
+    std::vector<double> cost;
+    size_t conf_off = 0, xyz_off = 0;
+    for (size_t k = 0; k < reqs.size(); k++) {
+        const DModel& h = b->img.host[k];
+        SvLig L;
+        L.req = std::move(reqs[k]);
+        L.model = (int)k;
+        L.first = (int)b->hc.size();
+        L.nchains = L.req.job.num_chains;
+        require(!s.free_flags.empty(), "serve: too many ligands in flight");
+        L.flag = s.free_flags.back();
+        s.free_flags.pop_back();
+        s.flags[L.flag] = 0u;
+        L.conf_off = conf_off;
+        L.xyz_off = xyz_off;
+        L.batch = b.get();
+        const sg_ligand_job& J = L.req.job;
+        for (int c = 0; c < J.num_chains; c++) {
+            Chain32 ch{};
+            ch.model = (int)k;
+            ch.steps = J.num_steps;
+            ch.maxiters = J.maxiters > 0 ? J.maxiters : L.req.p.maxiters;
+            ch.key0 = (uint32_t)J.seed;
+            ch.key1 = (uint32_t)(J.seed >> 32) ^ (uint32_t)(J.ligand_key >> 32);
+            ch.lig = (uint32_t)J.ligand_key;
+            ch.chain = (uint32_t)c;
+            const size_t kc = b->hc.size();
+            ch.out_e = reinterpret_cast<double*>(b->dmem + b->e_at) + kc * S;
+            ch.out_conf = reinterpret_cast<double*>(b->dmem + b->conf_at) + conf_off;
+            ch.out_coords = reinterpret_cast<float*>(b->dmem + b->xyz_at) + xyz_off;
+            ch.out_order = reinterpret_cast<int*>(b->dmem + b->order_at) + kc * S;
+            ch.out_count = reinterpret_cast<int*>(b->dmem + b->count_at) + kc;
+            ch.evals = reinterpret_cast<unsigned long long*>(b->dmem + b->evals_at) + kc;
+            ch.hits = reinterpret_cast<unsigned long long*>(b->dmem + hits_at) + 2 * kc;
+            ch.done_count = reinterpret_cast<unsigned*>(b->dmem + cnt_at) + k;
+            ch.host_flag = s.dflags + L.flag;
+            ch.lig_chains = J.num_chains;
+            ch.box = reinterpret_cast<const double*>(b->dmem + boxes_at) + 6 * L.req.rid;
+            b->hc.push_back(ch);
+            conf_off += (size_t)S * h.conf_size;
+            xyz_off += (size_t)S * h.nheavy * 3;
+        }
+        for (int c0 = 0; c0 < J.num_chains; c0 += wpb) {
+            items.push_back(Item32{(int)k, L.first + c0, std::min(wpb, J.num_chains - c0), L.req.rid});
+            cost.push_back((double)J.num_steps * h.cost * std::max(1, b->hc[L.first].maxiters));
+        }
+        b->ligs.push_back(std::move(L));
+    }
+    std::vector<int> order(items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    std::vector<Item32> q(items.size());
+    for (size_t k = 0; k < items.size(); k++) q[k] = items[order[k]];
+    cudaStream_t st = b->stream;
+    cuda_check(cudaMemcpyAsync(b->dmem, b->img.bytes.data(), b->img.bytes.size(), cudaMemcpyHostToDevice, st), "serve");
+    cuda_check(cudaMemcpyAsync(b->dmem + maps_at, tab.data(), tab.size() * sizeof(DMaps32), cudaMemcpyHostToDevice, st),
+               "serve");
+    cuda_check(cudaMemcpyAsync(b->dmem + boxes_at, boxes.data(), boxes.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               st),
+               "serve");
+    cuda_check(cudaMemcpyAsync(b->dmem + chains_at, b->hc.data(), b->hc.size() * sizeof(Chain32),
+                               cudaMemcpyHostToDevice, st),
+               "serve");
+    cuda_check(cudaMemcpyAsync(b->dmem + items_at, q.data(), q.size() * sizeof(Item32), cudaMemcpyHostToDevice, st),
+               "serve");
+    cuda_check(cudaMemsetAsync(b->dmem + queue_at, 0, 256, st), "serve");
+    cuda_check(cudaMemsetAsync(b->dmem + cnt_at, 0, reqs.size() * sizeof(unsigned) + 16, st), "serve");
+    MCParams32 P{};
+    for (int i = 0; i < 3; i++) {
+        P.hunt[i] = (float)p.hunt_cap[i];
+        P.auth[i] = (float)p.authentic_v[i];
+        P.box[i] = 0;
+        P.box[3 + i] = 0;
+    }
+    P.slope = (float)p.cache_slope;
+    P.temperature = p.temperature;
+    P.amplitude = p.mutation_amplitude;
+    P.min_rmsd = p.min_rmsd;
+    P.num_saved = S;
+    P.maxiters = p.maxiters;
+    P.accurate_line = p.accurate_line;
+    P.early_term = p.early_term;
+    // one block per work item, so blocks of later batches fill in as these retire
+    cuda_check(launch_mc32(reinterpret_cast<const DModel*>(b->dmem + b->img.dmodel_off), tables32(e), tab[0],
+                           reinterpret_cast<const DMaps32*>(b->dmem + maps_at),
+                           reinterpret_cast<const Chain32*>(b->dmem + chains_at),
+                           reinterpret_cast<const Item32*>(b->dmem + items_at), (int)q.size(), P,
+                           reinterpret_cast<unsigned*>(b->dmem + queue_at), (int)q.size(), wpb, stage_stride, ws_stride,
+                           st),
+               "serve: search launch");
+    cuda_check(cudaEventCreateWithFlags(&b->kdone, cudaEventDisableTiming), "serve");
+    cuda_check(cudaEventRecord(b->kdone, st), "serve");
+    s.inflight_bytes += b->bytes;
+    s.inflight_ligs += (int)b->ligs.size();
+    s.inflight.push_back(std::move(b));
+}
+
+// A ligand's chains are done: copy their containers back and merge them.
+static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
+    const DModel& h = b.img.host[L.model];
+    const int S = b.S, cs = h.conf_size, H = h.nheavy;
+    const size_t nc = L.nchains;
+    std::vector<double> he(nc * S), hconf((size_t)nc * S * cs);
+    std::vector<float> hxyz((size_t)nc * S * H * 3);
+    std::vector<int> horder(nc * S), hcount(nc);
+    std::vector<unsigned long long> hev(nc);
+    cudaStream_t cp = s.copy_stream;
+    auto get = [&](void* dst, size_t from, size_t bytes) {
+        if (bytes) cuda_check(cudaMemcpyAsync(dst, b.dmem + from, bytes, cudaMemcpyDeviceToHost, cp), "serve: fetch");
+    };
+    get(he.data(), b.e_at + (size_t)L.first * S * sizeof(double), he.size() * sizeof(double));
+    get(hconf.data(), b.conf_at + L.conf_off * sizeof(double), hconf.size() * sizeof(double));
+    get(hxyz.data(), b.xyz_at + L.xyz_off * sizeof(float), hxyz.size() * sizeof(float));
+    get(horder.data(), b.order_at + (size_t)L.first * S * sizeof(int), horder.size() * sizeof(int));
+    get(hcount.data(), b.count_at + (size_t)L.first * sizeof(int), hcount.size() * sizeof(int));
+    get(hev.data(), b.evals_at + (size_t)L.first * sizeof(unsigned long long), hev.size() * sizeof(unsigned long long));
+    cuda_check(cudaStreamSynchronize(cp), "serve: fetch");
+    for (size_t k = 0; k < nc; k++) {
+        L.evals += hev[k];
+        const int cnt = std::min(std::max(hcount[k], 0), S);
+        for (int i = 0; i < cnt; i++) {
+            const int slot = horder[k * S + i];
+            if (slot < 0 || slot >= S) continue;
+            SvPose t;
+            t.e = he[k * S + slot];
+            const double* c = &hconf[(k * S + slot) * cs];
+            t.conf.assign(c, c + cs);
+            const float* x = &hxyz[(k * S + slot) * H * 3];
+            t.xyz.assign(x, x + (size_t)H * 3);
+            sv_add_pose(L.poses, std::move(t), 2.0, S);
+        }
+    }
+}
+
+// One FP64 refinement launch for the merged poses of every ligand that
+// finished since the last one (ligands of any batch and receptor).
+struct RefineGroup {
+    std::vector<SvLig*> ligs;
+    std::vector<int> first;  // first pose of each ligand
+    std::vector<double> conf, e, xyz;
+    int cs = 0, hs = 1;
+    void* dbuf = nullptr;
+    cudaEvent_t ev = nullptr;
+};
+
+static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& fin) {
+    sg_engine* e = s.e;
+    auto g = std::make_unique<RefineGroup>();
+    std::vector<DModel> dms;
+    std::vector<int> pose_model, pose_maxit;
+    std::vector<DReceptor*> recs;
+    size_t ws = 0;
+    int np = 0;
+    for (auto& [b, L] : fin) {
+        const DModel& h = b->img.host[L->model];
+        g->cs = std::max(g->cs, h.conf_size);
+        g->hs = std::max(g->hs, h.nheavy);
+        ws = std::max(ws, ws64_bytes(h));
+    }
+    require(ws <= (size_t)e->max_smem, "serve: model too large for the plain path's shared memory");
+    // refine_structure needs the pose's receptor: one launch per receptor in the group
+    std::map<int, std::vector<std::pair<SvBatch*, SvLig*>>> by_rec;
+    for (auto& f : fin) by_rec[f.second->req.rid].push_back(f);
+    for (auto& [rid, members] : by_rec) {
+        for (auto& [b, L] : members) {
+            const int m = (int)dms.size();
+            dms.push_back(b->img.host[L->model]);
+            g->ligs.push_back(L);
+            g->first.push_back(np);
+            const int mi = L->req.job.maxiters > 0 ? L->req.job.maxiters : L->req.p.maxiters;
+            for (const SvPose& t : L->poses) {
+                g->conf.insert(g->conf.end(), t.conf.begin(), t.conf.end());
+                g->conf.resize((size_t)(np + 1) * g->cs, 0.0);
+                pose_model.push_back(m);
+                pose_maxit.push_back(mi);
+                np++;
+            }
+            L->state = 1;
+        }
+    }
+    g->first.push_back(np);
+    if (np == 0) {
+        for (SvLig* L : g->ligs) L->state = 3;  // nothing to refine: publish as is
+        s.refining.push_back(std::move(g));
+        return;
+    }
+    const size_t cb = g->conf.size() * sizeof(double), eb = (size_t)np * sizeof(double),
+                 xb = (size_t)np * g->hs * 3 * sizeof(double), ib = (size_t)np * sizeof(int),
+                 mb = dms.size() * sizeof(DModel);
+    cudaStream_t rs = s.refine_stream;
+    cuda_check(cudaMallocAsync(&g->dbuf, cb + eb + xb + 2 * ib + mb + 256, rs), "serve: refine memory");
+    char* base = static_cast<char*>(g->dbuf);
+    DModel* d_models = reinterpret_cast<DModel*>(base);
+    double* dc = reinterpret_cast<double*>(base + ((mb + 15) & ~(size_t)15));
+    double* de = dc + g->conf.size();
+    double* dx = de + np;
+    int* dpm = reinterpret_cast<int*>(dx + (size_t)np * g->hs * 3);
+    int* dmi = dpm + np;
+    cuda_check(cudaMemcpyAsync(d_models, dms.data(), mb, cudaMemcpyHostToDevice, rs), "serve");
+    cuda_check(cudaMemcpyAsync(dc, g->conf.data(), cb, cudaMemcpyHostToDevice, rs), "serve");
+    cuda_check(cudaMemcpyAsync(dpm, pose_model.data(), ib, cudaMemcpyHostToDevice, rs), "serve");
+    cuda_check(cudaMemcpyAsync(dmi, pose_maxit.data(), ib, cudaMemcpyHostToDevice, rs), "serve");
+    int p0 = 0;
+    for (auto& [rid, members] : by_rec) {
+        int n = 0;
+        for (auto& [b, L] : members) n += (int)L->poses.size();
+        if (n > 0) {
+            const sg_mc_params& P = members[0].second->req.p;
+            cuda_check(launch_refine64(d_models, ws, e->tables, e->rec[rid].dhdr.as<DReceptor>(), dpm + p0, n,
+                                       dc + (size_t)p0 * g->cs, g->cs, P.authentic_v, P.maxiters, dmi + p0,
+                                       P.accurate_line, P.early_term, de + p0, dx + (size_t)p0 * g->hs * 3, g->hs,
+                                       s.d_err, rs),
+                       "serve: refine launch");
+        }
+        p0 += n;
+    }
+    g->e.resize(np);
+    g->xyz.resize((size_t)np * g->hs * 3);
+    cuda_check(cudaMemcpyAsync(g->conf.data(), dc, cb, cudaMemcpyDeviceToHost, rs), "serve");
+    cuda_check(cudaMemcpyAsync(g->e.data(), de, eb, cudaMemcpyDeviceToHost, rs), "serve");
+    cuda_check(cudaMemcpyAsync(g->xyz.data(), dx, xb, cudaMemcpyDeviceToHost, rs), "serve");
+    cuda_check(cudaFreeAsync(g->dbuf, rs), "serve");
+    g->dbuf = nullptr;
+    cuda_check(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming), "serve");
+    cuda_check(cudaEventRecord(g->ev, rs), "serve");
+    s.refining.push_back(std::move(g));
+}
+
+// The refinement is done: publish the result.  mu held.
+static void publish(Server& s, const RefineGroup& g, size_t k) {
+    SvLig& L = *g.ligs[k];
+    const int np = (int)L.poses.size();
+    const int cs = L.poses.empty() ? 0 : (int)L.poses[0].conf.size();
+    const int H = L.poses.empty() ? 0 : (int)L.poses[0].xyz.size() / 3;
+    ServeDone d;
+    d.info.ticket = L.req.ticket;
+    d.info.status = SG_OK;
+    d.info.conf_size = L.req.m->d.conf_size;
+    d.info.num_heavy = H;
+    d.info.evals = L.evals;
+    for (int i = 0; i < np; i++) {
+        const size_t q = (size_t)g.first[k] + i;
+        L.poses[i].e = g.e[q];
+        std::memcpy(L.poses[i].conf.data(), &g.conf[q * g.cs], cs * sizeof(double));
+        L.poses[i].xyz.assign(&g.xyz[q * g.hs * 3], &g.xyz[q * g.hs * 3] + (size_t)H * 3);
+    }
+    std::stable_sort(L.poses.begin(), L.poses.end(), [](const SvPose& a, const SvPose& c) { return a.e < c.e; });
+    d.info.count = np;
+    for (const SvPose& t : L.poses) {
+        d.e.push_back(t.e);
+        d.conf.insert(d.conf.end(), t.conf.begin(), t.conf.end());
+        d.coords.insert(d.coords.end(), t.xyz.begin(), t.xyz.end());
+    }
+    d.info.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - L.req.t_submit).count();
+    s.done[L.req.ticket] = std::move(d);
+    s.done_order.push_back(L.req.ticket);
+    L.state = 2;
+    s.free_flags.push_back(L.flag);
+    s.inflight_ligs--;
+}
+
+static void fail_all(Server& s, int code, const std::string& why) {
+    s.error = code;
+    s.error_text = why;
+    auto fail = [&](uint64_t ticket, Clock::time_point t0) {
+        ServeDone d;
+        d.info.ticket = ticket;
+        d.info.status = code;
+        d.info.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        s.done[ticket] = std::move(d);
+        s.done_order.push_back(ticket);
+    };
+    for (auto& b : s.inflight)
+        for (auto& L : b->ligs)
+            if (L.state != 2) fail(L.req.ticket, L.req.t_submit);
+    for (auto& r : s.queue) fail(r.ticket, r.t_submit);
+    s.queue.clear();
+    s.inflight.clear();
+    s.refining.clear();
+    s.inflight_bytes = 0;
+    s.cv_done.notify_all();
+}
+
+static void worker(Server* sp) {
+    Server& s = *sp;
+    cudaSetDevice(s.e->device);
+    std::unique_lock<std::mutex> lk(s.mu);
+    for (;;) {
+        bool busy = false;
+        try {
+            // 1. launch.  While fewer ligands are in flight than the device holds
+            // at once (max_inflight_ligands), whatever waits goes out at once;
+            // beyond that, requests gather for up to max_wait_ms into bigger
+            // launches.  Same search parameters per launch; device memory
+            // held for requests in flight stays under the budget.
+            if (!s.queue.empty() && (!s.free_streams.empty() || (int)s.streams.size() < Server::kMaxStreams)) {
+                const double waited =
+                    std::chrono::duration<double, std::milli>(Clock::now() - s.queue.front().t_submit).count();
+                const bool room = s.inflight_ligs < s.o.max_inflight_ligands;
+                if (room || (int)s.queue.size() >= s.o.max_batch_ligands || waited >= s.o.max_wait_ms || s.stopping) {
+                    std::vector<ServeReq> take;
+                    size_t bytes = 0;
+                    const int cap = std::min(s.o.max_batch_ligands, (int)s.free_flags.size());
+                    while (!s.queue.empty() && (int)take.size() < cap) {
+                        ServeReq& r = s.queue.front();
+                        if (!take.empty() && !same_params(r.p, take[0].p)) break;
+                        if (s.inflight_bytes + bytes + r.bytes > s.o.hbm_budget_bytes &&
+                            !(take.empty() && s.inflight.empty()))
+                            break;
+                        bytes += r.bytes;
+                        take.push_back(std::move(r));
+                        s.queue.pop_front();
+                    }
+                    if (!take.empty()) {
+                        launch_batch(s, std::move(take));
+                        busy = true;
+                    }
+                }
+            }
+            // 2. ligands whose chains are done: merge, then one refinement launch for all
+            std::vector<std::pair<SvBatch*, SvLig*>> fin;
+            for (auto& b : s.inflight)
+                for (auto& L : b->ligs)
+                    if (L.state == 0 && s.flags[L.flag]) {
+                        fetch_merge(s, *b, L);
+                        fin.emplace_back(b.get(), &L);
+                    }
+            if (!fin.empty()) {
+                launch_refines(s, fin);
+                busy = true;
+            }
+            // refinements that finished: publish their ligands
+            for (size_t i = 0; i < s.refining.size();) {
+                RefineGroup& g = *s.refining[i];
+                if (!g.ev || cudaEventQuery(g.ev) == cudaSuccess) {
+                    for (size_t k = 0; k < g.ligs.size(); k++) {
+                        publish(s, g, k);
+                        g.ligs[k]->batch->published++;
+                    }
+                    if (g.ev) cudaEventDestroy(g.ev);
+                    s.refining.erase(s.refining.begin() + i);
+                    s.cv_done.notify_all();
+                    busy = true;
+                } else {
+                    i++;
+                }
+            }
+            // 3. retire batches whose kernel ended and whose ligands are all published
+            for (size_t i = 0; i < s.inflight.size();) {
+                SvBatch& b = *s.inflight[i];
+                if (b.published == (int)b.ligs.size() && cudaEventQuery(b.kdone) == cudaSuccess) {
+                    cuda_check(cudaFreeAsync(b.dmem, b.stream), "serve: free batch");
+                    cudaEventDestroy(b.kdone);
+                    s.free_streams.push_back(b.stream);
+                    s.inflight_bytes -= b.bytes;
+                    s.inflight.erase(s.inflight.begin() + i);
+                    busy = true;
+                } else {
+                    i++;
+                }
+            }
+            // device errors (overlap in a refinement) end the server
+            int herr = 0;
+            if (!busy && Clock::now() - s.last_err_check > std::chrono::milliseconds(10)) {
+                s.last_err_check = Clock::now();
+                cuda_check(cudaMemcpy(&herr, s.d_err, sizeof(int), cudaMemcpyDeviceToHost), "serve: error word");
+                if (herr != kDevOk)
+                    throw EngineError(herr == kDevOverlap ? SG_ERR_OVERLAP : SG_ERR_ARG,
+                                      "serve: device reported error " + std::to_string(herr));
+            }
+        } catch (EngineError& x) {
+            fail_all(s, x.code, x.what());
+        } catch (std::exception& x) {
+            fail_all(s, SG_ERR_ARG, x.what());
+        }
+        if (s.stopping && s.queue.empty() && s.inflight.empty() && s.refining.empty()) break;
+        if (!busy) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(100));
+            lk.lock();
+        }
+    }
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+static std::mutex g_srv_mu;
+static std::map<const sg_engine*, std::unique_ptr<Server>> g_servers;
+
+static Server* server_of(const sg_engine* e) {
+    std::lock_guard<std::mutex> lk(g_srv_mu);
+    auto it = g_servers.find(e);
+    return it == g_servers.end() ? nullptr : it->second.get();
+}
+
+// Stops the engine's server, if any (sg_destroy calls this first).
+void sg::serve_shutdown(sg_engine* e) {
+    Server* s = server_of(e);
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+    }
+    if (s->th.joinable()) s->th.join();
+    std::lock_guard<std::mutex> lk(g_srv_mu);
+    g_servers.erase(e);
+}
+
+extern "C" {
+
+int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
+    return guarded(e, [&] {
+        require(e->precision != SG_PREC_FP64, "serve needs an engine created with SG_PREC_FP32 or SG_PREC_FP32_H16");
+        require(e->has_tables, "no tables set");
+        require(!server_of(e), "serve: already started");
+        auto s = std::make_unique<Server>();
+        s->e = e;
+        if (o) s->o = *o;
+        if (s->o.max_batch_ligands <= 0) s->o.max_batch_ligands = 64;
+        if (s->o.max_wait_ms <= 0) s->o.max_wait_ms = 2.0;
+        if (s->o.max_inflight_ligands <= 0) s->o.max_inflight_ligands = 320;
+        if (s->o.hbm_budget_bytes == 0) {
+            size_t fr = 0, tot = 0;
+            cuda_check(cudaMemGetInfo(&fr, &tot), "serve: memory info");
+            s->o.hbm_budget_bytes = fr / 4;
+        }
+        cuda_check(cudaStreamCreateWithFlags(&s->refine_stream, cudaStreamNonBlocking), "serve: stream");
+        cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "serve: stream");
+        unsigned* hf = nullptr;
+        cuda_check(cudaHostAlloc((void**)&hf, Server::kFlags * sizeof(unsigned), cudaHostAllocMapped), "serve: flags");
+        std::memset(hf, 0, Server::kFlags * sizeof(unsigned));
+        s->flags = hf;
+        cuda_check(cudaHostGetDevicePointer((void**)&s->dflags, hf, 0), "serve: flags");
+        for (int i = Server::kFlags - 1; i >= 0; i--) s->free_flags.push_back(i);
+        cuda_check(cudaMalloc((void**)&s->d_err, sizeof(int)), "serve: error word");
+        cuda_check(cudaMemset(s->d_err, 0, sizeof(int)), "serve: error word");
+        Server* raw = s.get();
+        {
+            std::lock_guard<std::mutex> lk(g_srv_mu);
+            g_servers[e] = std::move(s);
+        }
+        raw->th = std::thread(worker, raw);
+    });
+}
+
+int sg_serve_submit(sg_engine* e, int rid, const sg_model_desc* m, const sg_ligand_job* job, const sg_mc_params* p,
+                    uint64_t* ticket) {
+    return guarded(e, [&] {
+        Server* s = server_of(e);
+        require(s, "serve: not started");
+        require(m && job && p && ticket, "serve: bad arguments");
+        require(job->num_chains >= 1 && job->num_chains <= 4096 && job->maxiters >= 0, "serve: bad ligand job");
+        require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->temperature > 0, "serve: bad search parameters");
+        require(m->num_movable <= 255, "mixed-precision path: at most 255 movable atoms per model");
+        RecState& r = receptor_for(e, rid);
+        ServeReq q;
+        q.m = std::make_shared<ModelCopy>(*m);
+        q.rid = rid;
+        q.job = *job;
+        q.job.model = 0;
+        q.p = *p;
+        q.bytes = req_bytes(*m, *job, p->num_saved_mins);
+        std::unique_lock<std::mutex> lk(s->mu);
+        require(s->error == SG_OK, "serve: stopped after an error: " + s->error_text);
+        require(!s->stopping, "serve: stopping");
+        require(q.bytes <= s->o.hbm_budget_bytes, "serve: the request needs more device memory than the budget");
+        lk.unlock();
+        // the receptor's maps for this ligand's types (built once, then resident)
+        {
+            std::vector<int> types;
+            for (int i = 0; i < m->num_movable; i++)
+                if (m->atom_type[i] < kNumTypes && !is_h(m->atom_type[i])) types.push_back(m->atom_type[i]);
+            bool missing = false;
+            for (int t : types) missing = missing || !r.built[t];
+            if (missing) {
+                lk.lock();  // the worker reads receptor state while launching
+                ensure_maps(e, r, types.data(), (int)types.size());
+                lk.unlock();
+            }
+        }
+        lk.lock();
+        q.ticket = s->next_ticket++;
+        q.t_submit = Clock::now();
+        *ticket = q.ticket;
+        s->queue.push_back(std::move(q));
+    });
+}
+
+int sg_serve_poll(sg_engine* e, sg_serve_done* out, int max, int wait_ms, int* nout) {
+    return guarded(e, [&] {
+        Server* s = server_of(e);
+        require(s, "serve: not started");
+        require(out && nout && max >= 0, "serve: bad arguments");
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->done_order.empty() && wait_ms > 0)
+            s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !s->done_order.empty(); });
+        int n = 0;
+        while (n < max && !s->done_order.empty()) {
+            const uint64_t t = s->done_order.front();
+            s->done_order.pop_front();
+            out[n++] = s->done[t].info;
+        }
+        *nout = n;
+    });
+}
+
+int sg_serve_fetch(sg_engine* e, uint64_t ticket, sg_ligand_result* out) {
+    return guarded(e, [&] {
+        Server* s = server_of(e);
+        require(s, "serve: not started");
+        require(out, "serve: bad arguments");
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->done.find(ticket);
+        require(it != s->done.end(), "serve: unknown or already fetched ticket");
+        const ServeDone& d = it->second;
+        out->count = d.info.count;
+        out->evals = d.info.evals;
+        if (d.info.count > 0) {
+            require(out->e && out->conf && out->coords, "serve: null result arrays");
+            std::memcpy(out->e, d.e.data(), d.e.size() * sizeof(double));
+            std::memcpy(out->conf, d.conf.data(), d.conf.size() * sizeof(double));
+            std::memcpy(out->coords, d.coords.data(), d.coords.size() * sizeof(double));
+        }
+        s->done.erase(it);
+    });
+}
+
+int sg_serve_stats(const sg_engine* e, int* queued, int* inflight_ligands, uint64_t* inflight_bytes) {
+    Server* s = server_of(e);
+    if (!s) return SG_ERR_STATE;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (queued) *queued = (int)s->queue.size();
+    int n = 0;
+    for (auto& b : s->inflight)
+        for (auto& L : b->ligs) n += L.state != 2;
+    if (inflight_ligands) *inflight_ligands = n;
+    if (inflight_bytes) *inflight_bytes = s->inflight_bytes;
+    return SG_OK;
+}
+
+int sg_serve_stop(sg_engine* e) {
+    return guarded(e, [&] {
+        Server* s = server_of(e);
+        require(s, "serve: not started");
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stopping = true;
+        }
+        if (s->th.joinable()) s->th.join();
+        for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+        cudaStreamSynchronize(s->refine_stream);
+        cudaStreamSynchronize(s->copy_stream);
+        for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+        cudaStreamDestroy(s->refine_stream);
+        cudaStreamDestroy(s->copy_stream);
+        cudaFreeHost((void*)s->flags);
+        cudaFree(s->d_err);
+        const int err = s->error;
+        const std::string why = s->error_text;
+        {
+            std::lock_guard<std::mutex> lk(g_srv_mu);
+            g_servers.erase(e);
+        }
+        if (err != SG_OK) throw EngineError(err, why);
+    });
+}
+
+}  // extern "C"

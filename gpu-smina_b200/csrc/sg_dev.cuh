@@ -148,11 +148,18 @@ struct Chain32 {
     int* out_count;
     unsigned long long* evals;
     unsigned long long* hits;  // [2]: grid lookups, in-cutoff pair lookups
+    // completion signal (serving; null otherwise): the last of the ligand's
+    // lig_chains chains to finish sets *host_flag (host-mapped memory)
+    unsigned* done_count;
+    volatile unsigned* host_flag;
+    int lig_chains;
+    const double* box;  // search box (lo xyz, hi xyz) of this chain's receptor; null: the launch's
 };
 
 // A block's unit of work: chains [first, first + count) of one model
 struct Item32 {
     int model, first, count;
+    int rec;  // receptor slot in the launch's map table (0 when the launch has one receptor)
 };
 
 // per-warp workspace (bytes, 16 B aligned)
@@ -218,7 +225,7 @@ struct MCParams32 {
     float slope;
     double temperature, amplitude, min_rmsd;
     int num_saved, maxiters, accurate_line, early_term;
-    double box_lo[3], box_hi[3];
+    double box[6];  // search box: lo xyz, hi xyz
 };
 
 // Per-warp FP64 workspace layout in shared memory (offsets in doubles)

@@ -81,6 +81,16 @@ class LigandResult(C.Structure):
     _fields_ = [("count", C.c_int), ("e", _dp), ("conf", _dp), ("coords", _dp), ("evals", C.c_uint64)]
 
 
+class ServeOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_ligands", C.c_int), ("max_wait_ms", C.c_double),
+                ("max_inflight_ligands", C.c_int)]
+
+
+class ServeDone(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int), ("count", C.c_int), ("conf_size", C.c_int),
+                ("num_heavy", C.c_int), ("evals", C.c_uint64), ("latency_ms", C.c_double)]
+
+
 _lib = None
 
 
@@ -134,6 +144,13 @@ def _declare(L):
         "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
         "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
         "sg_set_chains_per_block": [vp, C.c_int],
+        "sg_serve_start": [vp, C.POINTER(ServeOpts)],
+        "sg_serve_submit": [vp, C.c_int, C.POINTER(ModelDesc), C.POINTER(LigandJob), C.POINTER(MCParams),
+                            C.POINTER(C.c_uint64)],
+        "sg_serve_poll": [vp, C.POINTER(ServeDone), C.c_int, C.c_int, _ip],
+        "sg_serve_fetch": [vp, C.c_uint64, C.POINTER(LigandResult)],
+        "sg_serve_stats": [vp, _ip, _ip, C.POINTER(C.c_uint64)],
+        "sg_serve_stop": [vp],
     }.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -457,6 +474,39 @@ class Engine:
         return {"mc_ms": mc.value, "refine_ms": rf.value, "chains_per_block": wpb.value, "blocks": blocks.value,
                 "evals": ctr[0].value, "grid_lookups": ctr[1].value, "pair_lookups": ctr[2].value,
                 "h2d_bytes": ctr[3].value, "d2h_bytes": ctr[4].value}
+
+    # ---- serving (continuous batching) ----------------------------------------
+    def serve_start(self, hbm_budget_bytes=0, max_batch_ligands=0, max_wait_ms=0.0, max_inflight_ligands=0):
+        o = ServeOpts(hbm_budget_bytes, max_batch_ligands, max_wait_ms, max_inflight_ligands)
+        self._check(load().sg_serve_start(self._h, C.byref(o)))
+
+    def serve_submit(self, rid, m: Model, job: LigandJob, params: MCParams) -> int:
+        """Queues one ligand against receptor ``rid``; returns its ticket."""
+        t = C.c_uint64()
+        self._check(load().sg_serve_submit(self._h, rid, C.byref(m.desc), C.byref(job), C.byref(params), C.byref(t)))
+        return t.value
+
+    def serve_poll(self, max_n=256, wait_ms=0):
+        """Finished requests as (ticket, status, count, latency_ms, evals, conf_size, num_heavy) tuples."""
+        buf = (ServeDone * max_n)()
+        n = C.c_int()
+        self._check(load().sg_serve_poll(self._h, buf, max_n, wait_ms, C.byref(n)))
+        return [(buf[i].ticket, buf[i].status, buf[i].count, buf[i].latency_ms, buf[i].evals, buf[i].conf_size,
+                 buf[i].num_heavy) for i in range(n.value)]
+
+    def serve_fetch(self, ticket, count, conf_size, num_heavy):
+        e, conf, xyz = np.zeros(max(count, 1)), np.zeros((max(count, 1), conf_size)), np.zeros((max(count, 1), num_heavy, 3))
+        out = LigandResult(0, dptr(e), dptr(conf), dptr(xyz), 0)
+        self._check(load().sg_serve_fetch(self._h, ticket, C.byref(out)))
+        return {"e": e[:count].copy(), "conf": conf[:count].copy(), "coords": xyz[:count].copy(), "evals": int(out.evals)}
+
+    def serve_stats(self):
+        q, n, b = C.c_int(), C.c_int(), C.c_uint64()
+        self._check(load().sg_serve_stats(self._h, C.byref(q), C.byref(n), C.byref(b)))
+        return {"queued": q.value, "inflight": n.value, "inflight_bytes": b.value}
+
+    def serve_stop(self):
+        self._check(load().sg_serve_stop(self._h))
 
     def set_chains_per_block(self, n: int):
         self._check(load().sg_set_chains_per_block(self._h, n))

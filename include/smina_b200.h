@@ -22,6 +22,7 @@
  *                                                                        src/main/main.cpp:165-190
  *   sg_dock_batch32              GpuDocking::dock_batch (batched screen) src/gpu/gpu_docking.cpp:756-831
  *   sg_serve_*                   (no counterpart: continuous-batching request loop)
+ *   sg_dock_batch32_noalloc      (no counterpart: the batched search without device allocation)
  *   sg_last_error                the std::runtime_error text the reference throws
  *
  * Conventions
@@ -296,6 +297,50 @@ int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookup
  * pick the shape with the most resident chains per SM (the default).  The
  * chains of one block share one copy of their ligand's model. */
 int sg_set_chains_per_block(sg_engine* e, int n);
+
+/* ---- serving: a request loop with continuous batching ------------------
+ * No counterpart in the reference (its screens are offline batches).
+ * Requests (one ligand against one resident receptor) are queued by
+ * sg_serve_submit; a worker thread launches them as they arrive (in bigger
+ * launches once the device is full), ligands of different receptors in the
+ * same launch, each launch on its own stream with one block per group of
+ * chains, so new launches fill the GPU as older work retires.
+ * Admission keeps the device memory held for requests in flight under
+ * hbm_budget_bytes.  Each ligand is merged and refined (FP64) as soon as its
+ * own chains finish.  A result equals sg_dock_batch32's (refine = 1) for the
+ * same (seed, ligand_key), alone or in any mix.  While a server runs, the
+ * engine's other entry points must not be called except sg_serve_*. */
+typedef struct sg_serve_opts {
+    uint64_t hbm_budget_bytes;  /* 0: a quarter of the free device memory   */
+    int max_batch_ligands;      /* ligands per launch (0: 64)                */
+    double max_wait_ms;         /* once the device is full, how long requests
+                                   gather into a bigger launch (0: 2 ms)     */
+    int max_inflight_ligands;   /* ligands on the device before requests
+                                   start to gather (0: 320, a little over what
+                                   a B200 holds at once)                     */
+} sg_serve_opts;
+
+typedef struct sg_serve_done {
+    uint64_t ticket;
+    int status;                /* SG_OK, or the error that ended the request */
+    int count;                 /* poses (merged, refined, by energy)        */
+    int conf_size, num_heavy;  /* sizes for sg_serve_fetch's arrays         */
+    uint64_t evals;            /* eval_deriv calls of the search            */
+    double latency_ms;         /* submit to result                          */
+} sg_serve_done;
+
+int sg_serve_start(sg_engine* e, const sg_serve_opts* opts);
+/* job->model is ignored; the model is copied, so the caller may free it. */
+int sg_serve_submit(sg_engine* e, int receptor_id, const sg_model_desc* m, const sg_ligand_job* job,
+                    const sg_mc_params* p, uint64_t* ticket);
+/* Up to max finished requests (waits up to wait_ms for the first one). */
+int sg_serve_poll(sg_engine* e, sg_serve_done* out, int max, int wait_ms, int* nout);
+/* Copies a finished request's poses (arrays sized by its sg_serve_done)
+ * and forgets the ticket. */
+int sg_serve_fetch(sg_engine* e, uint64_t ticket, sg_ligand_result* out);
+int sg_serve_stats(const sg_engine* e, int* queued, int* inflight_ligands, uint64_t* inflight_bytes);
+/* Finishes every submitted request, then stops the worker. */
+int sg_serve_stop(sg_engine* e);
 
 #ifdef __cplusplus
 }
