@@ -141,6 +141,76 @@ def cpu_sample(models, gd, receptor, tables, exh, seed, nlig, threads, parallel=
     return len(idx) / dt, dt, idx
 
 
+def run_accuracy(args):
+    """Top-score agreement of the batched FP32 search with the plain FP64
+    search on a sample of the screen (smina's full step counts, exhaustiveness
+    8, merge + FP64 refinement on both sides).  Reports the spread of
+    best-energy differences FP32 - FP64 next to the seed-to-seed spread of
+    FP64 itself (two FP64 runs with different seeds)."""
+    spec = screen(args.ligands, args.seed)
+    idx = [int(i) for i in np.linspace(0, len(spec) - 1, args.accuracy)]
+    models = build_models([spec[i] for i in idx])
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    types = sorted({t for m in models for t in m.types() if 1 < t < 27})
+    e64 = sb.Engine(0, sb.PREC_FP64)
+    e64.set_tables(T)
+    e64.set_receptor(0, R, gd)
+    e64.build_grids(0, types)
+    e32 = sb.Engine(0, sb.PREC_FP32 if args.precision == "fp32" else sb.PREC_FP32_H16)
+    e32.set_tables(T)
+    e32.set_receptor(0, R, gd)
+    e32.build_grids(0, types)
+    p = make_params(models)
+    exh = args.exhaustiveness
+    cmax = max(m.conf_size for m in models)
+
+    def best64(seed):
+        confs, mts, moc, steps, its = [], [], [], [], []
+        for k, m in enumerate(models):
+            sp = m.search_params(9)
+            c, mt = m.seed_chains(seed + k, exh, gd)
+            cm = np.zeros((exh, cmax))
+            cm[:, :m.conf_size] = c
+            confs += list(cm)
+            mts += list(mt)
+            moc += [k] * exh
+            steps += [sp.num_steps] * exh
+            its += [sp.maxiters] * exh
+        t0 = time.perf_counter()
+        b = e64.dock(0, models, moc, confs, mts, p, steps=steps, maxiters=its)
+        out = []
+        for k, m in enumerate(models):
+            sp = m.search_params(9)
+            e, conf, _ = sb.merge_chains(b, m, first=exh * k, n=exh, max_size=p.num_saved_mins)
+            _, er, _ = e64.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v),
+                                  maxiters=sp.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
+            out.append(float(np.min(er)))
+        return np.array(out), time.perf_counter() - t0
+
+    a64, t_a = best64(args.seed)
+    b64, t_b = best64(args.seed + 7919)
+    jobs = jobs_for(models, list(range(len(models))), exh, args.seed, 0)
+    t0 = time.perf_counter()
+    r32 = e32.dock_batch(0, models, jobs, p, refine=True)
+    t32 = time.perf_counter() - t0
+    a32 = np.array([float(r["e"][0]) for r in r32])
+    d32, d64 = a32 - a64, b64 - a64
+    print(json.dumps({
+        "accuracy": f"top-score agreement, {len(models)} ligands spread over the screen, full smina steps, "
+                    f"exhaustiveness {exh}, merge + FP64 refine on both sides",
+        "precision": args.precision,
+        "fp32_minus_fp64": {"mean": float(d32.mean()), "sd": float(d32.std(ddof=1)),
+                            "median_abs": float(np.median(np.abs(d32)))},
+        "fp64_seed_to_seed": {"mean": float(d64.mean()), "sd": float(d64.std(ddof=1)),
+                              "median_abs": float(np.median(np.abs(d64)))},
+        "best_energy_mean": {"fp32": float(a32.mean()), "fp64": float(a64.mean())},
+        "wall_s": {"fp64_run": t_a, "fp64_run_2": t_b, "fp32_batched": t32},
+        "ligands_per_s": {"fp64_plain": len(models) / t_a, "fp32_batched": len(models) / t32},
+    }), flush=True)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -218,8 +288,13 @@ def main():
     ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--accuracy", type=int, default=0,
+                    help="instead of timing: top-score agreement FP32 vs FP64 on this many ligands")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
+    if args.accuracy:
+        run_accuracy(args)
+        return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

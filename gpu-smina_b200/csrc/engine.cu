@@ -821,7 +821,7 @@ int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, con
         size_t nconf_res = 0, nxyz_res = 0;
         for (int k = 0; k < nchains; k++) {
             const sg_chain_input& c = chains[k];
-            require(c.model >= 0 && c.model < nmodels && c.conf && c.mt, "dock: bad chain input");
+            require(c.model >= 0 && c.model < nmodels && c.conf && c.mt && c.maxiters >= 0, "dock: bad chain input");
             require(c.mt[624] <= 624, "dock: mt19937 index out of range");
             const DModel& h = pm.host[c.model];
             conf_off[k] = conf0.size();
@@ -849,6 +849,7 @@ int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, con
         for (int k = 0; k < nchains; k++) {
             hc[k].model = chains[k].model;
             hc[k].steps = chains[k].num_steps;
+            hc[k].maxiters = chains[k].maxiters > 0 ? chains[k].maxiters : p->maxiters;
             hc[k].conf0 = d_conf0.p() + conf_off[k];
             hc[k].mt = d_mt.p() + (size_t)k * 625;
             hc[k].out_e = d_e.p() + (size_t)k * S;

@@ -90,14 +90,14 @@ __global__ void __launch_bounds__(32) k_mc64(const DModel* models, DTables T, co
     for (unsigned step = 0; step < ch.steps; step++) {
         vcopy(w, cand, tmp, m.conf_size);
         mutate64(w, cand, P.amplitude);
-        const double cand_e = bfgs64(w, cand, P.maxiters, P.accurate_line, P.early_term, hunt);
+        const double cand_e = bfgs64(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt);
         if (step == 0 || metropolis64(w, tmp_e, cand_e, P.temperature)) {
             vcopy(w, tmp, cand, m.conf_size);
             tmp_e = cand_e;
             set_conf64(w, tmp);
             const int count = *ch.out_count;
             if (tmp_e < best_e || count < P.num_saved) {
-                tmp_e = bfgs64(w, tmp, P.maxiters, P.accurate_line, P.early_term, auth);
+                tmp_e = bfgs64(w, tmp, ch.maxiters, P.accurate_line, P.early_term, auth);
                 set_conf64(w, tmp);
                 add_to_output64(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved);
                 if (tmp_e < best_e) best_e = tmp_e;

@@ -273,6 +273,7 @@ SG_HD Ws64 ws64_layout(int natoms, int nframes, int npairs, int conf, int dof) {
 struct Chain64 {
     int model;
     unsigned steps;
+    int maxiters;
     const double* conf0;
     uint32_t* mt;        // [625] state (read + written)
     double* out_e;       // [num_saved]

@@ -4,6 +4,9 @@
  * descriptors of include/smina_b200.h.  Errors come back as a non-zero
  * status with a message in sgh_last_error().
  */
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -117,6 +120,49 @@ int sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims*
             std::memcpy(confs + (size_t)k * m->m.conf_size, cs[k].conf.data(), m->m.conf_size * sizeof(double));
             std::memcpy(mt + (size_t)k * 625, cs[k].mt, 625 * sizeof(uint32_t));
         }
+    });
+}
+
+// merge_output_containers (parallel_mc.cpp:64-76): every chain's poses in
+// chain order through add_to_output_container (coords.cpp:25-58)
+int sgh_merge_chains(const sg_chain_result* chains, int nchains, int conf_size, int nheavy, double min_rmsd,
+                     int max_size, double* out_e, double* out_conf, double* out_coords, int* out_count) {
+    return guarded([&] {
+        if (!chains || nchains < 0 || conf_size <= 0 || nheavy < 0 || max_size <= 0 || !out_e || !out_conf ||
+            !out_coords || !out_count)
+            throw std::runtime_error("merge: bad arguments");
+        struct Pose { double e; std::vector<double> c, x; };
+        std::vector<Pose> out;
+        const size_t H3 = (size_t)nheavy * 3;
+        for (int k = 0; k < nchains; k++)
+            for (int j = 0; j < chains[k].count; j++) {
+                Pose t;
+                t.e = chains[k].e[j];
+                t.c.assign(chains[k].conf + (size_t)j * conf_size, chains[k].conf + (size_t)(j + 1) * conf_size);
+                t.x.assign(chains[k].coords + j * H3, chains[k].coords + (j + 1) * H3);
+                size_t ci = out.size();
+                double cr = DBL_MAX;
+                for (size_t i = 0; i < out.size(); i++) {
+                    double acc = 0;
+                    for (size_t a = 0; a < H3; a++) acc += (t.x[a] - out[i].x[a]) * (t.x[a] - out[i].x[a]);
+                    const double r = H3 ? std::sqrt(acc / (double)nheavy) : 0.0;
+                    if (i == 0 || r < cr) { ci = i; cr = r; }
+                }
+                if (ci < out.size() && cr < min_rmsd) {
+                    if (t.e < out[ci].e) out[ci] = std::move(t);
+                } else if ((int)out.size() < max_size) {
+                    out.push_back(std::move(t));
+                } else if (!out.empty() && t.e < out.back().e) {
+                    out.back() = std::move(t);
+                }
+                std::stable_sort(out.begin(), out.end(), [](const Pose& a, const Pose& b) { return a.e < b.e; });
+            }
+        for (size_t i = 0; i < out.size(); i++) {
+            out_e[i] = out[i].e;
+            std::memcpy(out_conf + i * conf_size, out[i].c.data(), conf_size * sizeof(double));
+            std::memcpy(out_coords + i * H3, out[i].x.data(), H3 * sizeof(double));
+        }
+        *out_count = (int)out.size();
     });
 }
 

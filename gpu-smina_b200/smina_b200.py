@@ -65,7 +65,7 @@ class MCParams(C.Structure):
 
 
 class ChainInput(C.Structure):
-    _fields_ = [("model", C.c_int), ("num_steps", C.c_uint), ("conf", _dp), ("mt", _up)]
+    _fields_ = [("model", C.c_int), ("num_steps", C.c_uint), ("conf", _dp), ("mt", _up), ("maxiters", C.c_int)]
 
 
 class ChainResult(C.Structure):
@@ -123,6 +123,8 @@ def _declare(L):
         "sgh_make_box": [C.c_double * 3, C.c_double * 3, C.c_double, C.POINTER(GridDims)],
         "sgh_search_params": [vp, C.c_int, C.POINTER(MCParams)],
         "sgh_seed_chains": [vp, C.c_int, C.c_int, C.POINTER(GridDims), _dp, _up],
+        "sgh_merge_chains": [C.POINTER(ChainResult), C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp, _dp,
+                             _ip],
         "sg_create": [C.c_int, C.c_int, C.POINTER(vp)],
         "sg_set_tables": [vp, C.POINTER(TablesDesc)],
         "sg_set_receptor": [vp, C.c_int, C.POINTER(ReceptorDesc), C.POINTER(GridDims)],
@@ -310,7 +312,7 @@ class ChainBatch:
     count: np.ndarray = None
 
 
-def make_chain_batch(models, model_of_chain, confs, mts, steps, num_saved, heavy_of_model):
+def make_chain_batch(models, model_of_chain, confs, mts, steps, num_saved, heavy_of_model, maxiters=None):
     n = len(model_of_chain)
     ins = (ChainInput * n)()
     outs = (ChainResult * n)()
@@ -326,12 +328,26 @@ def make_chain_batch(models, model_of_chain, confs, mts, steps, num_saved, heavy
         keep += [c, m]
         ins[k].model = int(model_of_chain[k])
         ins[k].num_steps = int(steps[k] if hasattr(steps, "__len__") else steps)
+        ins[k].maxiters = int(maxiters[k]) if maxiters is not None else 0
         ins[k].conf = dptr(c)
         ins[k].mt = uptr(m)
         outs[k].e = e[k].ctypes.data_as(_dp)
         outs[k].conf = conf[k].ctypes.data_as(_dp)
         outs[k].coords = coords[k].ctypes.data_as(_dp)
     return ChainBatch(ins, outs, keep, e, conf, coords)
+
+
+def merge_chains(batch, model, first=0, n=None, min_rmsd=2.0, max_size=20):
+    """merge_output_containers over chains [first, first + n) of a ChainBatch."""
+    n = len(batch.count) - first if n is None else n
+    e = np.zeros(max_size)
+    conf = np.zeros((max_size, model.conf_size))
+    xyz = np.zeros((max_size, model.heavy, 3))
+    cnt = C.c_int()
+    res = C.cast(C.byref(batch.results, first * C.sizeof(ChainResult)), C.POINTER(ChainResult))
+    _check_host(load().sgh_merge_chains(res, n, model.conf_size, model.heavy, min_rmsd, max_size, dptr(e), dptr(conf),
+                                        dptr(xyz), C.byref(cnt)))
+    return e[:cnt.value], conf[:cnt.value], xyz[:cnt.value]
 
 
 # ---- engine ---------------------------------------------------------------------------
@@ -394,11 +410,12 @@ class Engine:
                                    accurate, early, dptr(e)))
         return confs, e
 
-    def dock(self, rid, models, model_of_chain, confs, mts, params: MCParams, steps=None):
+    def dock(self, rid, models, model_of_chain, confs, mts, params: MCParams, steps=None, maxiters=None):
+        """Plain FP64 chains (sg_dock); steps and maxiters may be per chain."""
         descs = (ModelDesc * len(models))(*[m.desc for m in models])
         heavy = [m.heavy for m in models]
         batch = make_chain_batch(models, model_of_chain, confs, mts,
-                                 params.num_steps if steps is None else steps, params.num_saved_mins, heavy)
+                                 params.num_steps if steps is None else steps, params.num_saved_mins, heavy, maxiters)
         self._check(load().sg_dock(self._h, rid, descs, len(models), batch.inputs, len(model_of_chain),
                                    C.byref(params), batch.results))
         batch.count = np.array([batch.results[k].count for k in range(len(model_of_chain))])

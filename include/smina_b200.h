@@ -161,6 +161,8 @@ typedef struct sg_chain_input {
     unsigned num_steps;
     const double* conf; /* [conf_size]                                   */
     const uint32_t* mt; /* [625]: state words then index (0..624)        */
+    int maxiters;       /* BFGS iterations; 0: sg_mc_params.maxiters
+                           (ChainInput::maxiters, gpu_kernels.h)         */
 } sg_chain_input;
 
 /* Result container of one chain (output_container, sorted ascending). */

@@ -61,6 +61,12 @@ int  sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out);
 /* confs [tasks][conf_size], mt [tasks][625] */
 int  sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims* box, double* confs, uint32_t* mt);
 
+/* merge_output_containers (parallel_mc.cpp:64-76): the chains' sorted
+ * containers merged in chain order with the given min_rmsd (2 in
+ * parallel_mc) into at most max_size poses; out arrays sized max_size. */
+int  sgh_merge_chains(const sg_chain_result* chains, int nchains, int conf_size, int nheavy, double min_rmsd,
+                      int max_size, double* out_e, double* out_conf, double* out_coords, int* out_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,7 +153,9 @@ int or_dock(or_ctx* o, const sg_model_desc* models, int nmodels, const sg_chain_
             Container c;
             uint64_t evals = 0;
             try {
-                mc_chain(o->c, m, *p, ci.conf, gen, ci.num_steps, c, &evals);
+                sg_mc_params pc = *p;  // a chain's own BFGS iteration count, if it has one
+                if (ci.maxiters > 0) pc.maxiters = ci.maxiters;
+                mc_chain(o->c, m, pc, ci.conf, gen, ci.num_steps, c, &evals);
             } catch (std::exception& e) {
                 failed = 1;
                 errmsg = e.what();

@@ -120,11 +120,11 @@ class Oracle:
                                    accurate, early, sb.dptr(e)))
         return confs, e
 
-    def dock(self, models, model_of_chain, confs, mts, params, steps=None, threads=1):
+    def dock(self, models, model_of_chain, confs, mts, params, steps=None, threads=1, maxiters=None):
         self.ensure(models)
         descs = (sb.ModelDesc * len(models))(*[m.desc for m in models])
         batch = sb.make_chain_batch(models, model_of_chain, confs, mts, params.num_steps if steps is None else steps,
-                                    params.num_saved_mins, [m.heavy for m in models])
+                                    params.num_saved_mins, [m.heavy for m in models], maxiters)
         self._check(load().or_dock(self.h, descs, len(models), batch.inputs, len(model_of_chain), C.byref(params),
                                    batch.results, threads))
         batch.count = np.array([batch.results[k].count for k in range(len(model_of_chain))])

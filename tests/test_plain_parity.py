@@ -109,6 +109,30 @@ def test_mc_chains_bit_exact(setup, heavy, rotors, seed, steps):
         assert_bitwise(b1.coords[k, :c, :m.heavy], b0.coords[k, :c, :m.heavy], f"chain {k} coords")
 
 
+def test_mixed_ligands_with_own_iteration_counts_bit_exact(setup):
+    """Chains of several ligands in one launch, each with its ligand's own
+    step and BFGS-iteration counts (ChainInput::maxiters)."""
+    eng, orc, gd = setup
+    models = [W.ligand(24, 5, 11), W.ligand(12, 0, 3), W.ligand(40, 10, 5)]
+    p = models[0].search_params()
+    confs, mts, moc, steps, its = [], [], [], [], []
+    for k, m in enumerate(models):
+        c, mt = m.seed_chains(50 + k, 2, gd)
+        cm = np.zeros((2, max(x.conf_size for x in models)))
+        cm[:, :m.conf_size] = c
+        confs += list(cm)
+        mts += list(mt)
+        moc += [k, k]
+        steps += [8 + 3 * k] * 2
+        its += [m.search_params().maxiters] * 2
+    b1 = eng.dock(0, models, moc, confs, mts, p, steps=steps, maxiters=its)
+    b0 = orc.dock(models, moc, confs, mts, p, steps=steps, maxiters=its, threads=6)
+    assert (b1.count == b0.count).all() and (b1.evals == b0.evals).all()
+    assert_bitwise(b1.e, b0.e, "energies")
+    e, conf, _ = sb.merge_chains(b1, models[2], first=4, n=2)
+    assert len(e) > 0 and np.all(np.diff(e) >= 0)
+
+
 def test_refine_bit_exact(setup):
     eng, orc, gd = setup
     m = W.ligand()
