@@ -104,11 +104,12 @@ def make_params(models):
     return p
 
 
-def jobs_for(models, idx, exh, seed, key_base):
+def jobs_for(models, idx, exh, seed, key_base, step_scale=1.0):
     jobs = []
     for j, k in enumerate(idx):
         sp = models[k].search_params(9)
-        jobs.append(sb.LigandJob(model=k, num_chains=exh, num_steps=sp.num_steps, maxiters=sp.maxiters,
+        steps = max(1, int(sp.num_steps * step_scale)) if step_scale != 1.0 else sp.num_steps
+        jobs.append(sb.LigandJob(model=k, num_chains=exh, num_steps=steps, maxiters=sp.maxiters,
                                  seed=seed, ligand_key=key_base + k))
     return jobs
 
@@ -288,6 +289,8 @@ def main():
     ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--step-scale", type=float, default=1.0,
+                    help="scale every ligand's Monte Carlo step count (profiling cases; 1 = smina's counts)")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="instead of timing: top-score agreement FP32 vs FP64 on this many ligands")
     args = ap.parse_args()
@@ -322,7 +325,7 @@ def main():
 
     def step(s):
         idx = list(range((s % nb) * B, (s % nb) * B + B))
-        jobs = jobs_for(models, idx, args.exhaustiveness, args.seed, key_base)
+        jobs = jobs_for(models, idx, args.exhaustiveness, args.seed, key_base, args.step_scale)
         sub = [models[k] for k in idx]
         for j, jb in enumerate(jobs):
             jb.model = j
@@ -380,7 +383,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), "
                                    f"receptor 3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness "
-                                   f"{args.exhaustiveness}, smina step counts, {B} ligands per step",
+                                   f"{args.exhaustiveness}, smina step counts"
+                                   + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
+                                   + f", {B} ligands per step",
                        "precision": args.precision, "ligands_per_step": B, "global_batch": B * world,
                        "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)",
                        "chains_per_block": recs[-1][2]["chains_per_block"], "blocks": recs[-1][2]["blocks"]},

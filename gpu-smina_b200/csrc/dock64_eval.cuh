@@ -25,6 +25,7 @@ struct W64 {
     int lane;
     int* err;
     unsigned long long evals;
+    const double* box;  // this item's own box (lo xyz, hi xyz) for the direct sum; null: the receptor's
 };
 
 __device__ __forceinline__ V3<double> ld3(const double* p) { return {p[0], p[1], p[2]}; }
@@ -186,9 +187,10 @@ __device__ void direct_atoms64(W64& w, double v, double slope) {
         const double a[3] = {S[w.L.coords + 3 * i], S[w.L.coords + 3 * i + 1], S[w.L.coords + 3 * i + 2]};
         double adj[3] = {a[0], a[1], a[2]}, oobd[3] = {0, 0, 0}, oob = 0;
         for (int j = 0; j < 3; j++) {
-            if (G.gd_n[j] > 0) {
-                if (a[j] < G.gd_begin[j]) { adj[j] = G.gd_begin[j]; oobd[j] = -1; oob += fabs(a[j] - G.gd_begin[j]); }
-                else if (a[j] > G.gd_end[j]) { adj[j] = G.gd_end[j]; oobd[j] = 1; oob += fabs(a[j] - G.gd_end[j]); }
+            const double lo = w.box ? w.box[j] : G.gd_begin[j], hi = w.box ? w.box[3 + j] : G.gd_end[j];
+            if (w.box || G.gd_n[j] > 0) {
+                if (a[j] < lo) { adj[j] = lo; oobd[j] = -1; oob += fabs(a[j] - lo); }
+                else if (a[j] > hi) { adj[j] = hi; oobd[j] = 1; oob += fabs(a[j] - hi); }
             }
         }
         oob *= slope;

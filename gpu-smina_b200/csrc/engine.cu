@@ -235,6 +235,18 @@ static void cell_bricks(const DGeom& g, bool first_query, std::vector<double>& l
     }
 }
 
+// the receptor's 3 A cell lists (first-query bricks for the maps, full
+// bricks for the direct sum), built once
+void ensure_cells(sg_engine* e, RecState& r) {
+    if (r.pop_start.p) return;
+    std::vector<double> lo, hi;
+    cell_bricks(r.geom, true, lo, hi);
+    build_cells(e, r, lo, hi, r.pop_start, r.pop_atoms);
+    cell_bricks(r.geom, false, lo, hi);
+    build_cells(e, r, lo, hi, r.full_start, r.full_atoms);
+    refresh_header(e, r);
+}
+
 void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes) {
     require(e->has_tables, "no tables set");
     std::vector<int> need;
@@ -244,13 +256,7 @@ void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes) {
         if (!r.built[t] && std::find(need.begin(), need.end(), t) == need.end()) need.push_back(t);
     }
     if (need.empty()) return;
-    if (!r.pop_start.p) {
-        std::vector<double> lo, hi;
-        cell_bricks(r.geom, true, lo, hi);
-        build_cells(e, r, lo, hi, r.pop_start, r.pop_atoms);
-        cell_bricks(r.geom, false, lo, hi);
-        build_cells(e, r, lo, hi, r.full_start, r.full_atoms);
-    }
+    ensure_cells(e, r);
     const size_t npts = (size_t)r.geom.dim[0] * r.geom.dim[1] * r.geom.dim[2];
     const bool charged = e->tables.nc > 1;
     std::vector<double*> maps, cmaps;
@@ -540,10 +546,10 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
             int fill[4] = {};
         };
         std::vector<Chunk> chunks;
-        const bool packable = M <= 255;
+        const bool packable = N <= 255;  // 8-bit atom indices (inflex atoms take part in pairs too)
         for (int k = 0; k < P && packable; k++) {
             const int u = d.pairs[2 * k], v = d.pairs[2 * k + 1];
-            require(u >= 0 && v >= 0 && u < M && v < M && u != v, "model: pair atoms must be distinct movable atoms");
+            require(u >= 0 && v >= 0 && u < N && v < N && u != v, "model: pair atoms must be distinct atoms");
             require((pair_tp[k] & 0x1ff) < (int)kSlotPairMask, "model: type pair index out of range");
             const uint32_t base = ((uint32_t)(pair_tp[k] & 0x1ff) << 16) | ((pair_tp[k] >> 30) & 1 ? kSlotSwap : 0) |
                                   (k >= d.num_other_pairs ? kSlotIntra : 0);
@@ -567,8 +573,8 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
             if (!placed) {
                 chunks.emplace_back();
                 Chunk& ch = chunks.back();
-                ch.out_used.assign(M, 0);
-                ch.in_used.assign(M, 0);
+                ch.out_used.assign(N, 0);
+                ch.in_used.assign(N, 0);
                 for (uint32_t& x : ch.slot) x = kSlotEmpty;
                 ch.out_used[u] = ch.in_used[v] = 1;
                 ch.amod[0] = 1 << (u & 7);
@@ -738,6 +744,7 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
         PackedModels pm;
         pack_models(e, m, 1, pm);
         if (!direct) ensure_model_maps(e, r, pm, m, 1);
+        else ensure_cells(e, r);
         require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
         const DModel& h = pm.host[0];
         Staged<double> dc, de, dg, dx;
@@ -746,7 +753,7 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
         dg.make((size_t)nconfs * h.dof, e->stream);
         if (out_coords) dx.make((size_t)nconfs * h.nmov * 3, e->stream);
         if (!direct && e->precision != SG_PREC_FP64) {  // the mixed-precision evaluation
-            require(h.npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 atoms per model");
             const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
             const size_t stage =
                 (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
@@ -909,6 +916,7 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
     return guarded(e, [&] {
         require(pose_model && confs && cap && out_e && nposes > 0 && maxiters >= 0, "refine: bad arguments");
         RecState& r = receptor_for(e, rid);
+        ensure_cells(e, r);
         PackedModels pm;
         pack_models(e, models, nmodels, pm);
         require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
@@ -921,9 +929,48 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
         dx.make((size_t)nposes * hs * 3, e->stream);
         dpm.make(nposes, e->stream, pose_model);
         cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(), nposes,
-                                   dc.p(), cs, cap, maxiters, nullptr, accurate_line, early_term, de.p(), dx.p(), hs,
+                                   dc.p(), cs, cap, maxiters, nullptr, nullptr, accurate_line, early_term, de.p(), dx.p(), hs,
                                    e->d_err.as<int>(), e->stream),
                    "refine launch");
+        dc.fetch(confs, e->stream);
+        de.fetch(out_e, e->stream);
+        if (out_coords) dx.fetch(out_coords, e->stream);
+        e->check_device_errors();
+    });
+}
+
+int sg_minimize(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const int* pose_model, int nposes,
+                double* confs, int conf_stride, const double* boxes, const double cap[3], const int* maxiters,
+                int accurate_line, int early_term, double* out_e, double* out_coords, int coord_stride) {
+    return guarded(e, [&] {
+        require(pose_model && confs && cap && maxiters && out_e && nposes > 0, "minimize: bad arguments");
+        RecState& r = receptor_for(e, rid);
+        ensure_cells(e, r);
+        PackedModels pm;
+        pack_models(e, models, nmodels, pm);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        require(conf_stride >= pm.max_conf && coord_stride >= pm.max_heavy, "minimize: strides too small");
+        for (int k = 0; k < nposes; k++) {
+            require(pose_model[k] >= 0 && pose_model[k] < nmodels && maxiters[k] >= 0, "minimize: bad pose");
+            if (boxes)  // a pose's box must lie inside the receptor's, where its cell lists are
+                for (int d = 0; d < 3; d++)
+                    require(boxes[6 * k + d] >= r.gd.begin[d] && boxes[6 * k + 3 + d] <= r.gd.end[d] &&
+                                boxes[6 * k + d] <= boxes[6 * k + 3 + d],
+                            "minimize: a pose's box must lie inside the receptor's box");
+        }
+        Staged<double> dc, de, dx, db;
+        Staged<int> dpm, dmi;
+        dc.make((size_t)nposes * conf_stride, e->stream, confs);
+        de.make(nposes, e->stream);
+        dx.make((size_t)nposes * coord_stride * 3, e->stream);
+        dpm.make(nposes, e->stream, pose_model);
+        dmi.make(nposes, e->stream, maxiters);
+        if (boxes) db.make((size_t)nposes * 6, e->stream, boxes);
+        cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(),
+                                   nposes, dc.p(), conf_stride, cap, 0, dmi.p(), boxes ? db.p() : nullptr,
+                                   accurate_line, early_term, de.p(), dx.p(), coord_stride, e->d_err.as<int>(),
+                                   e->stream),
+                   "minimize launch");
         dc.fetch(confs, e->stream);
         de.fetch(out_e, e->stream);
         if (out_coords) dx.fetch(out_coords, e->stream);

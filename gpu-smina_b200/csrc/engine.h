@@ -127,7 +127,8 @@ cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor
 cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
                         const MCParams64&, int*, cudaStream_t);
 cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
-                            const double[3], int, const int*, int, int, double*, double*, int, int*, cudaStream_t);
+                            const double[3], int, const int* pose_maxiters, const double* pose_box, int, int, double*,
+                            double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
 int mc32_occupancy(int wpb, size_t smem);
 cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
@@ -147,6 +148,7 @@ struct ModelImage {
 };
 void pack_models_image(const sg_model_desc* models, int nmodels, char* dev_base, ModelImage& img);
 RecState& receptor_for(sg_engine* e, int rid);
+void ensure_cells(sg_engine* e, RecState& r);
 void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes);
 void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels);
 void refresh_header(sg_engine* e, RecState& r);

@@ -126,7 +126,7 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         uint64_t h2d = pm.ints.bytes + pm.flts.bytes + pm.dbls.bytes + pm.dmodels.bytes, d2h = 0;
         size_t ws_stride = 0, stage_stride = 0;
         for (const DModel& h : pm.host) {
-            require(h.npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 atoms per model");
             ws_stride = std::max(ws_stride, ws32_bytes(h));
             stage_stride = std::max(stage_stride, (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks,
                                                                         h.nlig, h.nblocks, h.ntors));
@@ -308,7 +308,7 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
                 cuda_check(cudaEventRecord(ev[2], e->stream), "event");
                 cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(),
                                            dpm.as<int>(), nposes, dc.as<double>(), cs, p->authentic_v, p->maxiters,
-                                           dmi.as<int>(), p->accurate_line, p->early_term, de.as<double>(),
+                                           dmi.as<int>(), nullptr, p->accurate_line, p->early_term, de.as<double>(),
                                            dx.as<double>(), hs, e->d_err.as<int>(), e->stream),
                            "refine launch");
                 cuda_check(cudaEventRecord(ev[3], e->stream), "event");

@@ -630,6 +630,7 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
     const Ws32& L = m.L;
     unsigned* C = w.counters();
     for (int i = w.lane; i < 65; i += 32) C[i] = 0;
+    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);  // inflex atoms stay here
     copyd(w, w.d(L.x_tmp), confs + (size_t)k * m.conf_size, m.conf_size);
     const float e = eval_deriv32(w.at(L.x_tmp), make_float3(v0, v1, v2), slope, w.at(L.g));
     const double* g = w.d(L.g);

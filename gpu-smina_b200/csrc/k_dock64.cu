@@ -14,6 +14,7 @@ __device__ void init_ws64(W64& w, const DModel* m, const DTables* T, const DRece
     w.err = err;
     w.lane = threadIdx.x & 31;
     w.evals = 0;
+    w.box = nullptr;
     w.L = ws64_layout(m->natoms, m->nframes, m->npairs, m->conf_size, m->dof);
     w.pin = reinterpret_cast<uint8_t*>(w.s + w.L.pin);
     w.mt = reinterpret_cast<uint32_t*>(w.s + w.L.mt);
@@ -116,9 +117,10 @@ __device__ bool within64(W64& w, double margin) {
     for (int i = w.lane; i < m.nmov; i += 32) {
         if (is_h(m.type[i])) continue;
         for (int j = 0; j < 3; j++)
-            if (G.gd_n[j] > 0) {
+            if (w.box || G.gd_n[j] > 0) {
                 const double c = w.s[w.L.coords + 3 * i + j];
-                if (c < G.gd_begin[j] - margin || c > G.gd_end[j] + margin) ok = false;
+                const double lo = w.box ? w.box[j] : G.gd_begin[j], hi = w.box ? w.box[3 + j] : G.gd_end[j];
+                if (c < lo - margin || c > hi + margin) ok = false;
             }
     }
     return __all_sync(kFull, ok);
@@ -128,8 +130,8 @@ __device__ bool within64(W64& w, double margin) {
 __global__ void __launch_bounds__(32) k_refine64(const DModel* models, DTables T, const DReceptor* R,
                                                  const int* pose_model, int nposes, double* confs, int conf_stride,
                                                  double c0, double c1, double c2, int maxiters, const int* pose_maxiters,
-                                                 int accurate, int early, double* out_e, double* out_coords,
-                                                 int coord_stride, int* err) {
+                                                 const double* pose_box, int accurate, int early, double* out_e,
+                                                 double* out_coords, int coord_stride, int* err) {
     const int k = blockIdx.x;
     if (k >= nposes) return;
     const DModel* mp = models + pose_model[k];
@@ -139,6 +141,7 @@ __global__ void __launch_bounds__(32) k_refine64(const DModel* models, DTables T
     double* x = w.s + w.L.x_tmp;
     vcopy(w, x, confs + (size_t)k * conf_stride, m.conf_size);
     if (pose_maxiters) maxiters = pose_maxiters[k];  // per-ligand iteration limit
+    if (pose_box) w.box = pose_box + 6 * (size_t)k;  // the pose's own box
     double slope = 10;
     double e = 0;
     for (int p = 0; p < 5; p++) {
@@ -194,12 +197,12 @@ cudaError_t launch_mc64(const DModel* dms, size_t smem, const DTables& T, const 
 
 cudaError_t launch_refine64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const int* pose_model,
                             int n, double* confs, int conf_stride, const double cap[3], int maxiters,
-                            const int* pose_maxiters, int accurate, int early, double* e, double* coords,
-                            int coord_stride, int* err, cudaStream_t s) {
+                            const int* pose_maxiters, const double* pose_box, int accurate, int early, double* e,
+                            double* coords, int coord_stride, int* err, cudaStream_t s) {
     cudaError_t rc = prep((const void*)k_refine64, smem);
     if (rc != cudaSuccess) return rc;
     k_refine64<<<n, 32, smem, s>>>(dms, T, R, pose_model, n, confs, conf_stride, cap[0], cap[1], cap[2], maxiters,
-                                   pose_maxiters, accurate, early, e, coords, coord_stride, err);
+                                   pose_maxiters, pose_box, accurate, early, e, coords, coord_stride, err);
     return cudaGetLastError();
 }
 

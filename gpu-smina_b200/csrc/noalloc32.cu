@@ -111,7 +111,7 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
         require(models_at == 0, "fixed scratch: models must start the array");
         // the maps must already be resident: building them would allocate
         for (int k = 0; k < nmodels; k++) {
-            require(img.host[k].npchunks >= 0, "mixed-precision path: at most 255 movable atoms per model");
+            require(img.host[k].npchunks >= 0, "mixed-precision path: at most 255 atoms per model");
             for (int i = 0; i < models[k].num_movable; i++) {
                 const int t = models[k].atom_type[i];
                 if (t >= kNumTypes || is_h(t)) continue;

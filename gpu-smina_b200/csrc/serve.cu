@@ -463,7 +463,7 @@ static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& 
         if (n > 0) {
             const sg_mc_params& P = members[0].second->req.p;
             cuda_check(launch_refine64(d_models, ws, e->tables, e->rec[rid].dhdr.as<DReceptor>(), dpm + p0, n,
-                                       dc + (size_t)p0 * g->cs, g->cs, P.authentic_v, P.maxiters, dmi + p0,
+                                       dc + (size_t)p0 * g->cs, g->cs, P.authentic_v, P.maxiters, dmi + p0, nullptr,
                                        P.accurate_line, P.early_term, de + p0, dx + (size_t)p0 * g->hs * 3, g->hs,
                                        s.d_err, rs),
                        "serve: refine launch");
@@ -709,7 +709,7 @@ int sg_serve_submit(sg_engine* e, int rid, const sg_model_desc* m, const sg_liga
         require(m && job && p && ticket, "serve: bad arguments");
         require(job->num_chains >= 1 && job->num_chains <= 4096 && job->maxiters >= 0, "serve: bad ligand job");
         require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->temperature > 0, "serve: bad search parameters");
-        require(m->num_movable <= 255, "mixed-precision path: at most 255 movable atoms per model");
+        require(m->num_atoms <= 255, "mixed-precision path: at most 255 atoms per model");
         RecState& r = receptor_for(e, rid);
         ServeReq q;
         q.m = std::make_shared<ModelCopy>(*m);

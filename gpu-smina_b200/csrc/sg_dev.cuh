@@ -104,7 +104,7 @@ struct __align__(16) DModel {
     // Slot: a | b << 8 | type pair << 16 | swapped << 25 | intramolecular
     // (v[0]) << 26; unused slots kSlotEmpty (type pair 0x1ff, atoms 0 and 0,
     // so their loads stay in range).  Null when the model has more
-    // than 255 movable atoms.
+    // than 255 atoms.
     const uint32_t* pslot;    // [npchunks * 32]
     int cost;                 // relative cost of one evaluation (atoms + pairs + frames)
     int npchunks;

@@ -47,6 +47,24 @@ int sgh_model_from_pdbqt(const char* text, sgh_model** out) {
     });
 }
 void sgh_model_free(sgh_model* m) { delete m; }
+int sgh_model_from_pdbqt_flex(const char* ligand_text, const char* flex_text, sgh_model** out) {
+    *out = nullptr;
+    return guarded([&] {
+        if (!ligand_text || !flex_text) throw std::runtime_error("model: null text");
+        auto* m = new sgh_model{sgh::read_pdbqt_flex(ligand_text, flex_text)};
+        *out = m;
+    });
+}
+
+int sgh_make_flex_pdbqt(int residues, uint64_t seed, const double center[3], double shell, char* buf, int buflen) {
+    std::string t;
+    int rc = guarded([&] { t = sgh::make_flex_pdbqt(residues, seed, center, shell > 0 ? shell : 9.0); });
+    if (rc) return -1;
+    if ((int)t.size() + 1 > buflen) return (int)t.size() + 1;
+    std::memcpy(buf, t.c_str(), t.size() + 1);
+    return 0;
+}
+
 int sgh_model_desc(const sgh_model* m, sg_model_desc* out) {
     *out = m->m.desc();
     return SG_OK;

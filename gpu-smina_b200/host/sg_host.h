@@ -109,6 +109,10 @@ struct Model {
 // does, types it (model.cpp:448-566) and builds its pairs (model.cpp:598-624).
 // Throws std::runtime_error on malformed input.
 Model read_pdbqt_ligand(const std::string& text);
+// A ligand with the receptor's flexible residues (smina --flex): residues in
+// PDBQT BEGIN_RES/END_RES blocks (parse_pdbqt.cpp:412-437), the ligand
+// appended as model::append does.
+Model read_pdbqt_flex(const std::string& ligand_text, const std::string& flex_text);
 
 // ---- synthetic workloads ---------------------------------------------------
 struct Receptor {
@@ -122,6 +126,10 @@ std::string receptor_pdbqt(const Receptor& r);
 // Acyclic drug-like ligand: `heavy` heavy atoms, exactly `rotors` torsions,
 // placed near `center`; returned as PDBQT text.
 std::string make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3]);
+// `residues` flexible side chains with 2..4 chi torsions each, CA on a shell
+// of radius `shell` around `center`, side chains pointing into the cavity;
+// returned as flex PDBQT (BEGIN_RES ... END_RES).
+std::string make_flex_pdbqt(int residues, uint64_t seed, const double center[3], double shell = 9.0);
 
 // grid_dims for a cubic box of `size` A at granularity 0.375 (main.cpp:801-809)
 sg_grid_dims make_box(const double center[3], const double size[3], double granularity = 0.375);

@@ -395,6 +395,99 @@ std::string make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double
     throw std::runtime_error("could not place a ligand with the requested rotors");
 }
 
+// ---- flexible residues ---------------------------------------------------------------
+std::string make_flex_pdbqt(int residues, uint64_t seed, const double center[3], double shell) {
+    if (residues < 1 || residues > 32) throw std::runtime_error("flexible residues: 1..32");
+    Rng r(seed * 7919ull + 17);
+    const P3 c{center[0], center[1], center[2]};
+    std::string out;
+    std::vector<P3> placed;  // every side-chain atom so far, for spacing
+    int serial = 1;
+    auto line = [&](int n, const char* name, const char* res, int resnum, const P3& p, double q, const char* ad) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "ATOM  %5d  %-3s %3s A%4d    %8.3f%8.3f%8.3f  1.00  0.00    %+6.3f %-2s\n", n,
+                      name, res, resnum, p.x, p.y, p.z, q, ad);
+        out += buf;
+    };
+    static const char* names[] = {"CB", "CG", "CD", "CE", "CZ"};
+    for (int k = 0; k < residues; k++) {
+        const int chis = 2 + (int)r.below(3);  // 2..4
+        // the residue's CA on the shell, directions spread over the sphere
+        P3 dir{0, 0, 0};
+        for (int t = 0; t < 200; t++) {
+            P3 d = rand_unit(r);
+            bool ok = true;
+            for (const P3& q : placed) {
+                P3 e = (c + shell * d) - q;
+                if (dotp(e, e) < 5.0 * 5.0) { ok = false; break; }
+            }
+            dir = d;
+            if (ok) break;
+        }
+        std::vector<P3> pos{c + shell * dir};
+        P3 back = unit(pos[0] - c);  // points away from the centre
+        pos.push_back(pos[0] + 1.53 * (-1.0 * back));
+        for (int a = 2; a < chis + 2; a++) {  // X2 .. X(chis+1), growing into the cavity
+            P3 best{0, 0, 0};
+            double best_d = 1e30;
+            const P3 b = unit(pos[a - 2] - pos[a - 1]);
+            for (int t = 0; t < 24; t++) {
+                P3 q = pos[a - 1] + 1.53 * cone_dir(b, 109.5 * M_PI / 180, 2 * M_PI * r.uni(), r);
+                bool ok = true;
+                for (int i = 0; i + 2 < a && ok; i++) {
+                    P3 e = pos[i] - q;
+                    if (dotp(e, e) < 2.4 * 2.4) ok = false;
+                }
+                for (const P3& o : placed) {
+                    P3 e = o - q;
+                    if (dotp(e, e) < 3.2 * 3.2) { ok = false; break; }
+                }
+                P3 e = q - c;
+                const double dc = dotp(e, e) + (ok ? 0 : 1e6);
+                if (dc < best_d) { best_d = dc; best = q; }
+            }
+            pos.push_back(best);
+        }
+        const bool amine = r.uni() < 0.5;  // terminal N-H or O-H
+        const P3 hdir = unit(pos.back() - pos[pos.size() - 2]);
+        const P3 h = pos.back() + 1.0 * hdir;
+        const int resnum = 10 + 7 * k;
+        const char* res = amine ? "LYS" : "SER";
+        char head[64];
+        std::snprintf(head, sizeof head, "BEGIN_RES %s A%4d\n", res, resnum);
+        out += head;
+        out += "ROOT\n";
+        const int ca = serial++;
+        line(ca, "CA", res, resnum, pos[0], 0.0, "C");
+        out += "ENDROOT\n";
+        std::vector<int> sn(pos.size());
+        sn[0] = ca;
+        for (size_t a = 1; a < pos.size(); a++) sn[a] = serial++;
+        const int hs = serial++;
+        const int last = (int)pos.size() - 1;  // X(chis+1)
+        for (int b = 1; b <= chis; b++) {  // BRANCH X(b-1) X(b)
+            char br[64];
+            std::snprintf(br, sizeof br, "BRANCH %3d %3d\n", sn[b - 1], sn[b]);
+            out += br;
+            const bool tip = b == last - 1;
+            line(sn[b], names[b - 1], res, resnum, pos[b], 0.0, "C");
+            if (tip) {
+                line(sn[last], amine ? "NZ" : "OG", res, resnum, pos[last], amine ? -0.3 : -0.4, amine ? "N" : "OA");
+                line(hs, amine ? "HZ" : "HG", res, resnum, h, 0.2, "HD");
+            }
+        }
+        for (int b = chis; b >= 1; b--) {
+            char br[64];
+            std::snprintf(br, sizeof br, "ENDBRANCH %3d %3d\n", sn[b - 1], sn[b]);
+            out += br;
+        }
+        std::snprintf(head, sizeof head, "END_RES %s A%4d\n", res, resnum);
+        out += head;
+        for (const P3& q : pos) placed.push_back(q);
+    }
+    return out;
+}
+
 sg_grid_dims make_box(const double center[3], const double size[3], double granularity) {
     sg_grid_dims gd;
     for (int i = 0; i < 3; i++) {

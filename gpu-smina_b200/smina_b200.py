@@ -118,6 +118,8 @@ def _declare(L):
         "sgh_receptor_desc": [vp, C.POINTER(ReceptorDesc)],
         "sgh_receptor_pdbqt": [vp, C.c_char_p, C.c_int],
         "sgh_make_ligand_pdbqt": [C.c_int, C.c_int, C.c_uint64, C.c_double * 3, C.c_char_p, C.c_int],
+        "sgh_make_flex_pdbqt": [C.c_int, C.c_uint64, C.c_double * 3, C.c_double, C.c_char_p, C.c_int],
+        "sgh_model_from_pdbqt_flex": [C.c_char_p, C.c_char_p, C.POINTER(vp)],
         "sgh_tables_create": [C.c_char_p, C.c_char_p, C.c_double, C.POINTER(vp)],
         "sgh_tables_desc": [vp, C.POINTER(TablesDesc)],
         "sgh_make_box": [C.c_double * 3, C.c_double * 3, C.c_double, C.POINTER(GridDims)],
@@ -139,6 +141,8 @@ def _declare(L):
                       C.c_int, C.c_int, C.c_int, _dp, _dp],
         "sg_bfgs": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, C.c_int, C.c_int,
                     C.c_int, _dp],
+        "sg_minimize": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _ip, C.c_int, _dp, C.c_int, _dp, C.c_double * 3,
+                        _ip, C.c_int, C.c_int, _dp, _dp, C.c_int],
         "sg_dock_batch32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
                             C.POINTER(MCParams), C.c_int, C.POINTER(LigandResult)],
         "sg_dock_batch32_noalloc": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
@@ -193,12 +197,16 @@ def _check_host(rc):
 
 # ---- host-side objects -------------------------------------------------------------
 class Model:
-    """A docking model (ligand torsion tree, pairs) read from PDBQT text."""
+    """A docking model (ligand torsion tree, pairs) read from PDBQT text; with
+    ``flex`` (flex PDBQT text) the receptor's flexible residues join it."""
 
-    def __init__(self, pdbqt: str):
+    def __init__(self, pdbqt: str, flex: str | None = None):
         L = load()
         h = C.c_void_p()
-        _check_host(L.sgh_model_from_pdbqt(pdbqt.encode(), C.byref(h)))
+        if flex is None:
+            _check_host(L.sgh_model_from_pdbqt(pdbqt.encode(), C.byref(h)))
+        else:
+            _check_host(L.sgh_model_from_pdbqt_flex(pdbqt.encode(), flex.encode(), C.byref(h)))
         self._h = h
         self.pdbqt = pdbqt
         self.desc = ModelDesc()
@@ -270,6 +278,16 @@ def make_ligand_pdbqt(heavy: int, rotors: int, seed: int, center=(0.0, 0.0, 0.0)
         raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
     buf = C.create_string_buffer(need)
     L.sgh_make_ligand_pdbqt(heavy, rotors, seed, vec3(center), buf, need)
+    return buf.value.decode()
+
+
+def make_flex_pdbqt(residues: int, seed: int, center=(0.0, 0.0, 0.0), shell=9.0) -> str:
+    L = load()
+    need = L.sgh_make_flex_pdbqt(residues, seed, vec3(center), shell, None, 0)
+    if need < 0:
+        raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
+    buf = C.create_string_buffer(need)
+    L.sgh_make_flex_pdbqt(residues, seed, vec3(center), shell, buf, need)
     return buf.value.decode()
 
 
@@ -527,6 +545,26 @@ class Engine:
 
     def set_chains_per_block(self, n: int):
         self._check(load().sg_set_chains_per_block(self._h, n))
+
+    def minimize(self, rid, models, pose_model, confs, boxes=None, cap=(1000, 1000, 1000), maxiters=10,
+                 accurate_line=0, early_term=0):
+        """Batched local optimisation (sg_minimize): each pose refined in FP64 in
+        its own box (``boxes`` [n][6] lo xyz, hi xyz; None: the receptor's)."""
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        pm = np.ascontiguousarray(pose_model, dtype=np.int32)
+        n = len(pm)
+        cs = max(m.conf_size for m in models)
+        H = max(m.heavy for m in models)
+        c = np.zeros((n, cs))
+        src = np.asarray(confs, dtype=np.float64).reshape(n, -1)
+        c[:, :src.shape[1]] = src
+        mi = np.ascontiguousarray(np.broadcast_to(np.asarray(maxiters, dtype=np.int32), (n,)))
+        bx = None if boxes is None else np.ascontiguousarray(boxes, dtype=np.float64).reshape(n, 6)
+        e = np.zeros(n)
+        xyz = np.zeros((n, H, 3))
+        self._check(load().sg_minimize(self._h, rid, descs, len(models), iptr(pm), n, dptr(c), cs, dptr(bx), vec3(cap),
+                                       iptr(mi), accurate_line, early_term, dptr(e), dptr(xyz), H))
+        return c, e, xyz
 
     def close(self):
         if getattr(self, "_h", None):

@@ -20,6 +20,7 @@
  *                                                                        src/lib/monte_carlo.cpp:95-130
  *   sg_refine                    run_refine (refine_structure)          src/gpu/gpu_kernels_impl.cuh:999-1098,
  *                                                                        src/main/main.cpp:165-190
+ *   sg_minimize                  GpuDocking::minimize_batch             src/gpu/gpu_docking.cpp:690-742
  *   sg_dock_batch32              GpuDocking::dock_batch (batched screen) src/gpu/gpu_docking.cpp:756-831
  *   sg_serve_*                   (no counterpart: continuous-batching request loop)
  *   sg_dock_batch32_noalloc      (no counterpart: the batched search without device allocation)
@@ -232,6 +233,20 @@ int sg_refine(sg_engine* e, int receptor_id, const sg_model_desc* models, int nm
               const int* pose_model, int nposes, double* confs, const double cap[3],
               int maxiters, int accurate_line, int early_term,
               double* out_e, double* out_coords);
+
+/* Batched local optimisation (--minimize / --local_only): replaces
+ * GpuDocking::minimize_batch (src/gpu/gpu_docking.h:96-107,
+ * gpu_docking.cpp:690-742): refine_structure of every pose in FP64 against
+ * the direct receptor sum, each pose in its own box (boxes [n][6]: lo xyz,
+ * hi xyz, inside the receptor's box; NULL: the receptor's box) with its own
+ * BFGS iteration count (maxiters [n]).  confs [n][conf_stride] in/out,
+ * out_e [n] (max double if a pose never got inside its box), out_coords
+ * [n][coord_stride][3] heavy atoms (may be NULL). */
+int sg_minimize(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+                const int* pose_model, int nposes, double* confs, int conf_stride,
+                const double* boxes, const double cap[3], const int* maxiters,
+                int accurate_line, int early_term, double* out_e, double* out_coords,
+                int coord_stride);
 
 /* ---- batched mixed-precision docking (virtual screening) ---------------
  * Replaces GpuDocking::dock_batch (src/gpu/gpu_docking.h:91-94,

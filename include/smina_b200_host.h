@@ -35,6 +35,10 @@ typedef struct sgh_tables sgh_tables;
 const char* sgh_last_error(void);
 
 int  sgh_model_from_pdbqt(const char* text, sgh_model** out);
+/* A ligand plus the receptor's flexible residues (smina --flex; flex PDBQT
+ * with BEGIN_RES/END_RES blocks, parse_pdbqt.cpp:412-437), combined as
+ * model::append does (model.cpp:302-347). */
+int  sgh_model_from_pdbqt_flex(const char* ligand_text, const char* flex_text, sgh_model** out);
 void sgh_model_free(sgh_model* m);
 /* descriptor pointing into the model (valid while the model lives) */
 int  sgh_model_desc(const sgh_model* m, sg_model_desc* out);
@@ -49,6 +53,11 @@ int  sgh_receptor_desc(sgh_receptor* r, sg_receptor_desc* out);
 int  sgh_receptor_pdbqt(const sgh_receptor* r, char* buf, int buflen);
 /* returns 0, -1 on error, or the buffer size needed */
 int  sgh_make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3], char* buf, int buflen);
+/* `residues` synthetic flexible side chains (2..4 chi torsions each) with
+ * their CA on a shell of radius `shell` (0: 9 A) around `center`.  Like
+ * sgh_make_ligand_pdbqt: returns the size needed when buflen is too small,
+ * 0 when written, -1 on error. */
+int  sgh_make_flex_pdbqt(int residues, uint64_t seed, const double center[3], double shell, char* buf, int buflen);
 
 /* builtin_name: "vina"/"default", "vinardo", "dkoes_scoring", "dkoes_fast",
  * "ad4_scoring"; custom_text (if non-empty) takes precedence */

@@ -14,7 +14,7 @@ namespace orc {
 void mc_chain(const Ctx& c, const Model& m, const sg_mc_params& P, const double* conf0, MT& gen, unsigned steps,
               Container& out, uint64_t* evals);
 void refine(Ctx& c, const Model& m, double* conf, const double cap[3], const MinParams& mp, double& e_out,
-            std::vector<V3>& coords_out);
+            std::vector<V3>& coords_out, const sg_grid_dims* box = nullptr);
 double bfgs_cache(const Ctx& c, const Model& m, std::vector<double>& x, const double v[3], double slope,
                   const MinParams& mp, uint64_t* evals);
 void state_for_eval(const Model& m, State& s);
@@ -224,6 +224,37 @@ int or_refine(or_ctx* o, const sg_model_desc* models, const int* pose_model, int
             if (out_coords)
                 for (size_t a = 0; a < hc.size(); a++)
                     for (int d = 0; d < 3; d++) out_coords[((size_t)k * hc.size() + a) * 3 + d] = hc[a][d];
+        }
+    } catch (std::exception& e) {
+        o->err = e.what();
+        return std::string(e.what()).find("overlaps") != std::string::npos ? SG_ERR_OVERLAP : 1;
+    }
+    return 0;
+}
+
+/* minimize_batch (gpu_docking.h:96-107): refine_structure of each pose in
+ * its own box (boxes: [n][6] lo xyz, hi xyz, or null for the receptor's)
+ * with its own BFGS iteration count. */
+int or_minimize(or_ctx* o, const sg_model_desc* models, const int* pose_model, int nposes, double* confs,
+                int conf_stride, const double* boxes, const double cap[3], const int* maxiters, int accurate_line,
+                int early_term, double* out_e, double* out_coords, int coord_stride) {
+    Model m;
+    try {
+        for (int k = 0; k < nposes; k++) {
+            m.load(models[pose_model[k]]);
+            std::vector<V3> hc;
+            MinParams mp{maxiters[k], accurate_line, early_term};
+            sg_grid_dims gd = o->c.geom.gd;
+            if (boxes)
+                for (int d = 0; d < 3; d++) {
+                    gd.begin[d] = boxes[6 * k + d];
+                    gd.end[d] = boxes[6 * k + 3 + d];
+                    gd.n[d] = 1;
+                }
+            refine(o->c, m, confs + (size_t)k * conf_stride, cap, mp, out_e[k], hc, boxes ? &gd : nullptr);
+            if (out_coords)
+                for (size_t a = 0; a < hc.size(); a++)
+                    for (int d = 0; d < 3; d++) out_coords[((size_t)k * coord_stride + a) * 3 + d] = hc[a][d];
         }
     } catch (std::exception& e) {
         o->err = e.what();

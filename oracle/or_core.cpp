@@ -478,10 +478,11 @@ double eval_deriv(const Ctx& c, const Model& m, const double* conf, const double
 }
 
 // non_cache::eval_deriv (non_cache.cpp:109-191) + the rest of model::eval_deriv
+// box: the job's own box (minimize_batch, gpu_docking.h:96-107); null: the receptor's
 double eval_direct_deriv(Ctx& c, CellLists& cl, const Model& m, const double* conf, const double v[3], double slope,
-                         State& s, double* g, bool* overlap) {
+                         State& s, double* g, bool* overlap, const sg_grid_dims* box) {
     model_set(m, conf, s);
-    const sg_grid_dims& gd = c.geom.gd;
+    const sg_grid_dims& gd = box ? *box : c.geom.gd;
     double e = 0;
     for (int i = 0; i < m.num_movable; i++) {
         double this_e = 0, oob = 0;
@@ -525,8 +526,9 @@ double eval_direct_deriv(Ctx& c, CellLists& cl, const Model& m, const double* co
 }
 
 // non_cache::within (non_cache.cpp:93-107)
-static bool within(const Ctx& c, const Model& m, const State& s, double margin = 0.0001) {
-    const sg_grid_dims& gd = c.geom.gd;
+static bool within(const Ctx& c, const Model& m, const State& s, const sg_grid_dims* box = nullptr,
+                   double margin = 0.0001) {
+    const sg_grid_dims& gd = box ? *box : c.geom.gd;
     for (int i = 0; i < m.num_movable; i++) {
         if (is_h(m.type[i])) continue;
         for (int j = 0; j < 3; j++)
@@ -857,13 +859,15 @@ void mc_chain(const Ctx& c, const Model& m, const sg_mc_params& P, const double*
 }
 
 struct DirectFn {
-    Ctx* c; CellLists* cl; const Model* m; State* s; double v[3]; double slope;
-    double operator()(const double* x, double* g) { return eval_direct_deriv(*c, *cl, *m, x, v, slope, *s, g, nullptr); }
+    Ctx* c; CellLists* cl; const Model* m; State* s; double v[3]; double slope; const sg_grid_dims* box;
+    double operator()(const double* x, double* g) {
+        return eval_direct_deriv(*c, *cl, *m, x, v, slope, *s, g, nullptr, box);
+    }
 };
 
 // refine_structure (main.cpp:165-190)
 void refine(Ctx& c, const Model& m, double* conf, const double cap[3], const MinParams& mp, double& e_out,
-            std::vector<V3>& coords_out) {
+            std::vector<V3>& coords_out, const sg_grid_dims* box) {
     CellLists cl;
     cl.full_cells = c.full_cells;
     cl.init(c.rec, c.tab.cutoff_sqr, c.geom.gd);
@@ -873,14 +877,14 @@ void refine(Ctx& c, const Model& m, double* conf, const double cap[3], const Min
     double slope = 10;
     double e = 0;
     for (int p = 0; p < 5; p++) {
-        DirectFn fn{&c, &cl, &m, &s, {cap[0], cap[1], cap[2]}, slope};
+        DirectFn fn{&c, &cl, &m, &s, {cap[0], cap[1], cap[2]}, slope, box};
         e = bfgs(fn, m, x, g, mp);
         model_set(m, x.data(), s);
-        if (within(c, m, s)) break;
+        if (within(c, m, s, box)) break;
         slope *= 10;
     }
     coords_out = heavy_coords(m, s);
-    if (!within(c, m, s)) e = MAXF;
+    if (!within(c, m, s, box)) e = MAXF;
     e_out = e;
     std::copy(x.begin(), x.end(), conf);
 }

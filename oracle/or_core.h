@@ -152,7 +152,7 @@ void model_set(const Model& m, const double* conf, State& s);                   
 double eval_deriv(const Ctx& c, const Model& m, const double* conf, const double v[3], double slope,
                   State& s, double* g, uint64_t* evals);                                    // model.cpp:969-985
 double eval_direct_deriv(Ctx& c, CellLists& cl, const Model& m, const double* conf, const double v[3],
-                         double slope, State& s, double* g, bool* overlap);                  // non_cache.cpp:109-191
+                         double slope, State& s, double* g, bool* overlap, const sg_grid_dims* box = nullptr);                  // non_cache.cpp:109-191
 void populate(Ctx& c, const int* types, int ntypes);                                        // cache.cpp:116-206
 
 // search

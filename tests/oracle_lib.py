@@ -46,6 +46,8 @@ def load():
                          sb._dp],
             "or_refine": [vp, C.POINTER(sb.ModelDesc), sb._ip, C.c_int, sb._dp, C.c_double * 3, C.c_int, C.c_int,
                           C.c_int, sb._dp, sb._dp],
+            "or_minimize": [vp, C.POINTER(sb.ModelDesc), sb._ip, C.c_int, sb._dp, C.c_int, sb._dp, C.c_double * 3,
+                            sb._ip, C.c_int, C.c_int, sb._dp, sb._dp, C.c_int],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a
@@ -142,6 +144,24 @@ class Oracle:
         self._check(load().or_refine(self.h, descs, sb.iptr(pm), n, sb.dptr(confs), sb.vec3(cap), maxiters, accurate,
                                      early, sb.dptr(e), sb.dptr(x)))
         return confs, e, x
+
+    def minimize(self, models, pose_model, confs, boxes=None, cap=(1000, 1000, 1000), maxiters=10, accurate=0,
+                 early=0):
+        descs = (sb.ModelDesc * len(models))(*[m.desc for m in models])
+        pm = np.ascontiguousarray(pose_model, dtype=np.int32)
+        n = len(pm)
+        cs = max(m.conf_size for m in models)
+        H = max(m.heavy for m in models)
+        c = np.zeros((n, cs))
+        src = np.asarray(confs, dtype=np.float64).reshape(n, -1)
+        c[:, :src.shape[1]] = src
+        mi = np.ascontiguousarray(np.broadcast_to(np.asarray(maxiters, dtype=np.int32), (n,)))
+        bx = None if boxes is None else np.ascontiguousarray(boxes, dtype=np.float64).reshape(n, 6)
+        e = np.zeros(n)
+        x = np.zeros((n, H, 3))
+        self._check(load().or_minimize(self.h, descs, sb.iptr(pm), n, sb.dptr(c), cs, sb.dptr(bx), sb.vec3(cap),
+                                       sb.iptr(mi), accurate, early, sb.dptr(e), sb.dptr(x), H))
+        return c, e, x
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -146,3 +146,36 @@ def test_refine_bit_exact(setup):
     assert_bitwise(e1, e0, "refined energies")
     assert_bitwise(c1, c0, "refined confs")
     assert_bitwise(x1, x0, "refined coords")
+
+
+def test_minimize_in_own_boxes_bit_exact(setup):
+    """Batched local optimisation (minimize_batch): each pose in its own box
+    with its own iteration count, FP64 against the checker bit for bit;
+    poses outside their box are pulled in or get max energy."""
+    eng, orc, gd = setup
+    models = [W.ligand(24, 5, 11), W.ligand(40, 10, 5)]
+    rng = np.random.default_rng(5)
+    confs, pm, boxes, its = [], [], [], []
+    lo, hi = np.array(gd.begin[:]), np.array(gd.end[:])
+    for k in range(8):
+        mi = k % 2
+        m = models[mi]
+        c = W.random_confs(m, gd, 1, 200 + k)[0]
+        centre = c[:3]
+        half = rng.uniform(4.0, 8.0)
+        b = np.concatenate([np.maximum(lo, centre - half), np.minimum(hi, centre + half)])
+        cm = np.zeros(max(x.conf_size for x in models))
+        cm[:m.conf_size] = c
+        confs.append(cm)
+        pm.append(mi)
+        boxes.append(b)
+        its.append(5 + 3 * k)
+    c1, e1, x1 = eng.minimize(0, models, pm, confs, boxes=boxes, maxiters=its)
+    c0, e0, x0 = orc.minimize(models, pm, confs, boxes=boxes, maxiters=its)
+    assert_bitwise(e1, e0, "energies")
+    assert_bitwise(c1, c0, "confs")
+    assert_bitwise(x1, x0, "coords")
+    # no boxes: the receptor's box, like refine_structure
+    c2, e2, _ = eng.minimize(0, models, pm, confs, maxiters=its)
+    c3, e3, _ = orc.minimize(models, pm, confs, maxiters=its)
+    assert_bitwise(e2, e3, "energies (receptor box)")
