@@ -212,6 +212,69 @@ def run_accuracy(args):
     }), flush=True)
 
 
+SERVE_RECEPTORS = ((2000, 22.0), (3000, 26.0), (5000, 30.0))  # (heavy atoms, box edge in A)
+
+
+def run_serve(args):
+    """Serving: ``args.serve`` single-ligand requests with seeded Poisson
+    arrivals at ``args.rate`` per second, spread round-robin over three
+    resident receptors (2,000 / 3,000 / 5,000 heavy atoms in 22 / 26 / 30 A
+    boxes), ligands with heavy atoms U[10, 60] and rotors U[0, 15],
+    exhaustiveness 8.  Latency is the engine's own submit-to-result time of
+    each request (queueing, search, merge and FP64 refinement)."""
+    rng = np.random.default_rng(args.seed)
+    n = args.serve
+    spec = [(int(rng.integers(10, 61)), int(rng.integers(0, 16)), 20_000 + k) for k in range(n)]
+    models = build_models(spec)
+    T = sb.Tables("vina")
+    eng = sb.Engine(0, sb.PREC_FP32 if args.precision == "fp32" else sb.PREC_FP32_H16)
+    eng.set_tables(T)
+    types = sorted({t for m in models for t in m.types() if 1 < t < 27})
+    for i, (na, edge) in enumerate(SERVE_RECEPTORS):
+        eng.set_receptor(i, sb.Receptor(na, 7 + i, CENTER), sb.make_box(CENTER, (edge,) * 3))
+        eng.build_grids(i, types)
+    p = make_params(models)
+    jobs = jobs_for(models, list(range(n)), args.exhaustiveness, args.seed, 0, args.step_scale)
+    for j in jobs:
+        j.model = 0
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    eng.serve_start(max_wait_ms=2.0)
+    lat, evals = {}, 0
+    k = 0
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        while len(lat) < n:
+            now = time.perf_counter() - t0
+            while k < n and arrivals[k] <= now:
+                eng.serve_submit(k % len(SERVE_RECEPTORS), models[k], jobs[k], p)
+                k += 1
+            wait = 1 if k < n else 20
+            for (t, st, cnt, ms, ev, cs, nh) in eng.serve_poll(256, wait_ms=wait):
+                if st != 0:
+                    raise RuntimeError(f"request {t} failed with status {st}")
+                eng.serve_fetch(t, cnt, cs, nh)
+                lat[t] = ms
+                evals += ev
+        wall = time.perf_counter() - t0
+    eng.serve_stop()
+    v = np.array(list(lat.values()))
+    clocks = clk.summary()
+    print(json.dumps({
+        "mode": "serve", "metric": "request latency (p50/p99) and ligands/s under Poisson arrivals",
+        "value": n / wall, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "latency_ms": {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+                       "max": float(v.max()), "mean": float(v.mean())},
+        "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{n} requests, ligands heavy U[10,60] rotors U[0,15], receptors "
+                               f"{[r[0] for r in SERVE_RECEPTORS]} heavy atoms in {[r[1] for r in SERVE_RECEPTORS]} A "
+                               f"boxes at 0.375 A, exhaustiveness {args.exhaustiveness}, smina step counts"
+                               + (f" x {args.step_scale}" if args.step_scale != 1.0 else ""),
+                   "precision": args.precision, "arrivals": f"Poisson, seed {args.seed}"},
+        "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }), flush=True)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -293,10 +356,16 @@ def main():
                     help="scale every ligand's Monte Carlo step count (profiling cases; 1 = smina's counts)")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="instead of timing: top-score agreement FP32 vs FP64 on this many ligands")
+    ap.add_argument("--serve", type=int, default=0,
+                    help="instead of the screen: this many requests through the serving loop (p50/p99 latency)")
+    ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
     if args.accuracy:
         run_accuracy(args)
+        return
+    if args.serve:
+        run_serve(args)
         return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -74,11 +74,13 @@ __device__ __forceinline__ uint4 philox10(uint4 c, uint32_t k0, uint32_t k1) {
 }
 // uniform double in [0, 1) with 53 random bits; every lane computes the same
 // value.  Out of line: one copy of the ten rounds serves every draw site.
-__device__ __noinline__ double ph_u01(Philox& r) {
-    const uint4 o = philox10(make_uint4(r.n++, 0u, r.c2, r.c3), r.k0, r.k1);
+// The state is passed by value so that callers keep it in registers.
+__device__ __noinline__ double ph_u01_at(uint32_t n, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+    const uint4 o = philox10(make_uint4(n, 0u, c2, c3), k0, k1);
     const uint64_t v = ((uint64_t)(o.x >> 5) << 26) | (o.y >> 6);
     return (double)v * (1.0 / 9007199254740992.0);
 }
+__device__ __forceinline__ double ph_u01(Philox& r) { return ph_u01_at(r.n++, r.c2, r.c3, r.k0, r.k1); }
 __device__ __forceinline__ double ph_range(Philox& r, double a, double b) { return a + (b - a) * ph_u01(r); }
 __device__ __forceinline__ int ph_int(Philox& r, int n) {  // [0, n)
     const int k = (int)(ph_u01(r) * n);
@@ -164,7 +166,7 @@ __device__ __forceinline__ float warp_sum(float v) {
 
 // model::set frame by frame, level after level (trees of more than 32
 // frames); out of line because typical ligands never need it
-__device__ __noinline__ void set_frames_by_level(const W32& w, const double* conf) {
+__device__ __noinline__ void set_frames_by_level(W32 w, const double* conf) {
     const SModel& m = smodel();
     const int* fkind = sp<const int>(m.fkind);
     const int* fconf = sp<const int>(m.fconf);
@@ -337,15 +339,19 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
     return f + penalty;
 }
 
-// charge map lookup (charge-dependent scoring only), out of line
-__device__ __noinline__ float grid_charge32(int t, float3 loc, float slope, float v, float3& deriv) {
-    return grid_aux32(sG32, t, true, loc, slope, v, deriv);
+// charge map lookup (charge-dependent scoring only), out of line; returns
+// (energy, derivative).  Results come back by value so that no caller
+// variable has its address taken.
+__device__ __noinline__ float4 grid_charge32(int t, float3 loc, float slope, float v) {
+    float3 d;
+    const float e = grid_aux32(sG32, t, true, loc, slope, v, d);
+    return make_float4(e, d.x, d.y, d.z);
 }
 
 // table lookup with charge-weighted components (precalculate_linear element
-// eval_deriv); out of line, charge-dependent scoring only
-__device__ __noinline__ void table32_nc(const DTables32& T, int p, bool swap, float qa, float qb, float r2, float& e,
-                                           float& dor) {
+// eval_deriv); out of line, charge-dependent scoring only; returns (e, dor)
+__device__ __noinline__ float2 table32_nc(int p, bool swap, float qa, float qb, float r2) {
+    const DTables32& T = sT32;
     if (swap) { const float t = qa; qa = qb; qb = t; }
     const float rf = T.factor * r2;
     const int i1 = (int)rf;
@@ -355,8 +361,7 @@ __device__ __noinline__ void table32_nc(const DTables32& T, int p, bool swap, fl
     const float aa = fabsf(qa), bb = fabsf(qb), ab = qa * qb;
     const float e1 = c0.x + aa * c1.x + bb * c2.x + ab * c3.x, e2 = c0.z + aa * c1.z + bb * c2.z + ab * c3.z;
     const float d1 = c0.y + aa * c1.y + bb * c2.y + ab * c3.y, d2 = c0.w + aa * c1.w + bb * c2.w + ab * c3.w;
-    e = e1 + rem * (e2 - e1);
-    dor = d1 + rem * (d2 - d1);
+    return make_float2(e1 + rem * (e2 - e1), d1 + rem * (d2 - d1));
 }
 
 // model::eval_deriv in FP32; returns the energy (same on every lane), writes g (FP64)
@@ -385,9 +390,9 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
             ghits++;
             const float q = LQ[i].w;
             if (q != 0.f && sG32.c32[t]) {
-                float3 cd;
-                e += q * grid_charge32(t, loc, slope, v.y, cd);
-                d = d + q * cd;
+                const float4 cd = grid_charge32(t, loc, slope, v.y);
+                e += q * cd.x;
+                d = d + q * make_float3(cd.y, cd.z, cd.w);
                 ghits++;
             }
         }
@@ -442,7 +447,9 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
                 pe = tv[u].x + rem[u] * (tv[u].z - tv[u].x);
                 dor = tv[u].y + rem[u] * (tv[u].w - tv[u].y);
             } else {
-                table32_nc(T, (sl[u] >> 16) & 0x1ff, (sl[u] & kSlotSwap) != 0, LQ[ia[u]].w, LQ[ib[u]].w, r2[u], pe, dor);
+                const float2 ed = table32_nc((sl[u] >> 16) & 0x1ff, (sl[u] & kSlotSwap) != 0, LQ[ia[u]].w, LQ[ib[u]].w, r2[u]);
+                pe = ed.x;
+                dor = ed.y;
             }
             f[u] = dor * r[u];
             const float vv = (sl[u] & kSlotIntra) ? v.x : v.z;

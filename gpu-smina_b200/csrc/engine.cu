@@ -728,6 +728,9 @@ struct Staged {
         if (init) sg::cuda_check(cudaMemcpyAsync(d.p, init, n * sizeof(T), cudaMemcpyHostToDevice, s), "stage in");
     }
     T* p() { return d.as<T>(); }
+    void zero(cudaStream_t s) {  // for outputs with padding the kernel leaves alone
+        sg::cuda_check(cudaMemsetAsync(d.p, 0, std::max<size_t>(1, n) * sizeof(T), s), "zero output");
+    }
     void fetch(T* host, cudaStream_t s) {
         if (host && n) sg::cuda_check(cudaMemcpyAsync(host, d.p, n * sizeof(T), cudaMemcpyDeviceToHost, s), "stage out");
     }
@@ -927,6 +930,7 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
         dc.make((size_t)nposes * cs, e->stream, confs);
         de.make(nposes, e->stream);
         dx.make((size_t)nposes * hs * 3, e->stream);
+        dx.zero(e->stream);  // atoms past a pose's heavy count stay 0
         dpm.make(nposes, e->stream, pose_model);
         cuda_check(launch_refine64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(), nposes,
                                    dc.p(), cs, cap, maxiters, nullptr, nullptr, accurate_line, early_term, de.p(), dx.p(), hs,
@@ -963,6 +967,7 @@ int sg_minimize(sg_engine* e, int rid, const sg_model_desc* models, int nmodels,
         dc.make((size_t)nposes * conf_stride, e->stream, confs);
         de.make(nposes, e->stream);
         dx.make((size_t)nposes * coord_stride * 3, e->stream);
+        dx.zero(e->stream);  // atoms past a pose's heavy count stay 0
         dpm.make(nposes, e->stream, pose_model);
         dmi.make(nposes, e->stream, maxiters);
         if (boxes) db.make((size_t)nposes * 6, e->stream, boxes);

@@ -387,4 +387,47 @@ int sg_set_chains_per_block(sg_engine* e, int n) {
     return SG_OK;
 }
 
+int sg_autotune32(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const sg_ligand_job* jobs, int njobs,
+                  const sg_mc_params* p, double step_fraction, double* evals_per_s, int* chosen) {
+    if (!e || !jobs || !p || njobs <= 0 || !(step_fraction > 0 && step_fraction <= 1)) return SG_ERR_ARG;
+    const int cands[4] = {8, 4, 2, 1};
+    const int keep = e->force_wpb;
+    // the sample: every job with its step count scaled (at least one step)
+    std::vector<sg_ligand_job> sample(jobs, jobs + njobs);
+    for (auto& j : sample) j.num_steps = std::max(1, (int)(j.num_steps * step_fraction));
+    const int S = p->num_saved_mins;
+    int max_conf = 1, max_heavy = 1;
+    for (int k = 0; k < nmodels && models; k++) {
+        max_conf = std::max(max_conf, models[k].conf_size);
+        max_heavy = std::max(max_heavy, models[k].num_movable);  // bounds the heavy atoms
+    }
+    std::vector<double> se((size_t)njobs * std::max(S, 1)), sc((size_t)njobs * std::max(S, 1) * max_conf),
+        sx((size_t)njobs * std::max(S, 1) * max_heavy * 3);
+    std::vector<sg_ligand_result> res(njobs);
+    for (int j = 0; j < njobs; j++)
+        res[j] = {0, &se[(size_t)j * S], &sc[(size_t)j * S * max_conf], &sx[(size_t)j * S * max_heavy * 3], 0};
+    double best = -1;
+    int best_c = 0;
+    for (int i = 0; i < 4; i++) {
+        if (evals_per_s) evals_per_s[i] = 0;
+        e->force_wpb = cands[i];
+        const int rc = sg_dock_batch32(e, rid, models, nmodels, sample.data(), njobs, p, 0, res.data());
+        if (rc != SG_OK && rc != SG_ERR_ARG) {  // a device error ends the search; the shape stays as it was
+            e->force_wpb = keep;
+            return rc;
+        }
+        if (rc != SG_OK || e->last_wpb != cands[i] || e->last_mc_ms <= 0) continue;  // shape not possible here
+        const double v = (double)e->last_evals / (e->last_mc_ms * 1e-3);
+        if (evals_per_s) evals_per_s[i] = v;
+        if (v > best) { best = v; best_c = cands[i]; }
+    }
+    e->force_wpb = best_c ? best_c : keep;
+    if (chosen) *chosen = best_c;
+    if (!best_c) {
+        e->err = "autotune: no launch shape ran (" + e->err + ")";
+        return SG_ERR_ARG;
+    }
+    return SG_OK;
+}
+
 }  // extern "C"

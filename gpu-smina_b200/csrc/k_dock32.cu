@@ -149,22 +149,24 @@ __device__ __forceinline__ double line_fast32(const W32& w, int x_at, double pg,
     return alpha;
 }
 
-__device__ __noinline__ double line_accurate32(const W32& w, int x_at, double pg, double f0, int p_at, int xn_at,
-                                                int gn_at, double& f1, const Mode32& em) {
+// Out of line; arguments by value and (alpha, f1) returned by value, so that
+// no variable of the caller has its address taken.
+__device__ __noinline__ double2 line_accurate32(W32 w, int x_at, double pg, double f0, int p_at, int xn_at, int gn_at,
+                                                 Mode32 em) {
     const SModel& m = smodel();
     const int n = m.dof;
     const double* x = sp<const double>(x_at);
     const double* p = sp<const double>(p_at);
     double* x_new = sp<double>(xn_at);
     double* g_new = sp<double>(gn_at);
-    double a, alpha, alpha2 = 0, alamin, b, disc, f2 = 0, rhs1, rhs2, tmplam = 0;
+    double a, alpha, alpha2 = 0, alamin, b, disc, f1 = 0, f2 = 0, rhs1, rhs2, tmplam = 0;
     const double ALF = 1.0e-4, FIRST = 1.0;
     const double slope = pg;
     auto give_up = [&]() {
         copyd(w, x_new, x, m.conf_size);
         for (int i = w.lane; i < n; i += 32) g_new[i] = 0;
         __syncwarp();
-        return 0.0;
+        return make_double2(0.0, f1);
     };
     if (slope >= 0) return give_up();
     double test = 0;
@@ -178,7 +180,7 @@ __device__ __noinline__ double line_accurate32(const W32& w, int x_at, double pg
         increment32(w, x_new, p, alpha);
         f1 = feval32(xn_at, gn_at, em);
         if (alpha < alamin) return give_up();
-        if (f1 <= f0 + ALF * alpha * slope) return alpha;
+        if (f1 <= f0 + ALF * alpha * slope) return make_double2(alpha, f1);
         if (alpha == FIRST) {
             tmplam = -slope / (2.0 * (f1 - f0 - slope));
         } else {
@@ -208,7 +210,7 @@ __device__ __noinline__ double line_accurate32(const W32& w, int x_at, double pg
 // a row sweep read consecutive words.  Every entry (i, j) is computed from
 // (min(i, j), max(i, j)) operands in one fixed order, so h stays exactly
 // symmetric.  x_at: smem32 offset of the conf, optimised in place.
-__device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int early, const Mode32& em) {
+__device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int early, Mode32 em) {
     const W32 w = here();
     const SModel& m = smodel();
     const Ws32& L = m.L;
@@ -238,9 +240,14 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
         pg = warp_sum_d(pg);
         __syncwarp();
         SG_T1(t_alg, 5);
-        double f1 = 0;
-        const double alpha = accurate ? line_accurate32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em)
-                                      : line_fast32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em);
+        double f1 = 0, alpha;
+        if (accurate) {
+            const double2 r = line_accurate32(w, x_at, pg, f0, p_at, xn_at, gn_at, em);
+            alpha = r.x;
+            f1 = r.y;
+        } else {
+            alpha = line_fast32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em);
+        }
         if (alpha == 0) break;
         SG_T0(t_alg2);
         // y = g_new - g, g = g_new, and the three dot products the update needs
@@ -592,8 +599,9 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
 // whole launch uses G.
 __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
                                                             const DMaps32* maps_tab, const Chain32* chains,
-                                                            const Item32* items, int nitems, MCParams32 P,
-                                                            unsigned* queue, int stage_stride, int ws_stride) {
+                                                            const Item32* items, int nitems,
+                                                            const __grid_constant__ MCParams32 P, unsigned* queue,
+                                                            int stage_stride, int ws_stride) {
     __shared__ int s_item;
     const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
     if (tid == 0) { sT32 = T; sG32 = G; sWs0 = stage_stride; sWsStride = ws_stride; }
@@ -606,8 +614,7 @@ __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DM
         if (maps_tab && tid == 0) sG32 = maps_tab[item.rec];  // read after stage_model's barrier
         stage_model(models + item.model, tid, nthr);
         if (warp < item.count) {
-            const Chain32 ch = chains[item.first + warp];
-            run_chain32(ch, P);
+            run_chain32(chains[item.first + warp], P);
         }
         SG_T0(t_bar);
         __syncthreads();  // the staged model is in use until every warp is done

@@ -150,6 +150,8 @@ def _declare(L):
         "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
         "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
         "sg_set_chains_per_block": [vp, C.c_int],
+        "sg_autotune32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
+                          C.POINTER(MCParams), C.c_double, _dp, _ip],
         "sg_serve_start": [vp, C.POINTER(ServeOpts)],
         "sg_serve_submit": [vp, C.c_int, C.POINTER(ModelDesc), C.POINTER(LigandJob), C.POINTER(MCParams),
                             C.POINTER(C.c_uint64)],
@@ -545,6 +547,18 @@ class Engine:
 
     def set_chains_per_block(self, n: int):
         self._check(load().sg_set_chains_per_block(self._h, n))
+
+    def autotune(self, rid, models, jobs, params: MCParams, step_fraction=0.01):
+        """Times the search at 8, 4, 2 and 1 chains per block on ``jobs`` with
+        scaled step counts and keeps the fastest shape (sg_autotune32).
+        Returns (chosen, {shape: eval_deriv calls per second})."""
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        J = (LigandJob * len(jobs))(*jobs)
+        rate = np.zeros(4)
+        chosen = C.c_int()
+        self._check(load().sg_autotune32(self._h, rid, descs, len(models), J, len(jobs), C.byref(params),
+                                         float(step_fraction), dptr(rate), C.byref(chosen)))
+        return chosen.value, {c: float(v) for c, v in zip((8, 4, 2, 1), rate)}
 
     def minimize(self, rid, models, pose_model, confs, boxes=None, cap=(1000, 1000, 1000), maxiters=10,
                  accurate_line=0, early_term=0):

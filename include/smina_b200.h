@@ -228,7 +228,7 @@ int sg_bfgs(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs, d
  * slope 10, 100, ... (<= 5 tries) until every movable heavy atom is inside
  * the box.  confs [n][max conf_size over models] in/out, out_e [n] (max
  * double if it never got inside), out_coords [n][max heavy atoms][3]
- * (may be NULL). */
+ * (may be NULL; rows past a pose's own heavy-atom count are 0). */
 int sg_refine(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
               const int* pose_model, int nposes, double* confs, const double cap[3],
               int maxiters, int accurate_line, int early_term,
@@ -241,7 +241,8 @@ int sg_refine(sg_engine* e, int receptor_id, const sg_model_desc* models, int nm
  * hi xyz, inside the receptor's box; NULL: the receptor's box) with its own
  * BFGS iteration count (maxiters [n]).  confs [n][conf_stride] in/out,
  * out_e [n] (max double if a pose never got inside its box), out_coords
- * [n][coord_stride][3] heavy atoms (may be NULL). */
+ * [n][coord_stride][3] heavy atoms (may be NULL; rows past a pose's own
+ * heavy-atom count are 0). */
 int sg_minimize(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
                 const int* pose_model, int nposes, double* confs, int conf_stride,
                 const double* boxes, const double cap[3], const int* maxiters,
@@ -314,6 +315,19 @@ int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookup
  * pick the shape with the most resident chains per SM (the default).  The
  * chains of one block share one copy of their ligand's model. */
 int sg_set_chains_per_block(sg_engine* e, int n);
+
+/* Launch-shape autotuner for the search kernel: runs the given jobs with
+ * their step counts scaled by step_fraction (0 < f <= 1, at least one step
+ * each; no refinement) once per shape of 8, 4, 2 and 1 chains per block,
+ * times each search launch with CUDA events and keeps the fastest shape
+ * (as sg_set_chains_per_block would).  evals_per_s[4] (may be null) gets
+ * each shape's eval_deriv calls per second, 0 for a shape that cannot run;
+ * *chosen the shape kept.  Results of later calls do not depend on the
+ * shape.  The reference picks its launch shape (threads per chain) from the
+ * occupancy calculator alone: Residency / mc_residency,
+ * src/gpu/gpu_kernels.h:70-88. */
+int sg_autotune32(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels, const sg_ligand_job* jobs,
+                  int njobs, const sg_mc_params* p, double step_fraction, double* evals_per_s, int* chosen);
 
 /* ---- serving: a request loop with continuous batching ------------------
  * No counterpart in the reference (its screens are offline batches).

@@ -64,7 +64,12 @@ def at_discontinuity(m, gd, xyz, cutoff_sqr):
     flags = np.zeros(len(xyz), bool)
     if d.num_pairs:
         pr = np.ctypeslib.as_array(d.pairs, shape=(2 * d.num_pairs,)).reshape(-1, 2)
-        r2 = ((xyz[:, pr[:, 1]] - xyz[:, pr[:, 0]]) ** 2).sum(-1)
+        full = xyz
+        if d.num_atoms > xyz.shape[1]:  # fixed atoms of flexible residues keep their input coords
+            lab = np.ctypeslib.as_array(d.atom_lab, shape=(3 * d.num_atoms,)).reshape(-1, 3)
+            fixed = np.broadcast_to(lab[xyz.shape[1]:], (len(xyz),) + lab[xyz.shape[1]:].shape)
+            full = np.concatenate([xyz, fixed], axis=1)
+        r2 = ((full[:, pr[:, 1]] - full[:, pr[:, 0]]) ** 2).sum(-1)
         flags |= (np.abs(r2 - cutoff_sqr) < CUT_A2).any(1)
     heavy = np.where(np.array(m.types())[:m.num_movable] > 1)[0]
     lo, hi = np.array(gd.begin[:]), np.array(gd.end[:])
@@ -147,6 +152,27 @@ def test_batch_deterministic_and_shape_independent(base):
         for k in ("e", "conf", "coords"):
             assert np.array_equal(x[k], y[k]) and np.array_equal(x[k], z[k]), k
         assert x["evals"] == y["evals"] == z["evals"] > 0
+
+
+def test_autotune_keeps_a_shape_and_results(base):
+    """The launch-shape autotuner times every shape that fits and keeps the
+    fastest; docking results do not depend on the shape it keeps."""
+    engine, _, _, _ = base
+    eng = engine(sb.PREC_FP32)
+    models = [W.ligand(24, 5, 11), W.ligand(12, 0, 3), W.ligand(40, 10, 5)]
+    p = _params(models[0])
+    jobs = _jobs(models)
+    a = eng.dock_batch(0, models, jobs, p)
+    try:
+        chosen, rates = eng.autotune(0, models, jobs, p, step_fraction=0.5)
+        assert chosen in (8, 4, 2, 1) and rates[chosen] == max(rates.values()) > 0
+        b = eng.dock_batch(0, models, jobs, p)
+        assert eng.batch_stats()["chains_per_block"] == chosen
+    finally:
+        eng.set_chains_per_block(0)
+    for x, y in zip(a, b):
+        for k in ("e", "conf", "coords"):
+            assert np.array_equal(x[k], y[k]), k
 
 
 def test_batch_alone_equals_in_mix(base):
