@@ -212,6 +212,60 @@ def run_accuracy(args):
     }), flush=True)
 
 
+def run_plain64(args):
+    """The same screen through the plain FP64 path (the reference's
+    --gpu_fp64 search): every chain of every ligand in one sg_dock launch
+    with host-seeded mt19937 streams, then merge and FP64 refinement per
+    ligand.  Prints ligands/s of device-and-host wall time, for the
+    comparison with the batched FP32 search."""
+    spec = screen(args.ligands, args.seed)
+    models = build_models(spec)
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    eng = sb.Engine(0, sb.PREC_FP64)
+    eng.set_tables(T)
+    eng.set_receptor(0, R, gd)
+    eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
+    p = make_params(models)
+    exh = args.exhaustiveness
+    cmax = max(m.conf_size for m in models)
+    confs, mts, moc, steps, its = [], [], [], [], []
+    for k, m in enumerate(models):
+        sp = m.search_params(9)
+        c, mt = m.seed_chains(args.seed + k, exh, gd)
+        cm = np.zeros((exh, cmax))
+        cm[:, :m.conf_size] = c
+        confs += list(cm)
+        mts += list(mt)
+        moc += [k] * exh
+        n = max(1, int(sp.num_steps * args.step_scale)) if args.step_scale != 1.0 else sp.num_steps
+        steps += [n] * exh
+        its += [sp.maxiters] * exh
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        b = eng.dock(0, models, moc, confs, mts, p, steps=steps, maxiters=its)
+        t_dock = time.perf_counter() - t0
+        for k, m in enumerate(models):
+            sp = m.search_params(9)
+            e, conf, _ = sb.merge_chains(b, m, first=exh * k, n=exh, max_size=p.num_saved_mins)
+            eng.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v), maxiters=sp.maxiters,
+                       accurate_line=p.accurate_line, early_term=p.early_term)
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+    evals = int(np.sum(b.evals))
+    print(json.dumps({
+        "mode": "plain64", "metric": "ligands docked/sec, plain FP64 path", "value": len(models) / wall,
+        "unit": UNIT, "n_gpus": 1, "dtype": "f64", "data": "synthetic", "wall_s": wall, "search_wall_s": t_dock,
+        "evals_per_s": evals / t_dock,
+        "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), receptor "
+                               f"3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness {exh}, smina step counts"
+                               + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
+                               + ", all chains in one launch, merge + FP64 refine per ligand"},
+        "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }), flush=True)
+
+
 SERVE_RECEPTORS = ((2000, 22.0), (3000, 26.0), (5000, 30.0))  # (heavy atoms, box edge in A)
 
 
@@ -222,6 +276,8 @@ def run_serve(args):
     boxes), ligands with heavy atoms U[10, 60] and rotors U[0, 15],
     exhaustiveness 8.  Latency is the engine's own submit-to-result time of
     each request (queueing, search, merge and FP64 refinement)."""
+    # more hardware queues for the server's many streams (read when the CUDA context is created)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     rng = np.random.default_rng(args.seed)
     n = args.serve
     spec = [(int(rng.integers(10, 61)), int(rng.integers(0, 16)), 20_000 + k) for k in range(n)]
@@ -238,7 +294,7 @@ def run_serve(args):
     for j in jobs:
         j.model = 0
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
-    eng.serve_start(max_wait_ms=2.0)
+    eng.serve_start()
     lat, evals = {}, 0
     k = 0
     with Clocks(0) as clk:
@@ -352,6 +408,8 @@ def main():
     ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--autotune", type=float, default=0.01,
+                    help="step fraction of the launch-shape autotuning sample (0: no autotuning)")
     ap.add_argument("--step-scale", type=float, default=1.0,
                     help="scale every ligand's Monte Carlo step count (profiling cases; 1 = smina's counts)")
     ap.add_argument("--accuracy", type=int, default=0,
@@ -359,6 +417,8 @@ def main():
     ap.add_argument("--serve", type=int, default=0,
                     help="instead of the screen: this many requests through the serving loop (p50/p99 latency)")
     ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
+    ap.add_argument("--plain64", action="store_true",
+                    help="instead of the batched search: the same screen through the plain FP64 path")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
     if args.accuracy:
@@ -366,6 +426,9 @@ def main():
         return
     if args.serve:
         run_serve(args)
+        return
+    if args.plain64:
+        run_plain64(args)
         return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -384,10 +447,17 @@ def main():
     eng.set_tables(T)
     eng.set_receptor(0, R, gd)
     eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
-    if args.chains_per_block:
-        eng.set_chains_per_block(args.chains_per_block)
     p = make_params(models)
     B = args.batch or args.ligands
+    tuned = None
+    if args.chains_per_block:
+        eng.set_chains_per_block(args.chains_per_block)
+    elif args.autotune > 0:  # launch shape timed on a short sample of the screen, before any timed step
+        idx = list(range(B))  # one step's ligands, so the sample fills the device as a step does
+        sample = jobs_for(models, idx, args.exhaustiveness, args.seed, 10_000_000)
+        chosen, rates = eng.autotune(0, models[:B], sample, p, step_fraction=args.autotune)
+        tuned = {"chosen": chosen, "evals_per_s": {str(c): round(v) for c, v in rates.items()},
+                 "sample": f"{len(idx)} ligands at {args.autotune} of their steps"}
     nb = max(1, args.ligands // B)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
     key_base = 1_000_000 * rank
@@ -457,7 +527,8 @@ def main():
                                    + f", {B} ligands per step",
                        "precision": args.precision, "ligands_per_step": B, "global_batch": B * world,
                        "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)",
-                       "chains_per_block": recs[-1][2]["chains_per_block"], "blocks": recs[-1][2]["blocks"]},
+                       "chains_per_block": recs[-1][2]["chains_per_block"], "blocks": recs[-1][2]["blocks"],
+                       "autotune": tuned},
             "e2e": {"value": e2e, "unit": UNIT,
                     "h2d_bytes_per_step": int(sum(r[2]["h2d_bytes"] for r in recs) / len(recs)),
                     "d2h_bytes_per_step": int(sum(r[2]["d2h_bytes"] for r in recs) / len(recs))},

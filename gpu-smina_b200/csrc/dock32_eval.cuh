@@ -305,7 +305,7 @@ __device__ __forceinline__ float grid_aux32(const DMaps32& G, int t, bool charge
         else { region[i] = 0; a[i] = min((int)s[i], G.cdim[i] - 1); s[i] -= (float)a[i]; }
     }
     const float penalty = slope * (miss[0] * G.factor_inv[0] + miss[1] * G.factor_inv[1] + miss[2] * G.factor_inv[2]);
-    const size_t cell = (size_t)a[0] + (size_t)G.cdim[0] * ((size_t)a[1] + (size_t)G.cdim[1] * a[2]);
+    const int cell = a[0] + G.cdim[0] * (a[1] + G.cdim[1] * a[2]);
     float4 lo, hi;
     if (!charge_map && G.half) {
         const uint4 u = __ldg(G.m16[t] + cell);
@@ -410,6 +410,9 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
     const DTables32 T = sT32;
     const int lane = w.lane;
     unsigned hits = 0;
+    uint32_t nsl[SG_PAIR_CHUNKS];  // next round's slots, loaded a round ahead
+#pragma unroll
+    for (int u = 0; u < SG_PAIR_CHUNKS; u++) nsl[u] = u < nch ? PS[u * 32 + lane] : kSlotEmpty;
     for (int c = 0; c < nch; c += SG_PAIR_CHUNKS) {
         const int live = min(SG_PAIR_CHUNKS, nch - c);  // chunks this round (warp-uniform)
         uint32_t sl[SG_PAIR_CHUNKS];
@@ -419,7 +422,8 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
         bool ok[SG_PAIR_CHUNKS];
 #pragma unroll
         for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
-            sl[u] = u < live ? PS[(c + u) * 32 + lane] : kSlotEmpty;
+            sl[u] = nsl[u];
+            nsl[u] = c + SG_PAIR_CHUNKS + u < nch ? PS[(c + SG_PAIR_CHUNKS + u) * 32 + lane] : kSlotEmpty;
             ia[u] = sl[u] & 0xff;
             ib[u] = (sl[u] >> 8) & 0xff;
             r[u] = f3(X[ib[u]]) - f3(X[ia[u]]);
@@ -434,7 +438,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
                 const float rf = T.factor * r2[u];
                 const int i1 = ok[u] ? (int)rf : 0;
                 rem[u] = rf - (float)i1;
-                tv[u] = ok[u] ? __ldg(T.tab + ((size_t)((sl[u] >> 16) & 0x1ff) * T.n + i1)) : make_float4(0, 0, 0, 0);
+                tv[u] = ok[u] ? __ldg(T.tab + (int)(((sl[u] >> 16) & 0x1ffu) * (unsigned)T.n + (unsigned)i1)) : make_float4(0, 0, 0, 0);
             }
         }
         float3 f[SG_PAIR_CHUNKS];

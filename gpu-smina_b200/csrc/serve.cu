@@ -123,7 +123,8 @@ struct SvBatch {
     std::vector<Chain32> hc;
     size_t e_at = 0, conf_at = 0, xyz_at = 0, order_at = 0, count_at = 0, evals_at = 0;
     int S = 20;
-    cudaEvent_t kdone = nullptr;
+    cudaEvent_t kdone = nullptr;  // recorded once every ligand's chains are done (see worker)
+    int flagged = 0;               // ligands whose completion flag has been seen
     int published = 0;
 };
 
@@ -149,11 +150,12 @@ struct Server {
     volatile unsigned* flags = nullptr;
     unsigned* dflags = nullptr;
     std::vector<int> free_flags;
-    int* d_err = nullptr;
+    int* d_err = nullptr;            // device error word (refinement overlap)
+    volatile int* h_err = nullptr;   // pinned copy, refreshed after every refinement launch
     Clock::time_point last_err_check;
     std::vector<std::unique_ptr<struct RefineGroup>> refining;
     static constexpr int kFlags = 1 << 16;
-    static constexpr int kMaxStreams = 96;
+    static constexpr int kMaxStreams = 112;  // concurrent kernels: 128 per device, some kept for refines and copies
 };
 
 static size_t req_bytes(const sg_model_desc& m, const sg_ligand_job& j, int S) {
@@ -344,8 +346,10 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
                            reinterpret_cast<unsigned*>(b->dmem + queue_at), (int)q.size(), wpb, stage_stride, ws_stride,
                            st),
                "serve: search launch");
+    // The kernel-end event is recorded only when every ligand of the batch has
+    // flagged completion: a command queued behind a kernel that runs for
+    // seconds would hold up the hardware queue it shares with other streams.
     cuda_check(cudaEventCreateWithFlags(&b->kdone, cudaEventDisableTiming), "serve");
-    cuda_check(cudaEventRecord(b->kdone, st), "serve");
     s.inflight_bytes += b->bytes;
     s.inflight_ligs += (int)b->ligs.size();
     s.inflight.push_back(std::move(b));
@@ -475,6 +479,7 @@ static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& 
     cuda_check(cudaMemcpyAsync(g->conf.data(), dc, cb, cudaMemcpyDeviceToHost, rs), "serve");
     cuda_check(cudaMemcpyAsync(g->e.data(), de, eb, cudaMemcpyDeviceToHost, rs), "serve");
     cuda_check(cudaMemcpyAsync(g->xyz.data(), dx, xb, cudaMemcpyDeviceToHost, rs), "serve");
+    cuda_check(cudaMemcpyAsync((void*)s.h_err, s.d_err, sizeof(int), cudaMemcpyDeviceToHost, rs), "serve");
     cuda_check(cudaFreeAsync(g->dbuf, rs), "serve");
     g->dbuf = nullptr;
     cuda_check(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming), "serve");
@@ -544,16 +549,26 @@ static void worker(Server* sp) {
     for (;;) {
         bool busy = false;
         try {
-            // 1. launch.  While fewer ligands are in flight than the device holds
-            // at once (max_inflight_ligands), whatever waits goes out at once;
-            // beyond that, requests gather for up to max_wait_ms into bigger
-            // launches.  Same search parameters per launch; device memory
-            // held for requests in flight stays under the budget.
-            if (!s.queue.empty() && (!s.free_streams.empty() || (int)s.streams.size() < Server::kMaxStreams)) {
+            // 1. launch.  A launch holds one of at most kMaxStreams concurrent
+            // kernels until its last ligand is done, so the launches still
+            // possible must carry the ligands the device can still take
+            // (max_inflight_ligands): a launch goes out once that share has
+            // queued, or when the oldest request has waited max_wait_ms
+            // scaled by how scarce launches have become.  Beyond
+            // max_inflight_ligands requests gather up to max_batch_ligands.
+            // Same search parameters per launch; device memory held for
+            // requests in flight stays under the budget.
+            const int in_use = (int)(s.streams.size() - s.free_streams.size());
+            if (!s.queue.empty() && in_use < Server::kMaxStreams) {
                 const double waited =
                     std::chrono::duration<double, std::milli>(Clock::now() - s.queue.front().t_submit).count();
-                const bool room = s.inflight_ligs < s.o.max_inflight_ligands;
-                if (room || (int)s.queue.size() >= s.o.max_batch_ligands || waited >= s.o.max_wait_ms || s.stopping) {
+                const int slots = Server::kMaxStreams - in_use;
+                const int open = std::max(0, s.o.max_inflight_ligands - s.inflight_ligs);
+                const int share = std::max(1, (open + slots - 1) / slots);
+                const double gather_ms = s.o.max_wait_ms * (double)Server::kMaxStreams / slots;
+                const bool go = open > 0 ? ((int)s.queue.size() >= share || waited >= gather_ms)
+                                         : ((int)s.queue.size() >= s.o.max_batch_ligands || waited >= gather_ms);
+                if (go || s.stopping) {
                     std::vector<ServeReq> take;
                     size_t bytes = 0;
                     const int cap = std::min(s.o.max_batch_ligands, (int)s.free_flags.size());
@@ -580,6 +595,8 @@ static void worker(Server* sp) {
                     if (L.state == 0 && s.flags[L.flag]) {
                         fetch_merge(s, *b, L);
                         fin.emplace_back(b.get(), &L);
+                        if (++b->flagged == (int)b->ligs.size())  // its blocks are retiring now
+                            cuda_check(cudaEventRecord(b->kdone, b->stream), "serve: kernel end");
                     }
             if (!fin.empty()) {
                 launch_refines(s, fin);
@@ -604,7 +621,8 @@ static void worker(Server* sp) {
             // 3. retire batches whose kernel ended and whose ligands are all published
             for (size_t i = 0; i < s.inflight.size();) {
                 SvBatch& b = *s.inflight[i];
-                if (b.published == (int)b.ligs.size() && cudaEventQuery(b.kdone) == cudaSuccess) {
+                if (b.flagged == (int)b.ligs.size() && b.published == (int)b.ligs.size() &&
+                    cudaEventQuery(b.kdone) == cudaSuccess) {
                     cuda_check(cudaFreeAsync(b.dmem, b.stream), "serve: free batch");
                     cudaEventDestroy(b.kdone);
                     s.free_streams.push_back(b.stream);
@@ -615,11 +633,11 @@ static void worker(Server* sp) {
                     i++;
                 }
             }
-            // device errors (overlap in a refinement) end the server
-            int herr = 0;
+            // device errors (overlap in a refinement) end the server; the pinned
+            // copy is read without a CUDA call, so nothing waits on running kernels
             if (!busy && Clock::now() - s.last_err_check > std::chrono::milliseconds(10)) {
                 s.last_err_check = Clock::now();
-                cuda_check(cudaMemcpy(&herr, s.d_err, sizeof(int), cudaMemcpyDeviceToHost), "serve: error word");
+                const int herr = *s.h_err;
                 if (herr != kDevOk)
                     throw EngineError(herr == kDevOverlap ? SG_ERR_OVERLAP : SG_ERR_ARG,
                                       "serve: device reported error " + std::to_string(herr));
@@ -675,8 +693,8 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
         s->e = e;
         if (o) s->o = *o;
         if (s->o.max_batch_ligands <= 0) s->o.max_batch_ligands = 64;
-        if (s->o.max_wait_ms <= 0) s->o.max_wait_ms = 2.0;
-        if (s->o.max_inflight_ligands <= 0) s->o.max_inflight_ligands = 320;
+        if (s->o.max_wait_ms <= 0) s->o.max_wait_ms = 20.0;
+        if (s->o.max_inflight_ligands <= 0) s->o.max_inflight_ligands = 2 * e->num_sms;  // resident 8-chain blocks
         if (s->o.hbm_budget_bytes == 0) {
             size_t fr = 0, tot = 0;
             cuda_check(cudaMemGetInfo(&fr, &tot), "serve: memory info");
@@ -692,6 +710,10 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
         for (int i = Server::kFlags - 1; i >= 0; i--) s->free_flags.push_back(i);
         cuda_check(cudaMalloc((void**)&s->d_err, sizeof(int)), "serve: error word");
         cuda_check(cudaMemset(s->d_err, 0, sizeof(int)), "serve: error word");
+        int* he = nullptr;
+        cuda_check(cudaHostAlloc((void**)&he, sizeof(int), cudaHostAllocDefault), "serve: error word");
+        *he = kDevOk;
+        s->h_err = he;
         Server* raw = s.get();
         {
             std::lock_guard<std::mutex> lk(g_srv_mu);
@@ -813,6 +835,7 @@ int sg_serve_stop(sg_engine* e) {
         cudaStreamDestroy(s->copy_stream);
         cudaFreeHost((void*)s->flags);
         cudaFree(s->d_err);
+        cudaFreeHost((void*)s->h_err);
         const int err = s->error;
         const std::string why = s->error_text;
         {

@@ -340,15 +340,21 @@ int sg_autotune32(sg_engine* e, int receptor_id, const sg_model_desc* models, in
  * hbm_budget_bytes.  Each ligand is merged and refined (FP64) as soon as its
  * own chains finish.  A result equals sg_dock_batch32's (refine = 1) for the
  * same (seed, ligand_key), alone or in any mix.  While a server runs, the
- * engine's other entry points must not be called except sg_serve_*. */
+ * engine's other entry points must not be called except sg_serve_*.
+ * Launches go to up to 112 streams; with the driver's default of 8 hardware
+ * queues, streams share queues, so set CUDA_DEVICE_MAX_CONNECTIONS=32 in the
+ * environment before the process creates its CUDA context. */
 typedef struct sg_serve_opts {
     uint64_t hbm_budget_bytes;  /* 0: a quarter of the free device memory   */
     int max_batch_ligands;      /* ligands per launch (0: 64)                */
-    double max_wait_ms;         /* once the device is full, how long requests
-                                   gather into a bigger launch (0: 2 ms)     */
+    double max_wait_ms;         /* how long the oldest request may wait for
+                                   others to share its launch, scaled up as
+                                   the concurrent launches (at most 112) run
+                                   out (0: 20 ms)                            */
     int max_inflight_ligands;   /* ligands on the device before requests
-                                   start to gather (0: 320, a little over what
-                                   a B200 holds at once)                     */
+                                   start to gather (0: two per SM, what the
+                                   device holds at once with 8 chains per
+                                   ligand)                                   */
 } sg_serve_opts;
 
 typedef struct sg_serve_done {
