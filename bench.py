@@ -408,8 +408,9 @@ def main():
     ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
-    ap.add_argument("--autotune", type=float, default=0.01,
-                    help="step fraction of the launch-shape autotuning sample (0: no autotuning)")
+    ap.add_argument("--autotune", type=float, default=0.0,
+                    help="autotune the launch shape first on the step's ligands at this fraction of their steps "
+                         "(0: the occupancy rule; short samples overweight the wait for each block's slowest chain)")
     ap.add_argument("--step-scale", type=float, default=1.0,
                     help="scale every ligand's Monte Carlo step count (profiling cases; 1 = smina's counts)")
     ap.add_argument("--accuracy", type=int, default=0,

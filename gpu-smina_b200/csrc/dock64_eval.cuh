@@ -293,6 +293,135 @@ __device__ double energy64(W64& w) {
     return e;
 }
 
+// ---- energy-only scoring (final rescoring of docked poses) ---------------------------------
+// precalculate_linear::eval (precalculate.h:75-83,103-108,191-203): the fast
+// table's components at sz(factor r2), weighted by a's and b's charges
+// (result_components::eval, result_components.h:75-81); for t_a > t_b the
+// (t_b, t_a) entry with its A and B components swapped (swapOrder).
+__device__ __forceinline__ double table_fast64(const DTables& T, int ta, double qa, int tb, double qb, double r2) {
+    const bool sw = ta > tb;
+    const int p = sw ? tri_index(tb, ta) : tri_index(ta, tb);
+    const double* c = T.fast + ((size_t)p * T.n + (size_t)(T.factor * r2)) * T.nc;
+    double ca = 0, cb = 0, cab = 0;
+    if (T.nc > 1) { ca = sw ? c[2] : c[1]; cb = sw ? c[1] : c[2]; cab = c[3]; }
+    return c[0] + fabs(qa) * ca + fabs(qb) * cb + qa * qb * cab;
+}
+
+// non_cache::eval (non_cache.cpp:34-91): per movable heavy atom, the direct
+// sum over its clamped position's cell list, curled, plus the out-of-box
+// penalty; into eatom (summed in atom order by energy64)
+__device__ void direct_energy64(W64& w, double v, double slope) {
+    const DModel& m = *w.m;
+    const DReceptor& R = *w.R;
+    const DGeom& G = R.g;
+    double* S = w.s;
+    for (int i = w.lane; i < m.nmov; i += 32) {
+        const int t = m.type[i];
+        if (t >= kNumTypes || is_h(t)) { S[w.L.eatom + i] = 0; continue; }
+        const double a[3] = {S[w.L.coords + 3 * i], S[w.L.coords + 3 * i + 1], S[w.L.coords + 3 * i + 2]};
+        double adj[3] = {a[0], a[1], a[2]}, oob = 0;
+        for (int j = 0; j < 3; j++) {
+            if (G.gd_n[j] > 0) {
+                if (a[j] < G.gd_begin[j]) { adj[j] = G.gd_begin[j]; oob += fabs(a[j] - G.gd_begin[j]); }
+                else if (a[j] > G.gd_end[j]) { adj[j] = G.gd_end[j]; oob += fabs(a[j] - G.gd_end[j]); }
+            }
+        }
+        oob *= slope;
+        int ci[3];
+        for (int j = 0; j < 3; j++) ci[j] = (int)floor(adj[j] / 3.0) - G.cell_off[j];
+        double this_e = 0;
+        if (ci[0] >= 0 && ci[1] >= 0 && ci[2] >= 0 && ci[0] < G.cell_dim[0] && ci[1] < G.cell_dim[1] &&
+            ci[2] < G.cell_dim[2]) {
+            const int cell = ci[0] + G.cell_dim[0] * (ci[1] + G.cell_dim[1] * ci[2]);
+            for (int k = R.full_start[cell]; k < R.full_start[cell + 1]; k++) {
+                const int j = R.full_atoms[k];
+                const V3<double> rba{adj[0] - R.xyz[3 * j], adj[1] - R.xyz[3 * j + 1], adj[2] - R.xyz[3 * j + 2]};
+                const double r2 = norm2(rba);
+                if (r2 < w.T->cutoff_sqr) this_e += table_fast64(*w.T, t, m.charge[i], R.type[j], R.charge[j], r2);
+            }
+        } else {
+            atomicExch(w.err, kDevBadModel);
+        }
+        curl_e(this_e, v);
+        S[w.L.eatom + i] = this_e + oob;
+    }
+}
+
+// model::eval_interacting_pairs (model.cpp:885-902) for every pair: curled
+// energy into pe, in-cutoff flag into pin
+__device__ void pairs_energy64(W64& w, const double v[3]) {
+    const DModel& m = *w.m;
+    double* S = w.s;
+    for (int k = w.lane; k < m.npairs; k += 32) {
+        const int a = m.pairs[2 * k], b = m.pairs[2 * k + 1];
+        const double r2 = norm2(ld3(S + w.L.coords + 3 * a) - ld3(S + w.L.coords + 3 * b));
+        uint8_t in = 0;
+        if (r2 < w.T->cutoff_sqr) {
+            double pe = table_fast64(*w.T, m.type[a], m.charge[a], m.type[b], m.charge[b], r2);
+            curl_e(pe, m.pair_group[k] == 0 ? v[2] : v[0]);
+            S[w.L.pe + k] = pe;
+            in = 1;
+        }
+        w.pin[k] = in;
+    }
+    __syncwarp();
+}
+
+// model::eval_intramolecular (model.cpp:1027-1079) after pairs_energy64 on the
+// same coords: each ligand's pairs, then every flexible movable atom against
+// every receptor atom (curled per pair), then flex-flex other pairs.  One
+// running sum in the reference's order; the flex-rigid energies of 32
+// receptor atoms are computed at once and added by lane 0 in atom order.
+__device__ double intramolecular64(W64& w, const double v[3]) {
+    const DModel& m = *w.m;
+    const DReceptor& R = *w.R;
+    const double* S = w.s;
+    auto in_ligand = [&](int i) {
+        for (int l = 0; l < m.nlig; l++)
+            if (i >= m.lig_begin[l] && i < m.lig_end[l]) return true;
+        return false;
+    };
+    double e = 0;
+    if (w.lane == 0) {
+        int start = m.nother;
+        for (int l = 0; l < m.nlig; l++) {
+            double el = 0;
+            for (int k = start; k < m.lig_pair_end[l]; k++)
+                if (w.pin[k]) el += S[w.L.pe + k];
+            e += el;
+            start = m.lig_pair_end[l];
+        }
+    }
+    for (int i = 0; i < m.nmov; i++) {  // warp-uniform
+        if (in_ligand(i) || m.type[i] >= kNumTypes) continue;
+        const V3<double> a = ld3(S + w.L.coords + 3 * i);
+        for (int j0 = 0; j0 < R.natoms; j0 += 32) {
+            const int j = j0 + w.lane;
+            double this_e = 0;
+            bool add = false;
+            if (j < R.natoms && R.type[j] < kNumTypes) {
+                const double r2 = norm2(a - V3<double>{R.xyz[3 * j], R.xyz[3 * j + 1], R.xyz[3 * j + 2]});
+                if (r2 < w.T->cutoff_sqr) {
+                    this_e = table_fast64(*w.T, m.type[i], m.charge[i], R.type[j], R.charge[j], r2);
+                    curl_e(this_e, v[1]);
+                    add = true;
+                }
+            }
+            for (int l = 0; l < 32; l++) {
+                const double x = __shfl_sync(kFull, this_e, l);
+                const int ok = __shfl_sync(kFull, (int)add, l);
+                if (w.lane == 0 && ok) e += x;
+            }
+        }
+    }
+    if (w.lane == 0)
+        for (int k = 0; k < m.nother; k++) {
+            const int a = m.pairs[2 * k], b = m.pairs[2 * k + 1];
+            if (w.pin[k] && !in_ligand(a) && !in_ligand(b)) e += S[w.L.pe + k];
+        }
+    return __shfl_sync(kFull, e, 0);
+}
+
 // tree derivative: per-frame sums, children bottom-up, then the change vector
 __device__ void derivative64(W64& w, double* g) {
     const DModel& m = *w.m;

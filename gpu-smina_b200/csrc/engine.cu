@@ -943,6 +943,41 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
     });
 }
 
+int sg_score(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const int* pose_model, int nposes,
+             const double* confs, int conf_stride, const double v[3], double slope, double* out_e, double* out_intra,
+             double* out_coords, int coord_stride) {
+    return guarded(e, [&] {
+        require(pose_model && confs && v && out_e && out_intra && nposes > 0 && nposes <= (1 << 24),
+                "score: bad arguments");
+        require(e->has_tables, "no tables set");
+        RecState& r = receptor_for(e, rid);
+        ensure_cells(e, r);
+        PackedModels pm;
+        pack_models(e, models, nmodels, pm);
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
+        require(conf_stride >= pm.max_conf && (!out_coords || coord_stride >= pm.max_heavy), "score: strides too small");
+        for (int k = 0; k < nposes; k++) require(pose_model[k] >= 0 && pose_model[k] < nmodels, "score: bad pose model");
+        Staged<double> dc, de, di, dx;
+        Staged<int> dpm;
+        dc.make((size_t)nposes * conf_stride, e->stream, confs);
+        de.make(nposes, e->stream);
+        di.make(nposes, e->stream);
+        if (out_coords) {
+            dx.make((size_t)nposes * coord_stride * 3, e->stream);
+            dx.zero(e->stream);  // atoms past a pose's heavy count stay 0
+        }
+        dpm.make(nposes, e->stream, pose_model);
+        cuda_check(launch_score64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), dpm.p(),
+                                  nposes, dc.p(), conf_stride, v, slope, de.p(), di.p(), out_coords ? dx.p() : nullptr,
+                                  coord_stride, e->d_err.as<int>(), e->stream),
+                   "score launch");
+        de.fetch(out_e, e->stream);
+        di.fetch(out_intra, e->stream);
+        if (out_coords) dx.fetch(out_coords, e->stream);
+        e->check_device_errors();
+    });
+}
+
 int sg_minimize(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const int* pose_model, int nposes,
                 double* confs, int conf_stride, const double* boxes, const double cap[3], const int* maxiters,
                 int accurate_line, int early_term, double* out_e, double* out_coords, int coord_stride) {

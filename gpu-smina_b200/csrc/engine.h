@@ -126,11 +126,18 @@ cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor
                           int, int, int, double*, int*, cudaStream_t);
 cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
                         const MCParams64&, int*, cudaStream_t);
+cudaError_t launch_score64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const int* pose_model,
+                           int n, const double* confs, int conf_stride, const double v[3], double slope, double* e,
+                           double* intra, double* coords, int coord_stride, int* err, cudaStream_t s);
 cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DReceptor*, const int*, int, double*, int,
                             const double[3], int, const int* pose_maxiters, const double* pose_box, int, int, double*,
                             double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
 int mc32_occupancy(int wpb, size_t smem);
+cudaError_t serve_prepare32(size_t smem_fixed);
+cudaError_t launch_mc32_fixed(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
+                              const Item32*, int nitems, const MCParams32&, unsigned* queue, int blocks, int wpb,
+                              size_t stage_stride, size_t ws_stride, size_t smem_fixed, cudaStream_t s);
 cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
                         const Item32*, int nitems, const MCParams32&, unsigned*, int blocks, int wpb,
                         size_t stage_stride, size_t ws_stride, cudaStream_t);

@@ -679,6 +679,22 @@ cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G,
     return cudaGetLastError();
 }
 
+// Serving launches: many launches of k_mc32 run at once, so they all take the
+// same dynamic shared memory (set once here), which keeps every SM's
+// shared-memory configuration the same for all of them and sets no function
+// attribute while earlier launches run.
+cudaError_t serve_prepare32(size_t smem_fixed) { return prep32((const void*)k_mc32, smem_fixed); }
+
+cudaError_t launch_mc32_fixed(const DModel* dms, const DTables32& T, const DMaps32& G, const DMaps32* maps_tab,
+                              const Chain32* chains, const Item32* items, int nitems, const MCParams32& P,
+                              unsigned* queue, int blocks, int wpb, size_t stage_stride, size_t ws_stride,
+                              size_t smem_fixed, cudaStream_t s) {
+    if (stage_stride + (size_t)wpb * ws_stride > smem_fixed) return cudaErrorInvalidValue;
+    k_mc32<<<blocks, 32 * wpb, smem_fixed, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
+                                                (int)stage_stride, (int)ws_stride);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_eval32(const DModel* dm, size_t stage, size_t ws, const DTables32& T, const DMaps32& G, int n,
                           const double* confs, const double v[3], double slope, double* e, double* g, double* coords,
                           cudaStream_t s) {

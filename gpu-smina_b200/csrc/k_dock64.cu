@@ -159,6 +159,37 @@ __global__ void __launch_bounds__(32) k_refine64(const DModel* models, DTables T
             st3(out_coords + ((size_t)k * coord_stride + a) * 3, ld3(w.s + w.L.coords + 3 * m.heavy[a]));
 }
 
+// Final rescoring (finish_docking, main.cpp:257-282): per pose, model::eval on
+// the direct receptor sum (model.cpp:938-967 with non_cache::eval) and
+// model::eval_intramolecular (model.cpp:1027-1079), both on the fast table,
+// plus the heavy-atom coordinates of the pose.
+__global__ void __launch_bounds__(32) k_score64(const DModel* models, DTables T, const DReceptor* R,
+                                                const int* pose_model, int n, const double* confs, int conf_stride,
+                                                double v0, double v1, double v2, double slope, double* out_e,
+                                                double* out_intra, double* out_coords, int coord_stride, int* err) {
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    W64 w;
+    init_ws64(w, models + pose_model[k], &T, R, err);
+    const DModel& m = *w.m;
+    double* x = w.s + w.L.x_tmp;
+    vcopy(w, x, confs + (size_t)k * conf_stride, m.conf_size);
+    const double v[3] = {v0, v1, v2};
+    set_conf64(w, x);
+    direct_energy64(w, v[1], slope);
+    pairs_energy64(w, v);
+    __syncwarp();
+    const double e = energy64(w);
+    const double intra = intramolecular64(w, v);
+    if (w.lane == 0) {
+        out_e[k] = e;
+        out_intra[k] = intra;
+    }
+    if (out_coords)
+        for (int a = w.lane; a < m.nheavy; a += 32)
+            st3(out_coords + ((size_t)k * coord_stride + a) * 3, ld3(w.s + w.L.coords + 3 * m.heavy[a]));
+}
+
 // ---- host launchers -------------------------------------------------------------------------
 size_t ws64_bytes(const DModel& hm) {
     return (size_t)ws64_layout(hm.natoms, hm.nframes, hm.npairs, hm.conf_size, hm.dof).total * sizeof(double);
@@ -203,6 +234,16 @@ cudaError_t launch_refine64(const DModel* dms, size_t smem, const DTables& T, co
     if (rc != cudaSuccess) return rc;
     k_refine64<<<n, 32, smem, s>>>(dms, T, R, pose_model, n, confs, conf_stride, cap[0], cap[1], cap[2], maxiters,
                                    pose_maxiters, pose_box, accurate, early, e, coords, coord_stride, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_score64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const int* pose_model,
+                           int n, const double* confs, int conf_stride, const double v[3], double slope, double* e,
+                           double* intra, double* coords, int coord_stride, int* err, cudaStream_t s) {
+    cudaError_t rc = prep((const void*)k_score64, smem);
+    if (rc != cudaSuccess) return rc;
+    k_score64<<<n, 32, smem, s>>>(dms, T, R, pose_model, n, confs, conf_stride, v[0], v[1], v[2], slope, e, intra,
+                                  coords, coord_stride, err);
     return cudaGetLastError();
 }
 

@@ -154,6 +154,11 @@ struct Server {
     volatile int* h_err = nullptr;   // pinned copy, refreshed after every refinement launch
     Clock::time_point last_err_check;
     std::vector<std::unique_ptr<struct RefineGroup>> refining;
+    // pinned staging buffers for refinements (copies into pageable memory
+    // would make the worker wait for the refinement kernel)
+    std::vector<std::pair<size_t, char*>> pin_free;
+    std::vector<char*> pin_all;
+    size_t smem_block = 0;  // dynamic shared memory of every search launch (same for all, set at start)
     static constexpr int kFlags = 1 << 16;
     static constexpr int kMaxStreams = 112;  // concurrent kernels: 128 per device, some kept for refines and copies
 };
@@ -245,14 +250,12 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     }
     ws_stride = (ws_stride + 15) & ~(size_t)15;
     for (auto& r : reqs) max_chains = std::max(max_chains, r.job.num_chains);
-    int wpb = 0, occ = 0;
+    // the most chains per block that fit the server's fixed shared memory per block
+    int wpb = 0;
     for (int c : {8, 4, 2, 1}) {
         if (e->force_wpb && c != e->force_wpb) continue;
         if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;
-        const size_t smem = stage_stride + (size_t)c * ws_stride;
-        if (smem > (size_t)e->max_smem) continue;
-        const int o2 = mc32_occupancy(c, smem);
-        if (o2 * c > occ * wpb) { wpb = c; occ = o2; }
+        if (stage_stride + (size_t)c * ws_stride <= s.smem_block) { wpb = c; break; }
     }
     require(wpb > 0, "serve: model too large for the mixed-precision path's shared memory");
     std::vector<Item32> items;
@@ -339,12 +342,12 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     P.accurate_line = p.accurate_line;
     P.early_term = p.early_term;
     // one block per work item, so blocks of later batches fill in as these retire
-    cuda_check(launch_mc32(reinterpret_cast<const DModel*>(b->dmem + b->img.dmodel_off), tables32(e), tab[0],
-                           reinterpret_cast<const DMaps32*>(b->dmem + maps_at),
-                           reinterpret_cast<const Chain32*>(b->dmem + chains_at),
-                           reinterpret_cast<const Item32*>(b->dmem + items_at), (int)q.size(), P,
-                           reinterpret_cast<unsigned*>(b->dmem + queue_at), (int)q.size(), wpb, stage_stride, ws_stride,
-                           st),
+    cuda_check(launch_mc32_fixed(reinterpret_cast<const DModel*>(b->dmem + b->img.dmodel_off), tables32(e), tab[0],
+                                 reinterpret_cast<const DMaps32*>(b->dmem + maps_at),
+                                 reinterpret_cast<const Chain32*>(b->dmem + chains_at),
+                                 reinterpret_cast<const Item32*>(b->dmem + items_at), (int)q.size(), P,
+                                 reinterpret_cast<unsigned*>(b->dmem + queue_at), (int)q.size(), wpb, stage_stride,
+                                 ws_stride, s.smem_block, st),
                "serve: search launch");
     // The kernel-end event is recorded only when every ligand of the batch has
     // flagged completion: a command queued behind a kernel that runs for
@@ -397,11 +400,32 @@ static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
 struct RefineGroup {
     std::vector<SvLig*> ligs;
     std::vector<int> first;  // first pose of each ligand
-    std::vector<double> conf, e, xyz;
+    std::vector<double> conf;  // the merged poses' confs, built on the host
     int cs = 0, hs = 1;
     void* dbuf = nullptr;
     cudaEvent_t ev = nullptr;
+    char* pin = nullptr;  // pinned copy of the device buffer's layout
+    size_t pin_cap = 0;
+    const double *out_conf = nullptr, *out_e = nullptr, *out_xyz = nullptr;  // results, in pin
 };
+
+static char* pin_get(Server& s, size_t bytes, size_t& cap) {
+    for (size_t i = 0; i < s.pin_free.size(); i++)
+        if (s.pin_free[i].first >= bytes) {
+            char* p = s.pin_free[i].second;
+            cap = s.pin_free[i].first;
+            s.pin_free.erase(s.pin_free.begin() + i);
+            return p;
+        }
+    cap = std::max<size_t>(bytes, 1 << 20);
+    char* p = nullptr;
+    cuda_check(cudaHostAlloc((void**)&p, cap, cudaHostAllocDefault), "serve: pinned staging");
+    s.pin_all.push_back(p);
+    return p;
+}
+static void pin_put(Server& s, char* p, size_t cap) {
+    if (p) s.pin_free.emplace_back(cap, p);
+}
 
 static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& fin) {
     sg_engine* e = s.e;
@@ -448,18 +472,23 @@ static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& 
                  xb = (size_t)np * g->hs * 3 * sizeof(double), ib = (size_t)np * sizeof(int),
                  mb = dms.size() * sizeof(DModel);
     cudaStream_t rs = s.refine_stream;
-    cuda_check(cudaMallocAsync(&g->dbuf, cb + eb + xb + 2 * ib + mb + 256, rs), "serve: refine memory");
+    const size_t total = cb + eb + xb + 2 * ib + mb + 256;
+    cuda_check(cudaMallocAsync(&g->dbuf, total, rs), "serve: refine memory");
+    // the same layout in a pinned buffer: one copy in, one copy of the results out
+    const size_t c_at = (mb + 15) & ~(size_t)15, pm_at = c_at + cb + eb + xb;
+    g->pin = pin_get(s, total, g->pin_cap);
+    std::memcpy(g->pin, dms.data(), mb);
+    std::memcpy(g->pin + c_at, g->conf.data(), cb);
+    std::memcpy(g->pin + pm_at, pose_model.data(), ib);
+    std::memcpy(g->pin + pm_at + ib, pose_maxit.data(), ib);
     char* base = static_cast<char*>(g->dbuf);
     DModel* d_models = reinterpret_cast<DModel*>(base);
-    double* dc = reinterpret_cast<double*>(base + ((mb + 15) & ~(size_t)15));
+    double* dc = reinterpret_cast<double*>(base + c_at);
     double* de = dc + g->conf.size();
     double* dx = de + np;
-    int* dpm = reinterpret_cast<int*>(dx + (size_t)np * g->hs * 3);
+    int* dpm = reinterpret_cast<int*>(base + pm_at);
     int* dmi = dpm + np;
-    cuda_check(cudaMemcpyAsync(d_models, dms.data(), mb, cudaMemcpyHostToDevice, rs), "serve");
-    cuda_check(cudaMemcpyAsync(dc, g->conf.data(), cb, cudaMemcpyHostToDevice, rs), "serve");
-    cuda_check(cudaMemcpyAsync(dpm, pose_model.data(), ib, cudaMemcpyHostToDevice, rs), "serve");
-    cuda_check(cudaMemcpyAsync(dmi, pose_maxit.data(), ib, cudaMemcpyHostToDevice, rs), "serve");
+    cuda_check(cudaMemcpyAsync(base, g->pin, pm_at + 2 * ib, cudaMemcpyHostToDevice, rs), "serve");
     int p0 = 0;
     for (auto& [rid, members] : by_rec) {
         int n = 0;
@@ -474,11 +503,10 @@ static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& 
         }
         p0 += n;
     }
-    g->e.resize(np);
-    g->xyz.resize((size_t)np * g->hs * 3);
-    cuda_check(cudaMemcpyAsync(g->conf.data(), dc, cb, cudaMemcpyDeviceToHost, rs), "serve");
-    cuda_check(cudaMemcpyAsync(g->e.data(), de, eb, cudaMemcpyDeviceToHost, rs), "serve");
-    cuda_check(cudaMemcpyAsync(g->xyz.data(), dx, xb, cudaMemcpyDeviceToHost, rs), "serve");
+    cuda_check(cudaMemcpyAsync(g->pin + c_at, dc, cb + eb + xb, cudaMemcpyDeviceToHost, rs), "serve");
+    g->out_conf = reinterpret_cast<const double*>(g->pin + c_at);
+    g->out_e = g->out_conf + g->conf.size();
+    g->out_xyz = g->out_e + np;
     cuda_check(cudaMemcpyAsync((void*)s.h_err, s.d_err, sizeof(int), cudaMemcpyDeviceToHost, rs), "serve");
     cuda_check(cudaFreeAsync(g->dbuf, rs), "serve");
     g->dbuf = nullptr;
@@ -501,9 +529,9 @@ static void publish(Server& s, const RefineGroup& g, size_t k) {
     d.info.evals = L.evals;
     for (int i = 0; i < np; i++) {
         const size_t q = (size_t)g.first[k] + i;
-        L.poses[i].e = g.e[q];
-        std::memcpy(L.poses[i].conf.data(), &g.conf[q * g.cs], cs * sizeof(double));
-        L.poses[i].xyz.assign(&g.xyz[q * g.hs * 3], &g.xyz[q * g.hs * 3] + (size_t)H * 3);
+        L.poses[i].e = g.out_e[q];
+        std::memcpy(L.poses[i].conf.data(), &g.out_conf[q * g.cs], cs * sizeof(double));
+        L.poses[i].xyz.assign(&g.out_xyz[q * g.hs * 3], &g.out_xyz[q * g.hs * 3] + (size_t)H * 3);
     }
     std::stable_sort(L.poses.begin(), L.poses.end(), [](const SvPose& a, const SvPose& c) { return a.e < c.e; });
     d.info.count = np;
@@ -611,6 +639,7 @@ static void worker(Server* sp) {
                         g.ligs[k]->batch->published++;
                     }
                     if (g.ev) cudaEventDestroy(g.ev);
+                    pin_put(s, g.pin, g.pin_cap);
                     s.refining.erase(s.refining.begin() + i);
                     s.cv_done.notify_all();
                     busy = true;
@@ -694,12 +723,19 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
         if (o) s->o = *o;
         if (s->o.max_batch_ligands <= 0) s->o.max_batch_ligands = 64;
         if (s->o.max_wait_ms <= 0) s->o.max_wait_ms = 20.0;
-        if (s->o.max_inflight_ligands <= 0) s->o.max_inflight_ligands = 2 * e->num_sms;  // resident 8-chain blocks
+        // resident 8-chain blocks, less a few slots so that refinements find room beside the search
+        if (s->o.max_inflight_ligands <= 0) s->o.max_inflight_ligands = std::max(1, 2 * e->num_sms - 16);
         if (s->o.hbm_budget_bytes == 0) {
             size_t fr = 0, tot = 0;
             cuda_check(cudaMemGetInfo(&fr, &tot), "serve: memory info");
             s->o.hbm_budget_bytes = fr / 4;
         }
+        // Every search launch takes the same shared memory per block: two blocks
+        // fit an SM's 164 KB configuration (with the kernel's static shared
+        // memory and the 1 KB the driver keeps per block), which leaves L1 room
+        // for the gathers; bigger models run fewer chains per block.
+        s->smem_block = std::min<size_t>((size_t)e->max_smem, 82048);
+        cuda_check(serve_prepare32(s->smem_block), "serve: kernel attributes");
         cuda_check(cudaStreamCreateWithFlags(&s->refine_stream, cudaStreamNonBlocking), "serve: stream");
         cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "serve: stream");
         unsigned* hf = nullptr;
@@ -836,6 +872,7 @@ int sg_serve_stop(sg_engine* e) {
         cudaFreeHost((void*)s->flags);
         cudaFree(s->d_err);
         cudaFreeHost((void*)s->h_err);
+        for (char* p : s->pin_all) cudaFreeHost(p);
         const int err = s->error;
         const std::string why = s->error_text;
         {

@@ -19,7 +19,11 @@ struct sgh_receptor {
     std::vector<double> xyz, q;
     std::vector<int> t;
 };
-struct sgh_tables { sgh::Tables t; };
+struct sgh_tables {
+    sgh::Tables t;
+    std::vector<std::string> ci_names;  // conf-independent terms, in order, and their weights
+    std::vector<double> ci_w;
+};
 
 static thread_local std::string g_err;
 
@@ -112,6 +116,8 @@ int sgh_tables_create(const char* builtin_name, const char* custom_text, double 
         if (sf.indep.empty() && sf.dep.empty()) throw std::runtime_error("scoring function has no distance terms");
         sgh_tables* t = new sgh_tables();
         sgh::build_linear_tables(sf, factor, t->t);
+        t->ci_names = sf.conf_indep_names;
+        t->ci_w = sf.conf_indep_w;
         *out = t;
     });
 }
@@ -119,6 +125,79 @@ void sgh_tables_free(sgh_tables* t) { delete t; }
 int sgh_tables_desc(const sgh_tables* t, sg_tables_desc* out) {
     *out = t->t.desc();
     return SG_OK;
+}
+
+int sgh_model_conf_independent_inputs(const sgh_model* m, double out[7]) {
+    if (!m || !out) return SG_ERR_ARG;
+    std::copy(m->m.ci, m->m.ci + 7, out);
+    return SG_OK;
+}
+
+int sgh_tables_conf_independent(const sgh_tables* t, const double inputs[7], double x, double* out) {
+    if (!t || !inputs || !out) return SG_ERR_ARG;
+    return guarded([&] { *out = sgh::conf_independent(t->ci_names, t->ci_w, inputs, x); });
+}
+
+// finish_docking (main.cpp:257-324) for one ligand's refined poses
+int sgh_finish_docking(const sgh_tables* t, const double inputs[7], int n, const double* e_refined,
+                       const double* e_total, const double* e_intra, const double* coords, int heavy,
+                       double out_min_rmsd, int num_modes, double energy_range, int* out_index, double* out_e,
+                       int* out_count) {
+    if (!t || !inputs || n < 0 || heavy < 0 || !out_count || (n > 0 && (!e_refined || !e_total || !e_intra ||
+                                                                         !coords || !out_index || !out_e)))
+        return SG_ERR_ARG;
+    return guarded([&] {
+        *out_count = 0;
+        if (n == 0) return;
+        auto not_max = [](double x) { return x < 0.1 * DBL_MAX; };
+        std::vector<int> order(n);
+        for (int k = 0; k < n; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e_refined[a] < e_refined[b]; });
+        // the best mode's intramolecular energy, then every pose's adjusted energy
+        const double intra = e_intra[order[0]];
+        std::vector<double> e(n);
+        for (int k = 0; k < n; k++)
+            e[k] = not_max(e_refined[k]) ? sgh::conf_independent(t->ci_names, t->ci_w, inputs, e_total[k] - intra)
+                                         : e_refined[k];
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e[a] < e[b]; });
+        // remove_redundant (main.cpp:204-210): add_to_output_container (coords.cpp:25-58) pose by pose
+        auto rmsd = [&](int a, int b) {  // rmsd_upper_bound over heavy-atom coords
+            double acc = 0;
+            for (int i = 0; i < heavy; i++)
+                for (int d = 0; d < 3; d++) {
+                    const double x = coords[((size_t)a * heavy + i) * 3 + d] - coords[((size_t)b * heavy + i) * 3 + d];
+                    acc += x * x;
+                }
+            return heavy > 0 ? std::sqrt(acc / heavy) : 0.0;
+        };
+        std::vector<int> kept;
+        for (int k : order) {
+            size_t ci = kept.size();
+            double cr = DBL_MAX;
+            for (size_t i = 0; i < kept.size(); i++) {
+                const double r = rmsd(k, kept[i]);
+                if (i == 0 || r < cr) { ci = i; cr = r; }
+            }
+            if (ci < kept.size() && cr < out_min_rmsd) {
+                if (e[k] < e[kept[ci]]) kept[ci] = k;
+            } else if ((int)kept.size() < n) {
+                kept.push_back(k);
+            } else if (!kept.empty() && e[k] < e[kept.back()]) {
+                kept.back() = k;
+            }
+            std::stable_sort(kept.begin(), kept.end(), [&](int a, int b) { return e[a] < e[b]; });
+        }
+        // the modes written: at most num_modes, none at max energy or past energy_range
+        int how_many = 0;
+        for (size_t i = 0; i < kept.size(); i++) {
+            const double ei = e[kept[i]];
+            if (how_many >= num_modes || !not_max(ei) || ei > e[kept[0]] + energy_range) break;
+            out_index[how_many] = kept[i];
+            out_e[how_many] = ei;
+            how_many++;
+        }
+        *out_count = how_many;
+    });
 }
 
 int sgh_make_box(const double center[3], const double size[3], double granularity, sg_grid_dims* out) {

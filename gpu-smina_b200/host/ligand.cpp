@@ -482,6 +482,44 @@ Model read_pdbqt_ligand(const std::string& text) {
             }
         }
     }
+    // conf_independent_inputs (terms.cpp:83-120): counts over the ligand's
+    // heavy atoms; a rotatable bond is one across a branch axis (DISTANCE_ROTOR)
+    auto nbh = [&](int i) {  // num_bonded_heavy_atoms (terms.cpp:40-53)
+        int c = 0;
+        for (int j : bonds[i]) c += !is_hydrogen(F.atoms[j].type);
+        return c;
+    };
+    for (int i = 0; i < N; i++) {
+        const int t = F.atoms[i].type;
+        if (is_hydrogen(t)) continue;
+        unsigned ar = 0;  // atom_rotors (terms.cpp:55-81), rotable hydrogens fixed
+        for (int j : bonds[i])
+            if (mobility(i, j) == D_ROTOR && !is_hydrogen(F.atoms[j].type) && nbh(j) > 1 && nbh(i) > 1) ar++;
+        m.ci[0] += 0.5 * ar;                   // num_tors
+        m.ci[1] += ar > 2 ? 0.5 : 0.5 * ar;    // num_rotors
+        m.ci[2] += 1;                          // num_heavy_atoms
+        if (type_info(t).xs_hydrophobe) m.ci[3] += 1;
+        if (type_info(t).xs_acceptor || type_info(t).xs_donor) m.ci[4] += 1;
+    }
+    m.ci[5] = 1;  // num_ligands
+    // ligand_length: get_branch_metrics(...).corner2corner over the branch tree (model.cpp:62-109)
+    std::function<std::pair<long, long>(int)> metrics = [&](int f) -> std::pair<long, long> {
+        long c2c_max = 0;
+        std::vector<long> lengths;
+        for (int c = 0; c < nf; c++)
+            if (F.fparent[c] == f) {
+                auto r = metrics(c);
+                c2c_max = std::max(c2c_max, r.second);
+                lengths.push_back(r.first + 1);
+            }
+        if (lengths.empty()) return {0, 0};
+        std::sort(lengths.begin(), lengths.end());
+        long len = lengths.back(), c2c = len;
+        if (lengths.size() >= 2) c2c += lengths[lengths.size() - 1];  // as the reference adds it
+        if (c2c < c2c_max) c2c = c2c_max;
+        return {len, c2c};
+    };
+    m.ci[6] = (double)metrics(0).second;  // ligand_lengths_sum
     m.num_other_pairs = 0;
     m.num_ligands = 1;
     m.num_flex = 0;
@@ -670,6 +708,7 @@ Model read_pdbqt_flex(const std::string& ligand_text, const std::string& flex_te
     m.conf_size = L.conf_size + (int)F.fparent.size();
     m.dof = L.dof + (int)F.fparent.size();
     m.torsdof = L.torsdof;
+    std::copy(L.ci, L.ci + 7, m.ci);  // conf-independent inputs count ligand atoms only
     for (size_t k = 0; k < fpairs.size(); k += 2) {
         m.pairs.push_back(fmap(fpairs[k]));
         m.pairs.push_back(fmap(fpairs[k + 1]));

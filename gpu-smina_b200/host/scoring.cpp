@@ -8,6 +8,7 @@
  */
 #include "sg_host.h"
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <limits>
 #include <regex>
@@ -426,4 +427,58 @@ void build_linear_tables(const Scoring& sf, double factor, Tables& T) {
         }
 }
 
+// smooth_div (everything.h:55-59)
+static double smooth_div(double x, double y) {
+    if (std::abs(x) < DBL_EPSILON) return 0;
+    if (std::abs(y) < DBL_EPSILON) return (x * y > 0) ? DBL_MAX : -DBL_MAX;
+    return x / y;
+}
+
+// weighted_terms::conf_independent (weighted_terms.cpp:74-80): the enabled
+// conf-independent terms in order (terms.cpp:311-318), each with its own
+// weight, formulas of everything.h:730-1000.  in: num_tors, num_rotors,
+// num_heavy_atoms, num_hydrophobic_atoms, ligand_max_num_h_bonds,
+// num_ligands, ligand_lengths_sum.
+double conf_independent(const std::vector<std::string>& names, const std::vector<double>& weights, const double in[7],
+                        double x) {
+    for (size_t k = 0; k < names.size(); k++) {
+        const std::string& n = names[k];
+        const double r = weights[k];
+        if (n == "num_tors_add") {
+            x = x + r * in[0];
+        } else if (n == "num_tors_sqr") {
+            const double w = 0.1 * r;
+            x = x + w * (in[0] * in[0]) / 5;
+        } else if (n == "num_tors_sqrt") {
+            const double w = 0.1 * r;
+            x = x + w * std::sqrt(in[0]) / std::sqrt(5.0);
+        } else if (n == "num_tors_div") {
+            const double w = 0.1 * (r + 1);
+            x = smooth_div(x, 1 + w * in[0] / 5.0);
+        } else if (n == "num_tors_div_simple") {
+            x = smooth_div(x, 1 + r * in[0]);
+        } else if (n == "ligand_length") {
+            x = x + r * in[6];
+        } else if (n == "num_ligands") {
+            const double w = 1 * r;
+            x = x + w * in[5];
+        } else if (n == "num_heavy_atoms_div") {
+            const double w = 0.05 * r;
+            x = smooth_div(x, 1 + w * in[2]);
+        } else if (n == "num_heavy_atoms") {
+            const double w = 0.05 * r;
+            x = x + w * in[2];
+        } else if (n == "num_hydrophobic_atoms") {
+            const double w = 0.05 * r;
+            x = x + w * in[3];
+        } else if (n == "constant_term") {
+            x = x + r;
+        } else {
+            throw std::runtime_error("unknown conf-independent term " + n);
+        }
+    }
+    return x;
+}
+
 }  // namespace sgh
+

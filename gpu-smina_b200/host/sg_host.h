@@ -77,6 +77,9 @@ struct Tables {
     sg_tables_desc desc() const;
 };
 void build_linear_tables(const Scoring& sf, double factor, Tables& out);
+// weighted_terms::conf_independent: the conf-independent terms in order
+double conf_independent(const std::vector<std::string>& names, const std::vector<double>& weights, const double in[7],
+                        double x);
 
 // ---- molecules --------------------------------------------------------------
 struct Atom {
@@ -99,6 +102,10 @@ struct Model {
     int num_other_pairs = 0;
     int num_ligands = 0, num_flex = 0, conf_size = 0, dof = 0;
     int torsdof = 0;                              // TORSDOF of the ligand
+    // conf_independent_inputs of the ligand(s): num_tors, num_rotors,
+    // num_heavy_atoms, num_hydrophobic_atoms, ligand_max_num_h_bonds,
+    // num_ligands, ligand_lengths_sum
+    double ci[7] = {0, 0, 0, 0, 0, 0, 0};
     std::string name;
     sg_model_desc desc() const;
     int num_heavy_movable() const;

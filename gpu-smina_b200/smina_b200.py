@@ -141,6 +141,12 @@ def _declare(L):
                       C.c_int, C.c_int, C.c_int, _dp, _dp],
         "sg_bfgs": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, C.c_int, C.c_int,
                     C.c_int, _dp],
+        "sg_score": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _ip, C.c_int, _dp, C.c_int, C.c_double * 3, C.c_double,
+                     _dp, _dp, _dp, C.c_int],
+        "sgh_model_conf_independent_inputs": [vp, _dp],
+        "sgh_tables_conf_independent": [vp, _dp, C.c_double, _dp],
+        "sgh_finish_docking": [vp, _dp, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp,
+                               _ip],
         "sg_minimize": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _ip, C.c_int, _dp, C.c_int, _dp, C.c_double * 3,
                         _ip, C.c_int, C.c_int, _dp, _dp, C.c_int],
         "sg_dock_batch32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
@@ -236,6 +242,13 @@ class Model:
         load().sgh_search_params(self._h, num_modes, C.byref(p))
         return p
 
+    def conf_independent_inputs(self):
+        """num_tors, num_rotors, num_heavy_atoms, num_hydrophobic_atoms,
+        ligand_max_num_h_bonds, num_ligands, ligand_lengths_sum (terms.cpp:83-120)."""
+        out = np.zeros(7)
+        _check_host(load().sgh_model_conf_independent_inputs(self._h, dptr(out)))
+        return out
+
     def seed_chains(self, seed: int, tasks: int, box: GridDims):
         confs = np.zeros((tasks, self.conf_size))
         mt = np.zeros((tasks, 625), dtype=np.uint32)
@@ -303,6 +316,28 @@ class Tables:
         self._h = h
         self.desc = TablesDesc()
         L.sgh_tables_desc(h, C.byref(self.desc))
+
+    def conf_independent(self, inputs, x: float) -> float:
+        """The scoring function's conf-independent terms applied to x."""
+        out = C.c_double()
+        _check_host(load().sgh_tables_conf_independent(self._h, dptr(np.ascontiguousarray(inputs, dtype=np.float64)),
+                                                         float(x), C.byref(out)))
+        return out.value
+
+    def finish_docking(self, inputs, e_refined, e_total, e_intra, coords, out_min_rmsd=1.0, num_modes=9,
+                       energy_range=3.0):
+        """finish_docking for one ligand's refined poses (sgh_finish_docking):
+        returns (indices of the kept poses, their final energies)."""
+        er = np.ascontiguousarray(e_refined, dtype=np.float64)
+        n = len(er)
+        xyz = np.ascontiguousarray(coords, dtype=np.float64).reshape(n, -1, 3)
+        idx, e, cnt = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1)), C.c_int()
+        _check_host(load().sgh_finish_docking(self._h, dptr(np.ascontiguousarray(inputs, dtype=np.float64)), n,
+                                              dptr(er), dptr(np.ascontiguousarray(e_total, dtype=np.float64)),
+                                              dptr(np.ascontiguousarray(e_intra, dtype=np.float64)), dptr(xyz),
+                                              xyz.shape[1], out_min_rmsd, num_modes, energy_range, iptr(idx), dptr(e),
+                                              C.byref(cnt)))
+        return idx[:cnt.value].copy(), e[:cnt.value].copy()
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -559,6 +594,23 @@ class Engine:
         self._check(load().sg_autotune32(self._h, rid, descs, len(models), J, len(jobs), C.byref(params),
                                          float(step_fraction), dptr(rate), C.byref(chosen)))
         return chosen.value, {c: float(v) for c, v in zip((8, 4, 2, 1), rate)}
+
+    def score(self, rid, models, pose_model, confs, v=(1000, 1000, 1000), slope=1e6):
+        """finish_docking's energies per pose (sg_score): model::eval on the
+        direct receptor sum and model::eval_intramolecular, FP64.  Returns
+        (e_total [n], e_intra [n], heavy coords [n][H][3])."""
+        descs = (ModelDesc * len(models))(*[m.desc for m in models])
+        pm = np.ascontiguousarray(pose_model, dtype=np.int32)
+        n = len(pm)
+        cs = max(m.conf_size for m in models)
+        H = max(m.heavy for m in models)
+        c = np.zeros((n, cs))
+        src = np.asarray(confs, dtype=np.float64).reshape(n, -1)
+        c[:, :src.shape[1]] = src
+        e, intra, xyz = np.zeros(n), np.zeros(n), np.zeros((n, H, 3))
+        self._check(load().sg_score(self._h, rid, descs, len(models), iptr(pm), n, dptr(c), cs, vec3(v), slope, dptr(e),
+                                    dptr(intra), dptr(xyz), H))
+        return e, intra, xyz
 
     def minimize(self, rid, models, pose_model, confs, boxes=None, cap=(1000, 1000, 1000), maxiters=10,
                  accurate_line=0, early_term=0):

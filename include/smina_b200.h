@@ -21,6 +21,7 @@
  *   sg_refine                    run_refine (refine_structure)          src/gpu/gpu_kernels_impl.cuh:999-1098,
  *                                                                        src/main/main.cpp:165-190
  *   sg_minimize                  GpuDocking::minimize_batch             src/gpu/gpu_docking.cpp:690-742
+ *   sg_score                     finish_docking's rescoring energies    src/main/main.cpp:257-282
  *   sg_dock_batch32              GpuDocking::dock_batch (batched screen) src/gpu/gpu_docking.cpp:756-831
  *   sg_serve_*                   (no counterpart: continuous-batching request loop)
  *   sg_dock_batch32_noalloc      (no counterpart: the batched search without device allocation)
@@ -249,6 +250,21 @@ int sg_minimize(sg_engine* e, int receptor_id, const sg_model_desc* models, int 
                 int accurate_line, int early_term, double* out_e, double* out_coords,
                 int coord_stride);
 
+/* Final rescoring of docked poses (finish_docking, src/main/main.cpp:257-282):
+ * for every pose, model::eval on the direct receptor sum with the fast
+ * table (model.cpp:938-967, non_cache::eval non_cache.cpp:34-91) into
+ * out_e, and model::eval_intramolecular (model.cpp:1027-1079) into
+ * out_intra, both with terms curled at v (authentic_v in the reference) and
+ * the out-of-box penalty at `slope`; FP64, bit-exact with the CPU
+ * algorithm.  confs [n][conf_stride]; out_coords [n][coord_stride][3] heavy
+ * atoms (may be NULL; rows past a pose's heavy count are 0).  The rescored
+ * energy of a pose is then conf_independent(out_e - out_intra of the best
+ * pose): see sgh_finish_docking. */
+int sg_score(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmodels,
+             const int* pose_model, int nposes, const double* confs, int conf_stride,
+             const double v[3], double slope, double* out_e, double* out_intra,
+             double* out_coords, int coord_stride);
+
 /* ---- batched mixed-precision docking (virtual screening) ---------------
  * Replaces GpuDocking::dock_batch (src/gpu/gpu_docking.h:91-94,
  * gpu_docking.cpp:756): for every ligand job, its Monte Carlo chains,
@@ -354,7 +370,7 @@ typedef struct sg_serve_opts {
     int max_inflight_ligands;   /* ligands on the device before requests
                                    start to gather (0: two per SM, what the
                                    device holds at once with 8 chains per
-                                   ligand)                                   */
+                                   ligand, less 16 kept for refinements)     */
 } sg_serve_opts;
 
 typedef struct sg_serve_done {

@@ -44,6 +44,10 @@ void sgh_model_free(sgh_model* m);
 int  sgh_model_desc(const sgh_model* m, sg_model_desc* out);
 int  sgh_model_heavy(const sgh_model* m);
 int  sgh_model_torsdof(const sgh_model* m);
+/* conf_independent_inputs of the model's ligand (terms.cpp:83-120):
+ * out[7] = num_tors, num_rotors, num_heavy_atoms, num_hydrophobic_atoms,
+ * ligand_max_num_h_bonds, num_ligands, ligand_lengths_sum */
+int  sgh_model_conf_independent_inputs(const sgh_model* m, double out[7]);
 
 int  sgh_make_receptor(int heavy_atoms, uint64_t seed, const double center[3], double cavity_radius,
                        sgh_receptor** out);
@@ -64,6 +68,22 @@ int  sgh_make_flex_pdbqt(int residues, uint64_t seed, const double center[3], do
 int  sgh_tables_create(const char* builtin_name, const char* custom_text, double factor, sgh_tables** out);
 void sgh_tables_free(sgh_tables* t);
 int  sgh_tables_desc(const sgh_tables* t, sg_tables_desc* out);
+/* weighted_terms::conf_independent (weighted_terms.cpp:74-80): the scoring
+ * function's conf-independent terms (num_tors_div, ...) applied to x in
+ * order; inputs as sgh_model_conf_independent_inputs gives them */
+int  sgh_tables_conf_independent(const sgh_tables* t, const double inputs[7], double x, double* out);
+/* finish_docking (src/main/main.cpp:257-324) for one ligand: poses sorted by
+ * their refined energy; every pose not at max energy rescored as
+ * conf_independent(e_total - e_intra of the best pose) with e_total and
+ * e_intra from sg_score; sorted again; remove_redundant at out_min_rmsd over
+ * the heavy-atom coords [n][heavy][3]; at most num_modes poses, none at max
+ * energy or more than energy_range above the best.  out_index / out_e get
+ * the kept poses (indices into the inputs) and their final energies;
+ * *out_count how many. */
+int  sgh_finish_docking(const sgh_tables* t, const double inputs[7], int n, const double* e_refined,
+                        const double* e_total, const double* e_intra, const double* coords, int heavy,
+                        double out_min_rmsd, int num_modes, double energy_range, int* out_index, double* out_e,
+                        int* out_count);
 
 int  sgh_make_box(const double center[3], const double size[3], double granularity, sg_grid_dims* out);
 int  sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out);

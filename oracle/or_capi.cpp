@@ -263,6 +263,28 @@ int or_minimize(or_ctx* o, const sg_model_desc* models, const int* pose_model, i
     return 0;
 }
 
+/* finish_docking's rescoring energies per pose (model::eval on the direct
+ * sum, model::eval_intramolecular), heavy-atom coords */
+int or_score(or_ctx* o, const sg_model_desc* models, const int* pose_model, int nposes, const double* confs,
+             int conf_stride, const double v[3], double slope, double* out_e, double* out_intra, double* out_coords,
+             int coord_stride) {
+    Model m;
+    try {
+        for (int k = 0; k < nposes; k++) {
+            m.load(models[pose_model[k]]);
+            std::vector<V3> hc;
+            score_pose(o->c, m, confs + (size_t)k * conf_stride, v, slope, out_e[k], out_intra[k], hc);
+            if (out_coords)
+                for (size_t a = 0; a < hc.size(); a++)
+                    for (int d = 0; d < 3; d++) out_coords[((size_t)k * coord_stride + a) * 3 + d] = hc[a][d];
+        }
+    } catch (std::exception& e) {
+        o->err = e.what();
+        return 1;
+    }
+    return 0;
+}
+
 /* scalar math probes: fn 0 sin, 1 cos, 2 acos, 3 exp */
 void or_pm_eval(int fn, const double* x, double* y, int n) {
     for (int i = 0; i < n; i++) {

@@ -900,4 +900,115 @@ double bfgs_cache(const Ctx& c, const Model& m, std::vector<double>& x, const do
 
 void state_for_eval(const Model& m, State& s) { state_init(m, s); }
 
+
+// ---- final rescoring energies (finish_docking, main.cpp:257-282) -----------------------------
+// precalculate_linear::eval (precalculate.h:75-83,103-108,191-203) with
+// result_components::eval (result_components.h:75-81): the fast table at
+// sz(factor r2); for t1 > t2 the (t2, t1) components with A and B swapped
+static double table_eval_fast(const Tables& T, int t1, double qa, int t2, double qb, double r2) {
+    const double* c = &T.fast[((size_t)T.pair_index(t1, t2) * T.n + (size_t)(T.factor * r2)) * T.nc];
+    double comp[4] = {c[0], 0, 0, 0};
+    if (T.nc > 1) { comp[1] = c[1]; comp[2] = c[2]; comp[3] = c[3]; }
+    if (t1 > t2) std::swap(comp[1], comp[2]);  // result_components::swapOrder
+    return comp[0] + std::fabs(qa) * comp[1] + std::fabs(qb) * comp[2] + qa * qb * comp[3];
+}
+
+// model::eval_interacting_pairs (model.cpp:885-902)
+static double pairs_energy(const Tables& T, const Model& m, int begin, int end, double v, const State& s) {
+    double e = 0;
+    for (int k = begin; k < end; k++) {
+        const int a = m.pairs[k][0], b = m.pairs[k][1];
+        const double r2 = sqrv(s.coords[a] - s.coords[b]);
+        if (r2 < T.cutoff_sqr) {
+            double tmp = table_eval_fast(T, m.type[a], m.charge[a], m.type[b], m.charge[b], r2);
+            curl(tmp, v);
+            e += tmp;
+        }
+    }
+    return e;
+}
+
+static bool in_ligand(const Model& m, int i) {  // model::find_ligand(i) < ligands.size()
+    for (int l = 0; l < m.num_ligands; l++)
+        if (i >= m.lig_begin[l] && i < m.lig_end[l]) return true;
+    return false;
+}
+
+// model::eval (model.cpp:945-967) with non_cache::eval (non_cache.cpp:34-91),
+// and model::eval_intramolecular (model.cpp:1027-1079), at one conf
+void score_pose(Ctx& c, const Model& m, const double* conf, const double v[3], double slope, double& e_out,
+                double& intra_out, std::vector<V3>& coords_out) {
+    CellLists cl;
+    cl.full_cells = c.full_cells;
+    cl.init(c.rec, c.tab.cutoff_sqr, c.geom.gd);
+    State s;
+    state_init(m, s);
+    model_set(m, conf, s);
+    const sg_grid_dims& gd = c.geom.gd;
+    // non_cache::eval
+    double e = 0;
+    for (int i = 0; i < m.num_movable; i++) {
+        const int t = m.type[i];
+        if (t >= SG_NUM_TYPES || is_h(t)) continue;
+        double this_e = 0, oob = 0;
+        const V3 a = s.coords[i];
+        V3 adj = a;
+        for (int j = 0; j < 3; j++) {
+            if (gd.n[j] > 0) {
+                if (a[j] < gd.begin[j]) { adj[j] = gd.begin[j]; oob += std::fabs(a[j] - gd.begin[j]); }
+                else if (a[j] > gd.end[j]) { adj[j] = gd.end[j]; oob += std::fabs(a[j] - gd.end[j]); }
+            }
+        }
+        oob *= slope;
+        for (int j : cl.get(adj)) {
+            const double r2 = sqrv(adj - c.rec.xyz[j]);
+            if (r2 < c.tab.cutoff_sqr) this_e += table_eval_fast(c.tab, t, m.charge[i], c.rec.type[j], c.rec.charge[j], r2);
+        }
+        curl(this_e, v[1]);
+        e += this_e + oob;
+    }
+    // model::evale: + other pairs; model::eval: + each ligand's pairs
+    e += pairs_energy(c.tab, m, 0, m.num_other_pairs, v[2], s);
+    int start = m.num_other_pairs;
+    for (int l = 0; l < m.num_ligands; l++) {
+        e += pairs_energy(c.tab, m, start, m.lig_pair_end[l], v[0], s);
+        start = m.lig_pair_end[l];
+    }
+    // model::eval_intramolecular
+    double intra = 0;
+    start = m.num_other_pairs;
+    for (int l = 0; l < m.num_ligands; l++) {
+        intra += pairs_energy(c.tab, m, start, m.lig_pair_end[l], v[0], s);
+        start = m.lig_pair_end[l];
+    }
+    for (int i = 0; i < m.num_movable; i++) {  // flex-rigid
+        if (in_ligand(m, i)) continue;
+        const int t1 = m.type[i];
+        if (t1 >= SG_NUM_TYPES) continue;
+        for (size_t j = 0; j < c.rec.xyz.size(); j++) {
+            const int t2 = c.rec.type[j];
+            if (t2 >= SG_NUM_TYPES) continue;
+            const double r2 = sqrv(s.coords[i] - c.rec.xyz[j]);
+            if (r2 < c.tab.cutoff_sqr) {
+                double this_e = table_eval_fast(c.tab, t1, m.charge[i], t2, c.rec.charge[j], r2);
+                curl(this_e, v[1]);
+                intra += this_e;
+            }
+        }
+    }
+    for (int k = 0; k < m.num_other_pairs; k++) {  // flex-flex
+        const int a = m.pairs[k][0], b = m.pairs[k][1];
+        if (in_ligand(m, a) || in_ligand(m, b)) continue;
+        const double r2 = sqrv(s.coords[a] - s.coords[b]);
+        if (r2 < c.tab.cutoff_sqr) {
+            double this_e = table_eval_fast(c.tab, m.type[a], m.charge[a], m.type[b], m.charge[b], r2);
+            curl(this_e, v[2]);
+            intra += this_e;
+        }
+    }
+    e_out = e;
+    intra_out = intra;
+    coords_out = heavy_coords(m, s);
+}
+
 }  // namespace orc

@@ -160,5 +160,9 @@ struct Out { std::vector<double> c; double e; std::vector<V3> coords; };
 struct Container { std::vector<Out> v; };
 void add_to_output_container(Container& out, const Out& t, double min_rmsd, int max_size);  // coords.cpp:43-58
 struct MinParams { int maxiters; int accurate_line; int early_term; };
+// finish_docking's energies of one pose: model::eval on the direct sum and
+// model::eval_intramolecular, fast table (main.cpp:257-282)
+void score_pose(Ctx& c, const Model& m, const double* conf, const double v[3], double slope, double& e_out,
+                double& intra_out, std::vector<V3>& coords_out);
 }  // namespace orc
 #endif

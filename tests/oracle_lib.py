@@ -46,6 +46,8 @@ def load():
                          sb._dp],
             "or_refine": [vp, C.POINTER(sb.ModelDesc), sb._ip, C.c_int, sb._dp, C.c_double * 3, C.c_int, C.c_int,
                           C.c_int, sb._dp, sb._dp],
+            "or_score": [vp, C.POINTER(sb.ModelDesc), sb._ip, C.c_int, sb._dp, C.c_int, C.c_double * 3, C.c_double,
+                         sb._dp, sb._dp, sb._dp, C.c_int],
             "or_minimize": [vp, C.POINTER(sb.ModelDesc), sb._ip, C.c_int, sb._dp, C.c_int, sb._dp, C.c_double * 3,
                             sb._ip, C.c_int, C.c_int, sb._dp, sb._dp, C.c_int],
         }
@@ -162,6 +164,20 @@ class Oracle:
         self._check(load().or_minimize(self.h, descs, sb.iptr(pm), n, sb.dptr(c), cs, sb.dptr(bx), sb.vec3(cap),
                                        sb.iptr(mi), accurate, early, sb.dptr(e), sb.dptr(x), H))
         return c, e, x
+
+    def score(self, models, pose_model, confs, v=(1000, 1000, 1000), slope=1e6):
+        descs = (sb.ModelDesc * len(models))(*[m.desc for m in models])
+        pm = np.ascontiguousarray(pose_model, dtype=np.int32)
+        n = len(pm)
+        cs = max(m.conf_size for m in models)
+        H = max(m.heavy for m in models)
+        c = np.zeros((n, cs))
+        src = np.asarray(confs, dtype=np.float64).reshape(n, -1)
+        c[:, :src.shape[1]] = src
+        e, intra, x = np.zeros(n), np.zeros(n), np.zeros((n, H, 3))
+        self._check(load().or_score(self.h, descs, sb.iptr(pm), n, sb.dptr(c), cs, sb.vec3(v), slope, sb.dptr(e),
+                                    sb.dptr(intra), sb.dptr(x), H))
+        return e, intra, x
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
