@@ -297,6 +297,8 @@ def run_serve(args):
     eng.serve_start()
     lat, evals = {}, 0
     k = 0
+    occupancy = []  # (queued, ligands in flight) sampled every 100 ms
+    next_sample = 0.0
     with Clocks(0) as clk:
         t0 = time.perf_counter()
         while len(lat) < n:
@@ -304,6 +306,10 @@ def run_serve(args):
             while k < n and arrivals[k] <= now:
                 eng.serve_submit(k % len(SERVE_RECEPTORS), models[k], jobs[k], p)
                 k += 1
+            if now >= next_sample:
+                st = eng.serve_stats()
+                occupancy.append((st["queued"], st["inflight"]))
+                next_sample = now + 0.1
             wait = 1 if k < n else 20
             for (t, st, cnt, ms, ev, cs, nh) in eng.serve_poll(256, wait_ms=wait):
                 if st != 0:
@@ -321,6 +327,9 @@ def run_serve(args):
         "latency_ms": {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
                        "max": float(v.max()), "mean": float(v.mean())},
         "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
+        "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),
+                             "max": int(max(o[1] for o in occupancy))},
+        "queued": {"mean": float(np.mean([o[0] for o in occupancy])), "max": int(max(o[0] for o in occupancy))},
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{n} requests, ligands heavy U[10,60] rotors U[0,15], receptors "
                                f"{[r[0] for r in SERVE_RECEPTORS]} heavy atoms in {[r[1] for r in SERVE_RECEPTORS]} A "

@@ -527,7 +527,8 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
             __threadfence();  // this chain's results, before its count
             if (atomicAdd(ch.done_count, 1u) + 1 == (unsigned)ch.lig_chains) {
                 __threadfence_system();
-                *ch.host_flag = 1u;
+                *reinterpret_cast<volatile unsigned*>(ch.host_flag) = 1u;
+                __threadfence_system();
             }
         }
     }

@@ -677,11 +677,11 @@ static void worker(Server* sp) {
             fail_all(s, SG_ERR_ARG, x.what());
         }
         if (s.stopping && s.queue.empty() && s.inflight.empty() && s.refining.empty()) break;
-        if (!busy) {
-            lk.unlock();
-            std::this_thread::sleep_for(std::chrono::microseconds(100));
-            lk.lock();
-        }
+        // let submit / poll in between passes, busy or not
+        lk.unlock();
+        if (busy) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(100));
+        lk.lock();
     }
 }
 
