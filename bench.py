@@ -197,7 +197,10 @@ def run_accuracy(args):
     r32 = e32.dock_batch(0, models, jobs, p, refine=True)
     t32 = time.perf_counter() - t0
     a32 = np.array([float(r["e"][0]) for r in r32])
-    d32, d64 = a32 - a64, b64 - a64
+    r32b = e32.dock_batch(0, models, jobs_for(models, list(range(len(models))), exh, args.seed + 7919, 0), p,
+                          refine=True)
+    b32 = np.array([float(r["e"][0]) for r in r32b])
+    d32, d64, d3232 = a32 - a64, b64 - a64, b32 - a32
     print(json.dumps({
         "accuracy": f"top-score agreement, {len(models)} ligands spread over the screen, full smina steps, "
                     f"exhaustiveness {exh}, merge + FP64 refine on both sides",
@@ -206,6 +209,9 @@ def run_accuracy(args):
                             "median_abs": float(np.median(np.abs(d32)))},
         "fp64_seed_to_seed": {"mean": float(d64.mean()), "sd": float(d64.std(ddof=1)),
                               "median_abs": float(np.median(np.abs(d64)))},
+        "fp32_seed_to_seed": {"mean": float(d3232.mean()), "sd": float(d3232.std(ddof=1)),
+                              "median_abs": float(np.median(np.abs(d3232)))},
+        "fp32_seed_b_minus_fp64": {"mean": float((b32 - a64).mean()), "sd": float((b32 - a64).std(ddof=1))},
         "best_energy_mean": {"fp32": float(a32.mean()), "fp64": float(a64.mean())},
         "wall_s": {"fp64_run": t_a, "fp64_run_2": t_b, "fp32_batched": t32},
         "ligands_per_s": {"fp64_plain": len(models) / t_a, "fp32_batched": len(models) / t32},
