@@ -657,7 +657,13 @@ size_t ws32_bytes(const DModel& hm) {
     return (size_t)ws32_layout(hm.natoms, hm.nframes, hm.conf_size, hm.dof).total;
 }
 
+// Raises the kernel's dynamic shared memory limit to `smem` (never lowers it,
+// so launches sized against an earlier, larger limit stay valid).
 static cudaError_t prep32(const void* fn, size_t smem) {
+    cudaFuncAttributes fa{};
+    cudaError_t rc = cudaFuncGetAttributes(&fa, fn);
+    if (rc != cudaSuccess) return rc;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= smem) return cudaSuccess;
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
