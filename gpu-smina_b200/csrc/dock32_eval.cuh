@@ -23,7 +23,7 @@ constexpr unsigned kFull32 = 0xffffffffu;
 #endif
 
 #ifndef SG_PAIR_CHUNKS
-#define SG_PAIR_CHUNKS 2  // pair chunks (of 32) whose table loads are in flight together
+#define SG_PAIR_CHUNKS 3  // pair chunks (of 32) whose table loads are in flight together
 #endif
 
 // Section timers (compile with -DSG_PROFILE): lane 0 of every warp adds
