@@ -372,6 +372,66 @@ namespace sg {
 
 // Validates one model descriptor on the host so that no device index can
 // leave its array, then appends its packed arrays.
+// Mixed-precision pair schedule: chunks of 32 slots in which no atom is
+// the first atom of two pairs and none is the second atom of two pairs, so
+// one warp adds a chunk's forces without atomics (first atoms, then second
+// atoms).  A pair may be stored either way round: swapping the atoms toggles
+// the charge-role bit.  Within each quarter of a chunk (the 8 lanes that one
+// 16-byte shared-memory access serves at a time) the first atoms are
+// distinct modulo 8 and so are the second atoms, so the per-atom float4
+// loads and stores of a quarter hit 8 different bank groups.  pair_tp[k]:
+// type-pair index | (1 << 30) when the pair's first type is the larger.
+// Returns false (no schedule) for models of more than 255 atoms.
+static bool pack_pair_chunks(const sg_model_desc& d, const std::vector<int>& pair_tp, std::vector<uint32_t>& out) {
+    const int N = d.num_atoms, P = d.num_pairs;
+    out.clear();
+    if (N > 255) return false;  // 8-bit atom indices (inflex atoms take part in pairs too)
+    struct Chunk {
+        std::vector<char> out_used, in_used;
+        uint8_t amod[4] = {}, bmod[4] = {};  // bank groups taken per quarter (bit masks)
+        uint32_t slot[32];
+        int fill[4] = {};
+    };
+    std::vector<Chunk> chunks;
+    for (int k = 0; k < P; k++) {
+        const int u = d.pairs[2 * k], v = d.pairs[2 * k + 1];
+        require(u >= 0 && v >= 0 && u < N && v < N && u != v, "model: pair atoms must be distinct atoms");
+        require((pair_tp[k] & 0x1ff) < (int)kSlotPairMask, "model: type pair index out of range");
+        const uint32_t base = ((uint32_t)(pair_tp[k] & 0x1ff) << 16) | ((pair_tp[k] >> 30) & 1 ? kSlotSwap : 0) |
+                              (k >= d.num_other_pairs ? kSlotIntra : 0);
+        bool placed = false;
+        for (size_t c = 0; c < chunks.size() && !placed; c++) {
+            Chunk& ch = chunks[c];
+            for (int o = 0; o < 2 && !placed; o++) {
+                const int a = o ? v : u, b = o ? u : v;
+                if (ch.out_used[a] || ch.in_used[b]) continue;
+                for (int q = 0; q < 4; q++) {
+                    if (ch.fill[q] == 8 || (ch.amod[q] >> (a & 7) & 1) || (ch.bmod[q] >> (b & 7) & 1)) continue;
+                    ch.out_used[a] = ch.in_used[b] = 1;
+                    ch.amod[q] |= 1 << (a & 7);
+                    ch.bmod[q] |= 1 << (b & 7);
+                    ch.slot[8 * q + ch.fill[q]++] = (o ? base ^ kSlotSwap : base) | a | (b << 8);
+                    placed = true;
+                    break;
+                }
+            }
+        }
+        if (!placed) {
+            chunks.emplace_back();
+            Chunk& ch = chunks.back();
+            ch.out_used.assign(N, 0);
+            ch.in_used.assign(N, 0);
+            for (uint32_t& x : ch.slot) x = kSlotEmpty;
+            ch.out_used[u] = ch.in_used[v] = 1;
+            ch.amod[0] = 1 << (u & 7);
+            ch.bmod[0] = 1 << (v & 7);
+            ch.slot[ch.fill[0]++] = base | u | (v << 8);
+        }
+    }
+    for (const Chunk& ch : chunks) out.insert(out.end(), ch.slot, ch.slot + 32);
+    return true;
+}
+
 static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<double>& D, std::vector<float>& Fl,
                      std::vector<size_t>& ioff, std::vector<size_t>& doff, std::vector<size_t>& foff, DModel& hm) {
     const int N = d.num_atoms, M = d.num_movable, F = d.num_frames, P = d.num_pairs;
@@ -530,62 +590,11 @@ static void pack_one(const sg_model_desc& d, std::vector<int>& I, std::vector<do
                         "model: a subtree's atoms must follow its root frame's atoms contiguously");
         pv(sub_end);
     }
-    {   // Mixed-precision pair schedule: chunks of 32 slots in which no atom is
-        // the first atom of two pairs and none is the second atom of two pairs,
-        // so one warp adds a chunk's forces without atomics (first atoms, then
-        // second atoms).  A pair may be stored either way round: swapping the
-        // atoms toggles the charge-role bit.  Within each quarter of a chunk
-        // (the 8 lanes that one 16-byte shared-memory access serves at a time)
-        // the first atoms are distinct modulo 8 and so are the second atoms,
-        // so the per-atom float4 loads and stores of a quarter hit 8 different
-        // bank groups.
-        struct Chunk {
-            std::vector<char> out_used, in_used;
-            uint8_t amod[4] = {}, bmod[4] = {};  // bank groups taken per quarter (bit masks)
-            uint32_t slot[32];
-            int fill[4] = {};
-        };
-        std::vector<Chunk> chunks;
-        const bool packable = N <= 255;  // 8-bit atom indices (inflex atoms take part in pairs too)
-        for (int k = 0; k < P && packable; k++) {
-            const int u = d.pairs[2 * k], v = d.pairs[2 * k + 1];
-            require(u >= 0 && v >= 0 && u < N && v < N && u != v, "model: pair atoms must be distinct atoms");
-            require((pair_tp[k] & 0x1ff) < (int)kSlotPairMask, "model: type pair index out of range");
-            const uint32_t base = ((uint32_t)(pair_tp[k] & 0x1ff) << 16) | ((pair_tp[k] >> 30) & 1 ? kSlotSwap : 0) |
-                                  (k >= d.num_other_pairs ? kSlotIntra : 0);
-            bool placed = false;
-            for (size_t c = 0; c < chunks.size() && !placed; c++) {
-                Chunk& ch = chunks[c];
-                for (int o = 0; o < 2 && !placed; o++) {
-                    const int a = o ? v : u, b = o ? u : v;
-                    if (ch.out_used[a] || ch.in_used[b]) continue;
-                    for (int q = 0; q < 4; q++) {
-                        if (ch.fill[q] == 8 || (ch.amod[q] >> (a & 7) & 1) || (ch.bmod[q] >> (b & 7) & 1)) continue;
-                        ch.out_used[a] = ch.in_used[b] = 1;
-                        ch.amod[q] |= 1 << (a & 7);
-                        ch.bmod[q] |= 1 << (b & 7);
-                        ch.slot[8 * q + ch.fill[q]++] = (o ? base ^ kSlotSwap : base) | a | (b << 8);
-                        placed = true;
-                        break;
-                    }
-                }
-            }
-            if (!placed) {
-                chunks.emplace_back();
-                Chunk& ch = chunks.back();
-                ch.out_used.assign(N, 0);
-                ch.in_used.assign(N, 0);
-                for (uint32_t& x : ch.slot) x = kSlotEmpty;
-                ch.out_used[u] = ch.in_used[v] = 1;
-                ch.amod[0] = 1 << (u & 7);
-                ch.bmod[0] = 1 << (v & 7);
-                ch.slot[ch.fill[0]++] = base | u | (v << 8);
-            }
-        }
-        std::vector<int> ps;
-        for (const Chunk& ch : chunks)
-            for (int l = 0; l < 32; l++) ps.push_back((int)ch.slot[l]);
-        hm.npchunks = packable ? (int)chunks.size() : -1;
+    {   // mixed-precision pair schedule (pack_pair_chunks)
+        std::vector<uint32_t> slots;
+        const bool packable = pack_pair_chunks(d, pair_tp, slots);
+        std::vector<int> ps(slots.begin(), slots.end());
+        hm.npchunks = packable ? (int)(slots.size() / 32) : -1;
         pv(ps);
     }
     auto pf4 = [&](const double* xyz, const double* w4, size_t n) {
@@ -941,6 +950,29 @@ int sg_refine(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, c
         if (out_coords) dx.fetch(out_coords, e->stream);
         e->check_device_errors();
     });
+}
+
+int sg_pair_schedule(const sg_model_desc* m, uint32_t* out, int cap, int* nchunks) {
+    if (!m || !nchunks || cap < 0 || (cap > 0 && !out)) return SG_ERR_ARG;
+    try {
+        const int N = m->num_atoms, P = m->num_pairs;
+        if (N <= 0 || P < 0 || (P > 0 && (!m->pairs || !m->atom_type))) return SG_ERR_ARG;
+        std::vector<int> pair_tp(P);
+        for (int k = 0; k < P; k++) {
+            const int a = m->pairs[2 * k], b = m->pairs[2 * k + 1];
+            if (a < 0 || a >= N || b < 0 || b >= N || a == b) return SG_ERR_ARG;
+            const int ta = m->atom_type[a], tb = m->atom_type[b];
+            if (ta < 0 || tb < 0 || ta >= kNumTypes || tb >= kNumTypes) return SG_ERR_ARG;
+            pair_tp[k] = (ta <= tb ? tri_index(ta, tb) : tri_index(tb, ta)) | (ta > tb ? (1 << 30) : 0);
+        }
+        std::vector<uint32_t> slots;
+        if (!pack_pair_chunks(*m, pair_tp, slots)) return SG_ERR_ARG;
+        *nchunks = (int)(slots.size() / 32);
+        if ((size_t)cap >= slots.size()) std::copy(slots.begin(), slots.end(), out);
+        return SG_OK;
+    } catch (...) {
+        return SG_ERR_ARG;
+    }
 }
 
 int sg_score(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, const int* pose_model, int nposes,

@@ -143,6 +143,7 @@ def _declare(L):
                     C.c_int, _dp],
         "sg_score": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _ip, C.c_int, _dp, C.c_int, C.c_double * 3, C.c_double,
                      _dp, _dp, _dp, C.c_int],
+        "sg_pair_schedule": [C.POINTER(ModelDesc), _up, C.c_int, _ip],
         "sgh_model_conf_independent_inputs": [vp, _dp],
         "sgh_tables_conf_independent": [vp, _dp, C.c_double, _dp],
         "sgh_finish_docking": [vp, _dp, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_int, C.c_double, _ip, _dp,
@@ -241,6 +242,15 @@ class Model:
         p = MCParams()
         load().sgh_search_params(self._h, num_modes, C.byref(p))
         return p
+
+    def pair_schedule(self):
+        """The mixed-precision path's pair chunks (sg_pair_schedule): uint32 [nchunks][32]."""
+        n = C.c_int()
+        L = load()
+        _check_host(L.sg_pair_schedule(C.byref(self.desc), None, 0, C.byref(n)))
+        out = np.zeros(32 * n.value, dtype=np.uint32)
+        _check_host(L.sg_pair_schedule(C.byref(self.desc), uptr(out), len(out), C.byref(n)))
+        return out.reshape(n.value, 32)
 
     def conf_independent_inputs(self):
         """num_tors, num_rotors, num_heavy_atoms, num_hydrophobic_atoms,

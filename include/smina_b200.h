@@ -250,6 +250,16 @@ int sg_minimize(sg_engine* e, int receptor_id, const sg_model_desc* models, int 
                 int accurate_line, int early_term, double* out_e, double* out_coords,
                 int coord_stride);
 
+/* The mixed-precision path's pair schedule for one model, computed on the
+ * host (no device needed): chunks of 32 slots, slot = a | b << 8 |
+ * type pair << 16 | swap << 25 | intra << 26, empty slots with type pair
+ * 0x1ff.  Within a chunk no atom is twice a first (a) or twice a second (b)
+ * atom; within each 8-slot quarter the a's are distinct modulo 8 and so are
+ * the b's.  *nchunks gets the chunk count; out [cap] gets the slots when
+ * cap >= 32 * *nchunks.  No counterpart in the reference (its FP32 kernels
+ * gather pair forces per atom, gpu_flatten.cpp:217-235). */
+int sg_pair_schedule(const sg_model_desc* m, uint32_t* out, int cap, int* nchunks);
+
 /* Final rescoring of docked poses (finish_docking, src/main/main.cpp:257-282):
  * for every pose, model::eval on the direct receptor sum with the fast
  * table (model.cpp:938-967, non_cache::eval non_cache.cpp:34-91) into
