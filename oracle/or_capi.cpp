@@ -285,6 +285,30 @@ int or_score(or_ctx* o, const sg_model_desc* models, const int* pose_model, int 
     return 0;
 }
 
+/* quaternion and angle math (common.h:262-281, quaternion.cpp:42-139) on
+ * the rows of in[7] / q0[4]; the layout of out[22] is the reference probe's
+ * (oracle/ref_probe.cpp) */
+void or_quat_probe(const double* in, const double* q0, double* out, int n) {
+    for (int k = 0; k < n; k++) {
+        const double* x = in + 7 * k;
+        double* o = out + 22 * k;
+        const V3 axis(x[0], x[1], x[2]), rot(x[4], x[5], x[6]);
+        double ang = x[3];
+        normalize_angle(ang);
+        o[0] = ang;
+        const Q a = angle_to_quaternion(axis, x[3]);
+        const Q b = angle_to_quaternion(rot);
+        Q c{q0[4 * k], q0[4 * k + 1], q0[4 * k + 2], q0[4 * k + 3]};
+        const M3 m = quaternion_to_r3(c);
+        quaternion_increment(c, rot);
+        const Q qs[3] = {a, b, c};
+        for (int j = 0; j < 3; j++) {
+            o[1 + 4 * j] = qs[j].a; o[2 + 4 * j] = qs[j].b; o[3 + 4 * j] = qs[j].c; o[4 + 4 * j] = qs[j].d;
+        }
+        for (int j = 0; j < 9; j++) o[13 + j] = m.d[j];
+    }
+}
+
 /* scalar math probes: fn 0 sin, 1 cos, 2 acos, 3 exp */
 void or_pm_eval(int fn, const double* x, double* y, int n) {
     for (int i = 0; i < n; i++) {

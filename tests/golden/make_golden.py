@@ -1,7 +1,7 @@
 """Writes the golden vectors that pin the oracle's scalar math.
 
 Inputs are seeded; outputs come from the reference's own headers
-(src/lib/portable_math.h, src/gpu/gpu_rng.cuh) compiled by
+(src/lib/portable_math.h, src/gpu/gpu_rng.cuh, src/gpu/gpu_math.cuh) compiled by
 `make -C oracle ref` into oracle/_ref/libref_probe.so.  Run in a tree that
 has the reference mounted:  python tests/golden/make_golden.py
 """
@@ -58,6 +58,30 @@ def main():
                             "fl": hexs(fl), "int": it.tolist()})
     with open(os.path.join(HERE, "mt19937.json"), "w") as f:
         json.dump(mt, f)
+
+    # quaternion / angle math: axis-angle, rotation vectors (some below epsilon),
+    # angles over several turns, unit and slightly unnormalised quaternions
+    L.ref_quat_probe.argtypes = [dp, dp, dp, C.c_int]
+    n = 250
+    axis = rng.normal(size=(n, 3))
+    axis /= np.linalg.norm(axis, axis=1)[:, None]
+    angle = np.concatenate([rng.uniform(-np.pi, np.pi, 120), rng.uniform(-40, 40, 120),
+                            [np.pi, -np.pi, 3 * np.pi, -3 * np.pi, 0.0, 1e-12, 9.5, -9.5, 7 * np.pi, 2.5]])
+    rot = rng.normal(size=(n, 3)) * rng.choice([1e-18, 1e-3, 0.5, 2.0, 6.0], size=n)[:, None]
+    q0 = rng.normal(size=(n, 4))
+    q0 /= np.linalg.norm(q0, axis=1)[:, None]
+    q0[::7] *= 1 + rng.uniform(-1e-3, 1e-3, size=(len(q0[::7]), 1))
+    inp = np.ascontiguousarray(np.concatenate([axis, angle[:, None], rot], axis=1))
+    q0 = np.ascontiguousarray(q0)
+    res = np.zeros((n, 22))
+    L.ref_quat_probe(inp.ctypes.data_as(dp), q0.ctypes.data_as(dp), res.ctypes.data_as(dp), n)
+    quat = {"source": "reference src/gpu/gpu_math.cuh (FP64, host-compiled) via oracle/_ref/libref_probe.so",
+            "layout": "in[7] = axis xyz, angle, rotation xyz; out[22] = normalized_angle, angle_to_quaternion(axis, "
+                      "angle), angle_to_quaternion(rotation), quaternion_increment(q0, rotation), "
+                      "quaternion_to_r3(q0) column-major",
+            "in": hexs(inp.ravel()), "q0": hexs(q0.ravel()), "out": hexs(res.ravel())}
+    with open(os.path.join(HERE, "quaternion.json"), "w") as f:
+        json.dump(quat, f)
 
 
 if __name__ == "__main__":

@@ -56,6 +56,8 @@ def load():
             getattr(L, k).restype = C.c_int
         L.or_pm_eval.argtypes = [C.c_int, sb._dp, sb._dp, C.c_int]
         L.or_pm_eval.restype = None
+        L.or_quat_probe.argtypes = [sb._dp, sb._dp, sb._dp, C.c_int]
+        L.or_quat_probe.restype = None
         L.or_mt_probe.argtypes = [C.c_uint32, C.c_int, sb._up, C.c_double, C.c_double, sb._dp, C.c_int, C.c_int, sb._ip]
         L.or_mt_probe.restype = None
         _lib = L
@@ -209,3 +211,12 @@ def mt_probe(seed, n, a=-1.0, b=1.0, lo=0, hi=1000000):
     it = np.zeros(n, np.int32)
     load().or_mt_probe(seed, n, sb.uptr(raw), a, b, sb.dptr(fl), lo, hi, sb.iptr(it))
     return raw, fl, it
+
+
+def quat_probe(inp, q0):
+    """The oracle's quaternion / angle math on rows of in[7] and q0[4] (out[22])."""
+    inp = np.ascontiguousarray(inp, dtype=np.float64).reshape(-1, 7)
+    q0 = np.ascontiguousarray(q0, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((len(inp), 22))
+    load().or_quat_probe(sb.dptr(inp), sb.dptr(q0), sb.dptr(out), len(inp))
+    return out

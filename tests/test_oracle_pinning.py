@@ -1,9 +1,11 @@
 """Pins the CPU oracle against the reference.
 
-The oracle's fdlibm-method sin/cos/acos/exp and its mt19937 + Boost
-uniform_real/uniform_int must reproduce the reference's own implementations
-(src/lib/portable_math.h, src/gpu/gpu_rng.cuh) bit for bit; the golden
-vectors were produced from those headers by tests/golden/make_golden.py.
+The oracle's fdlibm-method sin/cos/acos/exp, its mt19937 + Boost
+uniform_real/uniform_int and its quaternion / angle math (normalize_angle,
+angle_to_quaternion, quaternion_increment, quaternion_to_r3) must reproduce
+the reference's own implementations (src/lib/portable_math.h,
+src/gpu/gpu_rng.cuh, src/gpu/gpu_math.cuh) bit for bit; the golden vectors
+were produced from those headers by tests/golden/make_golden.py.
 """
 import json
 import os
@@ -26,6 +28,13 @@ def test_portable_math_golden(name, fn):
     x, y = unhex(g["x"]), unhex(g["y"])
     got = OL.pm_eval(fn, x)
     assert np.array_equal(got.view(np.uint64), y.view(np.uint64))
+
+
+def test_quaternion_math_golden():
+    g = json.load(open(os.path.join(GOLD, "quaternion.json")))
+    inp, q0, want = unhex(g["in"]).reshape(-1, 7), unhex(g["q0"]).reshape(-1, 4), unhex(g["out"]).reshape(-1, 22)
+    got = OL.quat_probe(inp, q0)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
 
 
 def test_mt19937_known_answer():
