@@ -577,15 +577,15 @@ static void worker(Server* sp) {
     for (;;) {
         bool busy = false;
         try {
-            // 1. launch.  A launch holds one of at most kMaxStreams concurrent
+            // 1. launch.  At most max_inflight_ligands ligands are on the device;
+            // the rest wait here, so a launch never queues on the GPU behind
+            // resident work.  A launch holds one of at most kMaxStreams concurrent
             // kernels until its last ligand is done, so the launches still
-            // possible must carry the ligands the device can still take
-            // (max_inflight_ligands): a launch goes out once that share has
-            // queued, or when the oldest request has waited max_wait_ms
-            // scaled by how scarce launches have become.  Beyond
-            // max_inflight_ligands requests gather up to max_batch_ligands.
-            // Same search parameters per launch; device memory held for
-            // requests in flight stays under the budget.
+            // possible must carry the ligands the device can still take: a launch
+            // goes out once that share has queued, or when the oldest request has
+            // waited max_wait_ms scaled by how scarce launches have become.  Same
+            // search parameters per launch; device memory held for requests in
+            // flight stays under the budget.
             const int in_use = (int)(s.streams.size() - s.free_streams.size());
             if (!s.queue.empty() && in_use < Server::kMaxStreams) {
                 const double waited =
@@ -594,12 +594,11 @@ static void worker(Server* sp) {
                 const int open = std::max(0, s.o.max_inflight_ligands - s.inflight_ligs);
                 const int share = std::max(1, (open + slots - 1) / slots);
                 const double gather_ms = s.o.max_wait_ms * (double)Server::kMaxStreams / slots;
-                const bool go = open > 0 ? ((int)s.queue.size() >= share || waited >= gather_ms)
-                                         : ((int)s.queue.size() >= s.o.max_batch_ligands || waited >= gather_ms);
-                if (go || s.stopping) {
+                const bool go = open > 0 && ((int)s.queue.size() >= share || waited >= gather_ms || s.stopping);
+                if (go) {
                     std::vector<ServeReq> take;
                     size_t bytes = 0;
-                    const int cap = std::min(s.o.max_batch_ligands, (int)s.free_flags.size());
+                    const int cap = std::min({s.o.max_batch_ligands, (int)s.free_flags.size(), open});
                     while (!s.queue.empty() && (int)take.size() < cap) {
                         ServeReq& r = s.queue.front();
                         if (!take.empty() && !same_params(r.p, take[0].p)) break;

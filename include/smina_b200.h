@@ -377,10 +377,11 @@ typedef struct sg_serve_opts {
                                    others to share its launch, scaled up as
                                    the concurrent launches (at most 112) run
                                    out (0: 20 ms)                            */
-    int max_inflight_ligands;   /* ligands on the device before requests
-                                   start to gather (0: two per SM, what the
-                                   device holds at once with 8 chains per
-                                   ligand, less 16 kept for refinements)     */
+    int max_inflight_ligands;   /* at most this many ligands on the device;
+                                   later requests wait in the server's queue
+                                   (0: two per SM, what the device holds at
+                                   once with 8 chains per ligand, less 16
+                                   kept for refinements)                     */
 } sg_serve_opts;
 
 typedef struct sg_serve_done {
