@@ -570,6 +570,14 @@ static void fail_all(Server& s, int code, const std::string& why) {
     s.cv_done.notify_all();
 }
 
+// true once the event has completed; throws on a device error
+static bool event_done(cudaEvent_t ev) {
+    const cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaErrorNotReady) return false;
+    cuda_check(q, "serve: event");
+    return true;
+}
+
 static void worker(Server* sp) {
     Server& s = *sp;
     cudaSetDevice(s.e->device);
@@ -632,7 +640,7 @@ static void worker(Server* sp) {
             // refinements that finished: publish their ligands
             for (size_t i = 0; i < s.refining.size();) {
                 RefineGroup& g = *s.refining[i];
-                if (!g.ev || cudaEventQuery(g.ev) == cudaSuccess) {
+                if (!g.ev || event_done(g.ev)) {
                     for (size_t k = 0; k < g.ligs.size(); k++) {
                         publish(s, g, k);
                         g.ligs[k]->batch->published++;
@@ -650,7 +658,7 @@ static void worker(Server* sp) {
             for (size_t i = 0; i < s.inflight.size();) {
                 SvBatch& b = *s.inflight[i];
                 if (b.flagged == (int)b.ligs.size() && b.published == (int)b.ligs.size() &&
-                    cudaEventQuery(b.kdone) == cudaSuccess) {
+                    event_done(b.kdone)) {
                     cuda_check(cudaFreeAsync(b.dmem, b.stream), "serve: free batch");
                     cudaEventDestroy(b.kdone);
                     s.free_streams.push_back(b.stream);
@@ -669,6 +677,12 @@ static void worker(Server* sp) {
                 if (herr != kDevOk)
                     throw EngineError(herr == kDevOverlap ? SG_ERR_OVERLAP : SG_ERR_ARG,
                                       "serve: device reported error " + std::to_string(herr));
+                // a launch that failed on the device never raises its flags: the
+                // first batch's stream reports the error instead
+                if (!s.inflight.empty()) {
+                    const cudaError_t q = cudaStreamQuery(s.inflight.front()->stream);
+                    if (q != cudaSuccess && q != cudaErrorNotReady) cuda_check(q, "serve: search kernel");
+                }
             }
         } catch (EngineError& x) {
             fail_all(s, x.code, x.what());
