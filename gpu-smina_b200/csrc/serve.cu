@@ -358,57 +358,6 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     s.inflight.push_back(std::move(b));
 }
 
-// A ligand's chains are done: copy their containers back and merge them.
-static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
-    const DModel& h = b.img.host[L.model];
-    const int S = b.S, cs = h.conf_size, H = h.nheavy;
-    const size_t nc = L.nchains;
-    std::vector<double> he(nc * S), hconf((size_t)nc * S * cs);
-    std::vector<float> hxyz((size_t)nc * S * H * 3);
-    std::vector<int> horder(nc * S), hcount(nc);
-    std::vector<unsigned long long> hev(nc);
-    cudaStream_t cp = s.copy_stream;
-    auto get = [&](void* dst, size_t from, size_t bytes) {
-        if (bytes) cuda_check(cudaMemcpyAsync(dst, b.dmem + from, bytes, cudaMemcpyDeviceToHost, cp), "serve: fetch");
-    };
-    get(he.data(), b.e_at + (size_t)L.first * S * sizeof(double), he.size() * sizeof(double));
-    get(hconf.data(), b.conf_at + L.conf_off * sizeof(double), hconf.size() * sizeof(double));
-    get(hxyz.data(), b.xyz_at + L.xyz_off * sizeof(float), hxyz.size() * sizeof(float));
-    get(horder.data(), b.order_at + (size_t)L.first * S * sizeof(int), horder.size() * sizeof(int));
-    get(hcount.data(), b.count_at + (size_t)L.first * sizeof(int), hcount.size() * sizeof(int));
-    get(hev.data(), b.evals_at + (size_t)L.first * sizeof(unsigned long long), hev.size() * sizeof(unsigned long long));
-    cuda_check(cudaStreamSynchronize(cp), "serve: fetch");
-    for (size_t k = 0; k < nc; k++) {
-        L.evals += hev[k];
-        const int cnt = std::min(std::max(hcount[k], 0), S);
-        for (int i = 0; i < cnt; i++) {
-            const int slot = horder[k * S + i];
-            if (slot < 0 || slot >= S) continue;
-            SvPose t;
-            t.e = he[k * S + slot];
-            const double* c = &hconf[(k * S + slot) * cs];
-            t.conf.assign(c, c + cs);
-            const float* x = &hxyz[(k * S + slot) * H * 3];
-            t.xyz.assign(x, x + (size_t)H * 3);
-            sv_add_pose(L.poses, std::move(t), 2.0, S);
-        }
-    }
-}
-
-// One FP64 refinement launch for the merged poses of every ligand that
-// finished since the last one (ligands of any batch and receptor).
-struct RefineGroup {
-    std::vector<SvLig*> ligs;
-    std::vector<int> first;  // first pose of each ligand
-    std::vector<double> conf;  // the merged poses' confs, built on the host
-    int cs = 0, hs = 1;
-    void* dbuf = nullptr;
-    cudaEvent_t ev = nullptr;
-    char* pin = nullptr;  // pinned copy of the device buffer's layout
-    size_t pin_cap = 0;
-    const double *out_conf = nullptr, *out_e = nullptr, *out_xyz = nullptr;  // results, in pin
-};
-
 static char* pin_get(Server& s, size_t bytes, size_t& cap) {
     for (size_t i = 0; i < s.pin_free.size(); i++)
         if (s.pin_free[i].first >= bytes) {
@@ -426,6 +375,72 @@ static char* pin_get(Server& s, size_t bytes, size_t& cap) {
 static void pin_put(Server& s, char* p, size_t cap) {
     if (p) s.pin_free.emplace_back(cap, p);
 }
+
+// A ligand's chains are done: copy their containers back and merge them.
+static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
+    const DModel& h = b.img.host[L.model];
+    const int S = b.S, cs = h.conf_size, H = h.nheavy;
+    const size_t nc = L.nchains;
+    // one pinned staging buffer for the ligand's chain results
+    auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t eb = nc * S * sizeof(double), cb = (size_t)nc * S * cs * sizeof(double),
+                 xb = (size_t)nc * S * H * 3 * sizeof(float), ob = nc * S * sizeof(int), nb = nc * sizeof(int),
+                 vb = nc * sizeof(unsigned long long);
+    const size_t c_at = r16(eb), x_at = c_at + r16(cb), o_at = x_at + r16(xb), n_at = o_at + r16(ob),
+                 v_at = n_at + r16(nb), total = v_at + r16(vb);
+    size_t cap = 0;
+    char* hb = pin_get(s, total, cap);
+    const double* he = reinterpret_cast<const double*>(hb);
+    const double* hconf = reinterpret_cast<const double*>(hb + c_at);
+    const float* hxyz = reinterpret_cast<const float*>(hb + x_at);
+    const int* horder = reinterpret_cast<const int*>(hb + o_at);
+    const int* hcount = reinterpret_cast<const int*>(hb + n_at);
+    const unsigned long long* hev = reinterpret_cast<const unsigned long long*>(hb + v_at);
+    cudaStream_t cp = s.copy_stream;
+    auto get = [&](size_t to, size_t from, size_t bytes) {
+        if (bytes)
+            cuda_check(cudaMemcpyAsync(hb + to, b.dmem + from, bytes, cudaMemcpyDeviceToHost, cp), "serve: fetch");
+    };
+    get(0, b.e_at + (size_t)L.first * S * sizeof(double), eb);
+    get(c_at, b.conf_at + L.conf_off * sizeof(double), cb);
+    get(x_at, b.xyz_at + L.xyz_off * sizeof(float), xb);
+    get(o_at, b.order_at + (size_t)L.first * S * sizeof(int), ob);
+    get(n_at, b.count_at + (size_t)L.first * sizeof(int), nb);
+    get(v_at, b.evals_at + (size_t)L.first * sizeof(unsigned long long), vb);
+    const cudaError_t rc = cudaStreamSynchronize(cp);
+    if (rc != cudaSuccess) pin_put(s, hb, cap);
+    cuda_check(rc, "serve: fetch");
+    for (size_t k = 0; k < nc; k++) {
+        L.evals += hev[k];
+        const int cnt = std::min(std::max(hcount[k], 0), S);
+        for (int i = 0; i < cnt; i++) {
+            const int slot = horder[k * S + i];
+            if (slot < 0 || slot >= S) continue;
+            SvPose t;
+            t.e = he[k * S + slot];
+            const double* c = &hconf[(k * S + slot) * cs];
+            t.conf.assign(c, c + cs);
+            const float* x = &hxyz[(k * S + slot) * H * 3];
+            t.xyz.assign(x, x + (size_t)H * 3);
+            sv_add_pose(L.poses, std::move(t), 2.0, S);
+        }
+    }
+    pin_put(s, hb, cap);
+}
+
+// One FP64 refinement launch for the merged poses of every ligand that
+// finished since the last one (ligands of any batch and receptor).
+struct RefineGroup {
+    std::vector<SvLig*> ligs;
+    std::vector<int> first;  // first pose of each ligand
+    std::vector<double> conf;  // the merged poses' confs, built on the host
+    int cs = 0, hs = 1;
+    void* dbuf = nullptr;
+    cudaEvent_t ev = nullptr;
+    char* pin = nullptr;  // pinned copy of the device buffer's layout
+    size_t pin_cap = 0;
+    const double *out_conf = nullptr, *out_e = nullptr, *out_xyz = nullptr;  // results, in pin
+};
 
 static void launch_refines(Server& s, std::vector<std::pair<SvBatch*, SvLig*>>& fin) {
     sg_engine* e = s.e;
