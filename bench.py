@@ -388,15 +388,18 @@ def run_reference(args, world, rank):
     gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
     times = []
     for s in range(args.warmup + args.steps):
-        sub = [models[(s * parallel + i) % len(models)] for i in range(parallel)]
+        # ligands spread evenly over the screen, a different set each step
+        total = (args.warmup + args.steps) * parallel
+        stride = max(1, len(models) // total)
+        sub = [models[((s * parallel + i) * stride) % len(models)] for i in range(parallel)]
         v, dt, _ = cpu_sample(sub, gd, R, T, args.exhaustiveness, args.seed, len(sub), args.exhaustiveness, parallel)
         if s >= args.warmup:
             times.append((len(sub), dt))
     n = sum(a for a, _ in times)
     t = sum(b for _, b in times)
     value = n / t
-    sample = (f"{n} ligands of the screen ({parallel} at a time, {args.exhaustiveness} chains each at smina's full "
-              f"step count, merge + refine)")
+    sample = (f"{n} ligands spread over the screen ({parallel} at a time, {args.exhaustiveness} chains each at "
+              f"smina's full step count, merge + refine)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
