@@ -234,6 +234,7 @@ def run_plain64(args):
     eng.set_receptor(0, R, gd)
     eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
     p = make_params(models)
+    p.visited = 1 if args.visited else 0
     exh = args.exhaustiveness
     cmax = max(m.conf_size for m in models)
     confs, mts, moc, steps, its = [], [], [], [], []
@@ -252,18 +253,21 @@ def run_plain64(args):
         t0 = time.perf_counter()
         b = eng.dock(0, models, moc, confs, mts, p, steps=steps, maxiters=its)
         t_dock = time.perf_counter() - t0
+        best = []
         for k, m in enumerate(models):
             sp = m.search_params(9)
             e, conf, _ = sb.merge_chains(b, m, first=exh * k, n=exh, max_size=p.num_saved_mins)
-            eng.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v), maxiters=sp.maxiters,
-                       accurate_line=p.accurate_line, early_term=p.early_term)
+            _, er, _ = eng.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v),
+                                  maxiters=sp.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
+            best.append(float(np.min(er)) if len(er) else float("nan"))
         wall = time.perf_counter() - t0
     clocks = clk.summary()
     evals = int(np.sum(b.evals))
     print(json.dumps({
         "mode": "plain64", "metric": "ligands docked/sec, plain FP64 path", "value": len(models) / wall,
         "unit": UNIT, "n_gpus": 1, "dtype": "f64", "data": "synthetic", "wall_s": wall, "search_wall_s": t_dock,
-        "evals_per_s": evals / t_dock,
+        "evals_per_s": evals / t_dock, "evals": evals, "visited": bool(args.visited),
+        "best_energy_mean": float(np.mean(best)),
         "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), receptor "
                                f"3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness {exh}, smina step counts"
                                + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
@@ -438,6 +442,8 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
     ap.add_argument("--plain64", action="store_true",
                     help="instead of the batched search: the same screen through the plain FP64 path")
+    ap.add_argument("--visited", action="store_true",
+                    help="with --plain64: QuickVina 2's history check (not smina's search)")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
     if args.accuracy:

@@ -220,7 +220,95 @@ __device__ void bfgs_update64(W64& w, double* h, const double* p, const double* 
     __syncwarp();
 }
 
-__device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int early, const EvalMode& em) {
+// ---- QuickVina 2 history (not smina's search) ----------------------------------------------
+// Follows the reference's restatement of QuickVina 2 (gpu_mc.cuh:144-264;
+// Alhossary et al., Bioinformatics 2015): each chain keeps the last 5n points
+// its local optimisations visited.  A local optimisation runs only if one of
+// the 4n history points nearest its start passes the first-order consistency
+// check; until the history is full every start passes.
+__device__ inline Vis64 vis64_view(double* d, uint32_t* u, int n) {
+    Vis64 v;
+    v.x = d;
+    v.f = v.x + (size_t)5 * n * n;
+    v.now = v.f + 5 * n;
+    v.dist = v.now + n;
+    v.bits = u;
+    v.state = reinterpret_cast<int*>(u + 20 * n);
+    return v;
+}
+__device__ inline bool vis_bit(const uint32_t* b, int i) { return ((i < 32 ? b[0] >> i : b[1] >> (i - 32)) & 1u) != 0; }
+
+// visited::add (gpu_mc.cuh:163-205)
+__device__ void vis64_add(W64& w, const Vis64& V, const double* x, double f, const double* g) {
+    const DModel& m = *w.m;
+    const int n = m.dof, cap = 5 * n;
+    int slot = 0;
+    if (w.lane == 0) {
+        int* st = V.state;  // size, next slot, full
+        if (!st[2]) {
+            slot = st[0]++;
+            if (st[0] >= cap) { st[2] = 1; st[1] = 0; }
+        } else {
+            slot = st[1];
+            st[1] = (st[1] + 1) % cap;
+        }
+        V.f[slot] = f;
+        uint32_t zero[2] = {0, 0}, pos[2] = {0, 0};
+        for (int i = 0; i < n; i++)
+            if (g[i] == 0) zero[i >> 5] |= 1u << (i & 31);
+            else if (g[i] > 0) pos[i >> 5] |= 1u << (i & 31);
+        uint32_t* b = V.bits + 4 * slot;
+        b[0] = zero[0]; b[1] = zero[1]; b[2] = pos[0]; b[3] = pos[1];
+    }
+    slot = __shfl_sync(kFull, slot, 0);
+    for (int i = w.lane; i < n; i += 32) V.x[(size_t)slot * n + i] = conf_value64(m, x, i);
+    __syncwarp();
+}
+
+// visited::interesting (gpu_mc.cuh:207-264): the nearest history point that
+// passes the check (lowest index on ties) must rank below 4n by distance
+__device__ bool vis64_interesting(W64& w, const Vis64& V, const double* x, double f, const double* g) {
+    const DModel& m = *w.m;
+    const int n = m.dof, cap = 5 * n;
+    const int full = __shfl_sync(kFull, w.lane == 0 ? V.state[2] : 0, 0);
+    if (!full) return true;
+    for (int i = w.lane; i < n; i += 32) V.now[i] = conf_value64(m, x, i);
+    __syncwarp();
+    double best = kMaxFl;
+    int besti = cap;
+    for (int e = w.lane; e < cap; e += 32) {
+        const double* xe = V.x + (size_t)e * n;
+        const uint32_t* b = V.bits + 4 * e;
+        const bool newY = f - V.f[e] > 0;
+        double d2 = 0;
+        bool pass = true;
+        for (int i = 0; i < n; i++) {
+            const double dx = xe[i] - V.now[i];
+            d2 += dx * dx;
+            if (vis_bit(b, i) || g[i] == 0) continue;
+            const bool nowPos = g[i] > 0;
+            if (nowPos != vis_bit(b + 2, i)) continue;
+            const bool newX = V.now[i] - xe[i] > 0;
+            if (nowPos ^ newX ^ newY) pass = false;
+        }
+        V.dist[e] = d2;
+        if (pass && d2 < best) { best = d2; besti = e; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {  // argmin of (best, index)
+        const double ob = __shfl_xor_sync(kFull, best, o);
+        const int oi = __shfl_xor_sync(kFull, besti, o);
+        if (ob < best || (ob == best && oi < besti)) { best = ob; besti = oi; }
+    }
+    if (besti >= cap) return false;
+    __syncwarp();
+    int ahead = 0;
+    for (int e = w.lane; e < cap; e += 32) ahead += (V.dist[e] < best || (V.dist[e] == best && e < besti));
+    for (int o = 16; o > 0; o >>= 1) ahead += __shfl_xor_sync(kFull, ahead, o);
+    return ahead < 4 * n;
+}
+
+__device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int early, const EvalMode& em,
+                         const Vis64* vis = nullptr) {
     const DModel& m = *w.m;
     const int n = m.dof;
     double* S = w.s;
@@ -232,6 +320,10 @@ __device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int earl
     for (int i = w.lane; i < n; i += 32) h[i + i * (i + 1) / 2] = 1;
     __syncwarp();
     double f0 = feval(w, x, g, em);
+    if (vis) {
+        if (!vis64_interesting(w, *vis, x, f0, g)) return f0;
+        vis64_add(w, *vis, x, f0, g);
+    }
     const double f_orig = f0;
     vcopy(w, g_orig, g, n);
     vcopy(w, x_orig, x, m.conf_size);
@@ -259,6 +351,7 @@ __device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int earl
             }
         }
         bfgs_update64(w, h, p, y, alpha, n);
+        if (vis) vis64_add(w, *vis, x, f0, g);
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;

@@ -125,7 +125,7 @@ cudaError_t launch_eval64(const DModel*, size_t, const DTables&, const DReceptor
 cudaError_t launch_bfgs64(const DModel*, size_t, const DTables&, const DReceptor*, int, double*, const double[3], double,
                           int, int, int, double*, int*, cudaStream_t);
 cudaError_t launch_mc64(const DModel*, size_t, const DTables&, const DReceptor*, const Chain64*, int,
-                        const MCParams64&, int*, cudaStream_t);
+                        const MCParams64&, bool visited, int*, cudaStream_t);
 cudaError_t launch_score64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const int* pose_model,
                            int n, const double* confs, int conf_stride, const double v[3], double slope, double* e,
                            double* intra, double* coords, int coord_stride, int* err, cudaStream_t s);

@@ -70,6 +70,9 @@ __global__ void __launch_bounds__(32) k_bfgs64(const DModel* model, DTables T, c
 }
 
 // monte_carlo::operator() for one chain per block
+// VIS: chains may carry a QuickVina 2 history (a separate instantiation, so
+// smina's own search compiles exactly as without it)
+template <bool VIS>
 __global__ void __launch_bounds__(32) k_mc64(const DModel* models, DTables T, const DReceptor* R,
                                              const Chain64* chains, int nchains, MCParams64 P, int* err) {
     const int c = blockIdx.x;
@@ -87,18 +90,24 @@ __global__ void __launch_bounds__(32) k_mc64(const DModel* models, DTables T, co
     __syncwarp();
     const EvalMode hunt{{P.hunt[0], P.hunt[1], P.hunt[2]}, P.slope, false};
     const EvalMode auth{{P.auth[0], P.auth[1], P.auth[2]}, P.slope, false};
+    Vis64 vis_store{};
+    const Vis64* vis = nullptr;
+    if (VIS && ch.vis && m.dof <= kVisMaxN) {
+        vis_store = vis64_view(ch.vis, ch.vis_words, m.dof);
+        vis = &vis_store;
+    }
     double tmp_e = 0, best_e = kMaxFl;
     for (unsigned step = 0; step < ch.steps; step++) {
         vcopy(w, cand, tmp, m.conf_size);
         mutate64(w, cand, P.amplitude);
-        const double cand_e = bfgs64(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt);
+        const double cand_e = bfgs64(w, cand, ch.maxiters, P.accurate_line, P.early_term, hunt, vis);
         if (step == 0 || metropolis64(w, tmp_e, cand_e, P.temperature)) {
             vcopy(w, tmp, cand, m.conf_size);
             tmp_e = cand_e;
             set_conf64(w, tmp);
             const int count = *ch.out_count;
             if (tmp_e < best_e || count < P.num_saved) {
-                tmp_e = bfgs64(w, tmp, ch.maxiters, P.accurate_line, P.early_term, auth);
+                tmp_e = bfgs64(w, tmp, ch.maxiters, P.accurate_line, P.early_term, auth, vis);
                 set_conf64(w, tmp);
                 add_to_output64(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved);
                 if (tmp_e < best_e) best_e = tmp_e;
@@ -219,10 +228,12 @@ cudaError_t launch_bfgs64(const DModel* dm, size_t smem, const DTables& T, const
 }
 
 cudaError_t launch_mc64(const DModel* dms, size_t smem, const DTables& T, const DReceptor* R, const Chain64* chains,
-                        int n, const MCParams64& P, int* err, cudaStream_t s) {
-    cudaError_t rc = prep((const void*)k_mc64, smem);
+                        int n, const MCParams64& P, bool visited, int* err, cudaStream_t s) {
+    const void* fn = visited ? (const void*)k_mc64<true> : (const void*)k_mc64<false>;
+    cudaError_t rc = prep(fn, smem);
     if (rc != cudaSuccess) return rc;
-    k_mc64<<<n, 32, smem, s>>>(dms, T, R, chains, n, P, err);
+    if (visited) k_mc64<true><<<n, 32, smem, s>>>(dms, T, R, chains, n, P, err);
+    else k_mc64<false><<<n, 32, smem, s>>>(dms, T, R, chains, n, P, err);
     return cudaGetLastError();
 }
 

@@ -100,6 +100,7 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
                 "dock_batch32_noalloc needs an engine created with SG_PREC_FP32 or SG_PREC_FP32_H16");
         require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->maxiters >= 0 && p->temperature > 0,
                 "dock_batch32_noalloc: bad search parameters");
+        require(!p->visited, "the QuickVina 2 history (visited) runs on the plain path only");
         require(e->has_tables, "no tables set");
         RecState& r = receptor_for(e, rid);
         unsigned char* base = scratch_on(e->device);

@@ -795,6 +795,7 @@ int sg_serve_submit(sg_engine* e, int rid, const sg_model_desc* m, const sg_liga
         require(m && job && p && ticket, "serve: bad arguments");
         require(job->num_chains >= 1 && job->num_chains <= 4096 && job->maxiters >= 0, "serve: bad ligand job");
         require(p->num_saved_mins >= 1 && p->num_saved_mins <= 1024 && p->temperature > 0, "serve: bad search parameters");
+        require(!p->visited, "the QuickVina 2 history (visited) runs on the plain path only");
         require(m->num_atoms <= 255, "mixed-precision path: at most 255 atoms per model");
         RecState& r = receptor_for(e, rid);
         ServeReq q;

@@ -270,10 +270,28 @@ SG_HD Ws64 ws64_layout(int natoms, int nframes, int npairs, int conf, int dof) {
 }
 
 // Chain bookkeeping for the plain path (global memory)
+// A chain's QuickVina 2 history (plain path, MCParams::visited): 5n points
+// of n change coordinates, their energies, the zero and positive bits of their
+// gradients, and the ring state (size, next slot, full); scratch for the
+// point being checked and the distances.  n <= kVisMaxN.
+constexpr int kVisMaxN = 64;
+struct Vis64 {
+    double* x;        // [5n][n]
+    double* f;        // [5n]
+    double* now;      // [n]
+    double* dist;     // [5n]
+    uint32_t* bits;   // [5n][4]: zero bits (2 words), positive bits (2 words)
+    int* state;       // [3]
+};
+SG_HD size_t vis64_doubles(int n) { return (size_t)5 * n * n + 5 * n + n + 5 * n; }
+SG_HD size_t vis64_words(int n) { return (size_t)20 * n + 4; }
+
 struct Chain64 {
     int model;
     unsigned steps;
     int maxiters;
+    double* vis;         // history doubles (vis64_doubles(dof)), or null: no history
+    uint32_t* vis_words; // history words (vis64_words(dof), zeroed)
     const double* conf0;
     uint32_t* mt;        // [625] state (read + written)
     double* out_e;       // [num_saved]

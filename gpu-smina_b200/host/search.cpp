@@ -22,7 +22,7 @@ unsigned search_steps(const Model& m) {
 }
 
 sg_mc_params search_params(const Model& m, int num_modes) {
-    sg_mc_params p;
+    sg_mc_params p{};  // visited = 0: smina's search
     p.num_steps = search_steps(m);
     p.temperature = 1.2;
     p.mutation_amplitude = 2;

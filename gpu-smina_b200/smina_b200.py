@@ -61,7 +61,7 @@ class MCParams(C.Structure):
     _fields_ = [("num_steps", C.c_uint), ("temperature", C.c_double), ("mutation_amplitude", C.c_double),
                 ("min_rmsd", C.c_double), ("num_saved_mins", C.c_int), ("hunt_cap", C.c_double * 3),
                 ("authentic_v", C.c_double * 3), ("maxiters", C.c_int), ("accurate_line", C.c_int),
-                ("early_term", C.c_int), ("cache_slope", C.c_double)]
+                ("early_term", C.c_int), ("cache_slope", C.c_double), ("visited", C.c_int)]
 
 
 class ChainInput(C.Structure):

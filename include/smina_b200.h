@@ -154,6 +154,10 @@ typedef struct sg_mc_params {
     int accurate_line;          /* 1: accurate_line_search                */
     int early_term;             /* minimization_params::early_term        */
     double cache_slope;         /* grid out-of-box slope (1e6)            */
+    int visited;                /* 1: QuickVina 2's history check skips
+                                   local optimisations it deems redundant
+                                   (MCParams::visited, gpu_mc_structs.h:30-33;
+                                   not smina's search).  Plain path only.   */
 } sg_mc_params;
 
 /* One chain of the plain (FP64) path: its starting conf and the

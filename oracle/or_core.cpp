@@ -6,6 +6,7 @@
 #include "or_core.h"
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <stdexcept>
 
 namespace orc {
@@ -685,13 +686,79 @@ static double accurate_line_search(F& f, int n, const Model& m, const std::vecto
     }
 }
 
+// ---- QuickVina 2 history (the reference's gpu_mc.cuh:144-264; not smina's search) ----
+// A chain's last 5n visited points (n = dof) in change coordinates, their
+// energies and the zero / positive signs of their gradients.
+struct Visited {
+    int n = 0, size = 0, next = 0;
+    bool full = false;
+    std::vector<double> x, f;
+    std::vector<uint8_t> zero, pos;  // [5n][n]
+    explicit Visited(int n_) : n(n_), x(5 * (size_t)n_ * n_), f(5 * n_), zero(5 * (size_t)n_ * n_), pos(5 * (size_t)n_ * n_) {}
+};
+// visited::add (gpu_mc.cuh:163-205)
+static void visited_add(Visited& V, const Model& m, const double* x, double f, const double* g) {
+    const int n = V.n, cap = 5 * n;
+    int slot;
+    if (!V.full) {
+        slot = V.size++;
+        if (V.size >= cap) { V.full = true; V.next = 0; }
+    } else {
+        slot = V.next;
+        V.next = (V.next + 1) % cap;
+    }
+    V.f[slot] = f;
+    for (int i = 0; i < n; i++) {
+        V.zero[(size_t)slot * n + i] = g[i] == 0;
+        V.pos[(size_t)slot * n + i] = g[i] > 0;
+        V.x[(size_t)slot * n + i] = conf_value(m, x, i);
+    }
+}
+// visited::interesting (gpu_mc.cuh:207-264): until the history is full every
+// start is interesting; otherwise the nearest point passing the first-order
+// check (lowest index on ties) must rank below 4n by distance
+static bool visited_interesting(const Visited& V, const Model& m, const double* x, double f, const double* g) {
+    const int n = V.n, cap = 5 * n;
+    if (!V.full) return true;
+    std::vector<double> now(n), dist(cap);
+    for (int i = 0; i < n; i++) now[i] = conf_value(m, x, i);
+    double best = MAXF;
+    int besti = cap;
+    for (int e = 0; e < cap; e++) {
+        const double* xe = &V.x[(size_t)e * n];
+        const bool newY = f - V.f[e] > 0;
+        double d2 = 0;
+        bool pass = true;
+        for (int i = 0; i < n; i++) {
+            const double dx = xe[i] - now[i];
+            d2 += dx * dx;
+            if (V.zero[(size_t)e * n + i] || g[i] == 0) continue;
+            const bool nowPos = g[i] > 0;
+            if (nowPos != (V.pos[(size_t)e * n + i] != 0)) continue;
+            const bool newX = now[i] - xe[i] > 0;
+            if (nowPos ^ newX ^ newY) pass = false;
+        }
+        dist[e] = d2;
+        if (pass && d2 < best) { best = d2; besti = e; }
+    }
+    if (besti >= cap) return false;
+    int ahead = 0;
+    for (int e = 0; e < cap; e++) ahead += (dist[e] < best || (dist[e] == best && e < besti));
+    return ahead < 4 * n;
+}
+
 template <typename F>
-double bfgs(F& f, const Model& m, std::vector<double>& x, std::vector<double>& g, const MinParams& mp) {
+double bfgs(F& f, const Model& m, std::vector<double>& x, std::vector<double>& g, const MinParams& mp,
+            Visited* vis = nullptr) {
     const int n = m.dof;
     Tri h(n);
     for (int i = 0; i < n; i++) h.at(i, i) = 1;
     std::vector<double> g_new(g), x_new(x);
     double f0 = f(x.data(), g.data());
+    if (vis) {  // the reference's bfgs() with a history (gpu_mc.cuh:459-465)
+        if (!visited_interesting(*vis, m, x.data(), f0, g.data())) return f0;
+        visited_add(*vis, m, x.data(), f0, g.data());
+    }
     const double f_orig = f0;
     std::vector<double> g_orig(g), x_orig(x), p(g), y(n);
     for (unsigned step = 0; step < (unsigned)mp.maxiters; step++) {
@@ -722,6 +789,7 @@ double bfgs(F& f, const Model& m, std::vector<double>& x, std::vector<double>& g
             }
         }
         bfgs_update(h, p.data(), y.data(), alpha);
+        if (vis) visited_add(*vis, m, x.data(), f0, g.data());
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;
@@ -840,15 +908,17 @@ void mc_chain(const Ctx& c, const Model& m, const sg_mc_params& P, const double*
     tmp.e = 0;
     std::vector<double> g(m.dof, 0.0);
     double best_e = MAXF;
+    std::unique_ptr<Visited> vis;  // MCParams::visited: QuickVina 2's history (dof <= 64)
+    if (P.visited && m.dof <= 64) vis.reset(new Visited(m.dof));
     for (unsigned step = 0; step < steps; step++) {
         Out cand = tmp;
         mutate_conf(m, s, cand.c.data(), P.mutation_amplitude, gen);
-        cand.e = bfgs(hunt, m, cand.c, g, mp);
+        cand.e = bfgs(hunt, m, cand.c, g, mp, vis.get());
         if (step == 0 || metropolis_accept(tmp.e, cand.e, P.temperature, gen)) {
             tmp = cand;
             model_set(m, tmp.c.data(), s);
             if (tmp.e < best_e || (int)out.v.size() < P.num_saved_mins) {
-                tmp.e = bfgs(auth, m, tmp.c, g, mp);
+                tmp.e = bfgs(auth, m, tmp.c, g, mp, vis.get());
                 model_set(m, tmp.c.data(), s);
                 tmp.coords = heavy_coords(m, s);
                 add_to_output_container(out, tmp, P.min_rmsd, P.num_saved_mins);

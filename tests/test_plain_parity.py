@@ -179,3 +179,37 @@ def test_minimize_in_own_boxes_bit_exact(setup):
     c2, e2, _ = eng.minimize(0, models, pm, confs, maxiters=its)
     c3, e3, _ = orc.minimize(models, pm, confs, maxiters=its)
     assert_bitwise(e2, e3, "energies (receptor box)")
+
+
+@pytest.mark.parametrize("heavy,rotors,seed", [(24, 5, 11), (40, 10, 5)])
+def test_mc_chains_with_visited_history_bit_exact(setup, heavy, rotors, seed):
+    """MCParams::visited (QuickVina 2's history, the reference's
+    gpu_mc.cuh:144-264; not smina's search): chains skip local optimisations
+    the history deems redundant.  Bit-exact against the checker, and fewer
+    evaluations than the same chains without the history."""
+    eng, orc, gd = setup
+    m = W.ligand(heavy, rotors, seed)
+    p = m.search_params()
+    confs, mts = m.seed_chains(99, 4, gd)
+    plain = eng.dock(0, [m], [0] * 4, confs, mts, p, steps=80)
+    p.visited = 1
+    b1 = eng.dock(0, [m], [0] * 4, confs, mts, p, steps=80)
+    b0 = orc.dock([m], [0] * 4, confs, mts, p, steps=80, threads=4)
+    assert (b1.count == b0.count).all() and (b1.evals == b0.evals).all()
+    for k in range(4):
+        c = b0.count[k]
+        assert_bitwise(b1.e[k, :c], b0.e[k, :c], f"chain {k} energies")
+        assert_bitwise(b1.conf[k, :c, :m.conf_size], b0.conf[k, :c, :m.conf_size], f"chain {k} confs")
+    assert b1.evals.sum() < plain.evals.sum()
+
+
+def test_visited_history_is_refused_on_the_mixed_precision_path():
+    T, R, gd = W.tables(), W.receptor(), W.box()
+    eng = sb.Engine(0, sb.PREC_FP32)
+    eng.set_tables(T)
+    eng.set_receptor(0, R, gd)
+    m = W.ligand(12, 0, 3)
+    p = m.search_params()
+    p.visited = 1
+    with pytest.raises(sb.SminaError):
+        eng.dock_batch(0, [m], [sb.LigandJob(model=0, num_chains=2, num_steps=2, maxiters=0, seed=1, ligand_key=1)], p)
