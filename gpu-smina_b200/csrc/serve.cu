@@ -68,6 +68,7 @@ struct ServeReq {
     std::shared_ptr<ModelCopy> m;
     Clock::time_point t_submit;
     size_t bytes = 0;  // device memory its share of a batch needs
+    size_t stage = 0, ws = 0;  // its staged-model and per-chain workspace bytes in shared memory
 };
 
 struct ServeDone {
@@ -175,6 +176,17 @@ static bool same_params(const sg_mc_params& a, const sg_mc_params& b) {
            a.num_saved_mins == b.num_saved_mins && a.accurate_line == b.accurate_line && a.early_term == b.early_term &&
            a.cache_slope == b.cache_slope && std::equal(a.hunt_cap, a.hunt_cap + 3, b.hunt_cap) &&
            std::equal(a.authentic_v, a.authentic_v + 3, b.authentic_v);
+}
+
+// Chains per block a launch can run with the server's fixed shared memory,
+// given its largest staged model and workspace (0: none fits).
+static int serve_shape(const Server& s, size_t stage, size_t ws, int max_chains) {
+    for (int c : {8, 4, 2, 1}) {
+        if (s.e->force_wpb && c != s.e->force_wpb) continue;
+        if (!s.e->force_wpb && c > 1 && c / 2 >= max_chains) continue;
+        if (stage + (size_t)c * ws <= s.smem_block) return c;
+    }
+    return 0;
 }
 
 // Launches one batch; called by the worker with mu held.
@@ -622,9 +634,21 @@ static void worker(Server* sp) {
                     std::vector<ServeReq> take;
                     size_t bytes = 0;
                     const int cap = std::min({s.o.max_batch_ligands, (int)s.free_flags.size(), open});
+                    size_t t_stage = 0, t_ws = 0;
+                    int t_chains = 1, t_shape = 0;
                     while (!s.queue.empty() && (int)take.size() < cap) {
                         ServeReq& r = s.queue.front();
                         if (!take.empty() && !same_params(r.p, take[0].p)) break;
+                        // ligands that would force fewer chains per block on the
+                        // launch wait for one of their own
+                        const size_t n_stage = std::max(t_stage, r.stage), n_ws = std::max(t_ws, r.ws);
+                        const int n_chains = std::max(t_chains, r.job.num_chains);
+                        const int shape = serve_shape(s, n_stage, n_ws, n_chains);
+                        if (!take.empty() && shape < t_shape) break;
+                        t_stage = n_stage;
+                        t_ws = n_ws;
+                        t_chains = n_chains;
+                        t_shape = shape;
                         if (s.inflight_bytes + bytes + r.bytes > s.o.hbm_budget_bytes &&
                             !(take.empty() && s.inflight.empty()))
                             break;
@@ -805,6 +829,16 @@ int sg_serve_submit(sg_engine* e, int rid, const sg_model_desc* m, const sg_liga
         q.job.model = 0;
         q.p = *p;
         q.bytes = req_bytes(*m, *job, p->num_saved_mins);
+        {   // its staged model and workspace in shared memory (the launch shape it needs)
+            ModelImage probe;
+            pack_models_image(m, 1, reinterpret_cast<char*>(uintptr_t(1) << 20), probe);  // never dereferenced
+            const DModel& h = probe.host[0];
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 atoms per model");
+            q.ws = (ws32_bytes(h) + 15) & ~(size_t)15;
+            q.stage = (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
+            require(serve_shape(*s, q.stage, q.ws, job->num_chains) > 0,
+                    "serve: model too large for the mixed-precision path's shared memory");
+        }
         std::unique_lock<std::mutex> lk(s->mu);
         require(s->error == SG_OK, "serve: stopped after an error: " + s->error_text);
         require(!s->stopping, "serve: stopping");
