@@ -276,6 +276,85 @@ def run_plain64(args):
     }), flush=True)
 
 
+def heavy_rmsd(a, b):
+    """Heavy-atom RMSD of two poses of one model (same atom order, no
+    symmetry matching), as smina's rmsd_upper_bound (coords.cpp:25-33)."""
+    a, b = np.asarray(a, float).reshape(-1, 3), np.asarray(b, float).reshape(-1, 3)
+    return float(np.sqrt(((a - b) ** 2).sum(1).mean())) if len(a) else 0.0
+
+
+def run_redock(args):
+    """The single-ligand redock: a 24-heavy-atom, 5-rotor ligand against the
+    3,000-atom receptor (22 A box at 0.375 A, default scoring, smina's step
+    and BFGS-iteration counts).  Plain FP64 at exhaustiveness 8 and the
+    batched FP32 search at exhaustiveness 128, each repeated with
+    ``args.redock`` seeds; both merge with min_rmsd 2 and refine every
+    merged pose in FP64.  Reports, per seed, the FP32 top pose's energy
+    difference and heavy-atom RMSD against the FP64 top pose of the same
+    seed index, next to FP64's own seed-to-seed figures."""
+    reps = args.redock
+    m = sb.Model(sb.make_ligand_pdbqt(24, 5, args.seed, CENTER))
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    types = sorted({t for t in m.types() if 1 < t < 27})
+    e64 = sb.Engine(0, sb.PREC_FP64)
+    e64.set_tables(T)
+    e64.set_receptor(0, R, gd)
+    e64.build_grids(0, types)
+    e32 = sb.Engine(0, sb.PREC_FP32 if args.precision == "fp32" else sb.PREC_FP32_H16)
+    e32.set_tables(T)
+    e32.set_receptor(0, R, gd)
+    e32.build_grids(0, types)
+    p = m.search_params(9)
+    exh64, exh32 = 8, 128
+    seeds = [args.seed + 1009 * r for r in range(reps)]
+    confs, mts = [], []
+    for s in seeds:
+        c, mt = m.seed_chains(s, exh64, gd)
+        confs += list(c)
+        mts += list(mt)
+    t0 = time.perf_counter()
+    b = e64.dock(0, [m], [0] * (exh64 * reps), confs, mts, p)
+    top64 = []
+    for r in range(reps):
+        e, conf, _ = sb.merge_chains(b, m, first=exh64 * r, n=exh64, max_size=p.num_saved_mins)
+        _, er, xyz = e64.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v),
+                                maxiters=p.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
+        k = int(np.argmin(er))
+        top64.append((float(er[k]), xyz[k, :m.heavy]))
+    t64 = time.perf_counter() - t0
+    jobs = [sb.LigandJob(model=0, num_chains=exh32, num_steps=p.num_steps, maxiters=p.maxiters, seed=s,
+                         ligand_key=r) for r, s in enumerate(seeds)]
+    t0 = time.perf_counter()
+    r32 = e32.dock_batch(0, [m], jobs, p, refine=True)
+    t32 = time.perf_counter() - t0
+    top32 = []
+    for res in r32:
+        k = int(np.argmin(res["e"]))
+        top32.append((float(res["e"][k]), res["coords"][k]))
+    de = [top32[r][0] - top64[r][0] for r in range(reps)]
+    rmsd = [heavy_rmsd(top32[r][1], top64[r][1]) for r in range(reps)]
+    pairs = [(i, j) for i in range(reps) for j in range(i + 1, reps)]
+    de64 = [top64[j][0] - top64[i][0] for i, j in pairs]
+    rmsd64 = [heavy_rmsd(top64[i][1], top64[j][1]) for i, j in pairs]
+    print(json.dumps({
+        "mode": "redock",
+        "config": {"workload": f"single-ligand redock: ligand 24 heavy atoms, 5 rotors (seed {args.seed}); receptor "
+                               "3000 heavy atoms; 22 A box at 0.375 A; default scoring; smina step and iteration "
+                               f"counts ({p.num_steps} steps, {p.maxiters} BFGS iterations); FP64 plain at "
+                               f"exhaustiveness {exh64}, FP32 batched at exhaustiveness {exh32}; {reps} seeds; "
+                               "merge min_rmsd 2 + FP64 refine on both sides"},
+        "precision": args.precision,
+        "top_energy": {"fp64": [t[0] for t in top64], "fp32": [t[0] for t in top32]},
+        "fp32_minus_fp64_energy": de,
+        "fp32_vs_fp64_rmsd": rmsd,
+        "fp64_seed_to_seed_energy": de64,
+        "fp64_seed_to_seed_rmsd": rmsd64,
+        "wall_s": {"fp64_plain": t64, "fp32_batched": t32},
+    }), flush=True)
+
+
 SERVE_RECEPTORS = ((2000, 22.0), (3000, 26.0), (5000, 30.0))  # (heavy atoms, box edge in A)
 
 
@@ -444,10 +523,16 @@ def main():
                     help="instead of the batched search: the same screen through the plain FP64 path")
     ap.add_argument("--visited", action="store_true",
                     help="with --plain64: QuickVina 2's history check (not smina's search)")
+    ap.add_argument("--redock", type=int, default=0,
+                    help="instead of timing: the single-ligand redock (FP64 exhaustiveness 8, FP32 exhaustiveness "
+                         "128) with this many seeds; top-pose energy and RMSD differences")
     args = ap.parse_args()
     assert args.warmup >= 3, "at least 3 warm-up steps"
     if args.accuracy:
         run_accuracy(args)
+        return
+    if args.redock:
+        run_redock(args)
         return
     if args.serve:
         run_serve(args)
