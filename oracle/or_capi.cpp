@@ -211,13 +211,11 @@ int or_merge(const sg_chain_result* chains, int nchains, int conf_size, int nhea
 int or_refine(or_ctx* o, const sg_model_desc* models, const int* pose_model, int nposes, double* confs,
               const double cap[3], int maxiters, int accurate_line, int early_term, double* out_e,
               double* out_coords) {
-    const Model* cache_m = nullptr;
     Model m;
     try {
         for (int k = 0; k < nposes; k++) {
             const sg_model_desc& md = models[pose_model[k]];
             m.load(md);
-            (void)cache_m;
             std::vector<V3> hc;
             MinParams mp{maxiters, accurate_line, early_term};
             refine(o->c, m, confs + (size_t)k * m.conf_size, cap, mp, out_e[k], hc);
