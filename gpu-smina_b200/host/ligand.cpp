@@ -417,7 +417,7 @@ Model read_pdbqt_ligand(const std::string& text) {
     const int nf = (int)F.fparent.size();
 
     // assign_bonds (model.cpp:448-529): distance-based within non-variable pairs
-    auto mobility = [&](int i, int j) -> int { return i == j ? D_FIXED : F.mob[std::min(i, j)][std::max(i, j)]; };
+    auto mobility = [&](int i, int j) -> int { return i == j ? (int)D_FIXED : F.mob[std::min(i, j)][std::max(i, j)]; };
     auto d2 = [&](int i, int j) {
         double s = 0;
         for (int k = 0; k < 3; k++) { double d = F.atoms[i].xyz[k] - F.atoms[j].xyz[k]; s += d * d; }
