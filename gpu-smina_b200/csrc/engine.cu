@@ -111,6 +111,14 @@ void sg_destroy(sg_engine* e) {
 const char* sg_last_error(const sg_engine* e) { return e ? e->err.c_str() : "no engine"; }
 int sg_precision(const sg_engine* e) { return e ? e->precision : -1; }
 
+int sg_device_info(const sg_engine* e, int* device, int* num_sms, int* smem_optin) {
+    if (!e) return SG_ERR_ARG;
+    if (device) *device = e->device;
+    if (num_sms) *num_sms = e->num_sms;
+    if (smem_optin) *smem_optin = e->max_smem;
+    return SG_OK;
+}
+
 int sg_set_tables(sg_engine* e, const sg_tables_desc* t) {
     return guarded(e, [&] {
         require(t && t->smooth && t->fast, "tables: null pointers");

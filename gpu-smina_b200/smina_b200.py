@@ -128,6 +128,7 @@ def _declare(L):
         "sgh_merge_chains": [C.POINTER(ChainResult), C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp, _dp,
                              _ip],
         "sg_create": [C.c_int, C.c_int, C.POINTER(vp)],
+        "sg_device_info": [vp, _ip, _ip, _ip],
         "sg_set_tables": [vp, C.POINTER(TablesDesc)],
         "sg_set_receptor": [vp, C.c_int, C.POINTER(ReceptorDesc), C.POINTER(GridDims)],
         "sg_build_grids": [vp, C.c_int, _ip, C.c_int],
@@ -545,6 +546,12 @@ class Engine:
         return [{"e": e[:outs[k].count].copy(), "conf": conf[:outs[k].count].copy(),
                  "coords": xyz[:outs[k].count].copy(), "evals": int(outs[k].evals)}
                 for k, (e, conf, xyz) in enumerate(bufs)]
+
+    def device_info(self):
+        """sg_device_info: device ordinal, SM count, opt-in shared memory per block."""
+        d, sms, smem = C.c_int(), C.c_int(), C.c_int()
+        self._check(load().sg_device_info(self._h, C.byref(d), C.byref(sms), C.byref(smem)))
+        return {"device": d.value, "num_sms": sms.value, "smem_optin": smem.value}
 
     def batch_stats(self):
         """Timing and counters of the last dock_batch call."""

@@ -187,6 +187,12 @@ int  sg_create(int device, int precision, sg_engine** out);
 void sg_destroy(sg_engine* e);
 const char* sg_last_error(const sg_engine* e);
 int  sg_precision(const sg_engine* e);
+/* The engine's device ordinal, its SM count and the shared memory a block
+ * may opt in to (read at sg_create; no device work).  Any pointer may be
+ * NULL.  Callers size batches from it, as the reference's
+ * GpuDocking::chains_per_batch does from the device's residency
+ * (src/gpu/gpu_docking.h:109-111). */
+int  sg_device_info(const sg_engine* e, int* device, int* num_sms, int* smem_optin);
 
 /* Pair tables (copied to the device). */
 int sg_set_tables(sg_engine* e, const sg_tables_desc* t);
