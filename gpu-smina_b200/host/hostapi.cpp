@@ -210,6 +210,18 @@ int sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out) {
     return SG_OK;
 }
 
+int sgh_fast_chains(long long tasks, long long capacity, int chain_split, double step_fraction, double budget,
+                    unsigned steps, int* split, unsigned* chain_steps, double* fraction) {
+    if (tasks < 0 || capacity < 0 || chain_split < 0 || !(step_fraction >= 0) || !(budget >= 0) ||
+        step_fraction > 1 || budget > 1 || !split || !chain_steps)
+        return SG_ERR_ARG;
+    const sgh::FastPlan f = sgh::fast_plan((size_t)tasks, (size_t)capacity, chain_split, step_fraction, budget, steps);
+    *split = f.split;
+    *chain_steps = f.steps;
+    if (fraction) *fraction = f.fraction;
+    return SG_OK;
+}
+
 int sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims* box, double* confs, uint32_t* mt) {
     return guarded([&] {
         std::vector<sgh::ChainStart> cs = sgh::seed_chains(m->m, seed, tasks, *box);

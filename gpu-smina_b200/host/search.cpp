@@ -21,6 +21,28 @@ unsigned search_steps(const Model& m) {
     return unsigned(70 * 3 * (50 + heuristic) / 2);
 }
 
+// --fast's chain split (not smina's search), gpu_docking.cpp:87-112,168-220:
+// every task becomes `split` chains with ceil(steps * fraction / split) steps.
+// Automatic split (chain_split 0): the largest power of two from 32 down to
+// 4 whose chains stay within 4 waves of the device's resident capacity.
+// Automatic fraction (step_fraction 0): 1/2 for splits from 4 up to 31
+// (the device is full), else 1.  A first-pass budget > 0 overrides the
+// fraction.
+FastPlan fast_plan(size_t tasks, size_t capacity, int chain_split, double step_fraction, double budget,
+                   unsigned steps) {
+    FastPlan f;
+    if (chain_split > 0) {
+        f.split = chain_split;
+    } else {
+        f.split = 32;
+        while (f.split > 4 && tasks * (size_t)f.split > 4 * capacity) f.split /= 2;
+    }
+    f.fraction = budget > 0 ? budget : step_fraction > 0 ? step_fraction : (f.split >= 4 && f.split < 32 ? 0.5 : 1.0);
+    const double per = std::ceil(steps * f.fraction / f.split);
+    f.steps = per < 1 ? 1u : unsigned(per);
+    return f;
+}
+
 sg_mc_params search_params(const Model& m, int num_modes) {
     sg_mc_params p{};  // visited = 0: smina's search
     p.num_steps = search_steps(m);

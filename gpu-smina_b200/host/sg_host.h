@@ -144,6 +144,13 @@ sg_grid_dims make_box(const double center[3], const double size[3], double granu
 // ---- search parameters and seeding -------------------------------------------
 // setup_search (main.cpp:513-529): steps, maxiters, ...
 sg_mc_params search_params(const Model& m, int num_modes = 9);
+struct FastPlan {
+    int split = 1;
+    double fraction = 1;
+    unsigned steps = 1;
+};
+FastPlan fast_plan(size_t tasks, size_t capacity, int chain_split, double step_fraction, double budget,
+                   unsigned steps);
 unsigned search_steps(const Model& m);
 
 // mt19937 (Boost semantics)

@@ -125,6 +125,8 @@ def _declare(L):
         "sgh_make_box": [C.c_double * 3, C.c_double * 3, C.c_double, C.POINTER(GridDims)],
         "sgh_search_params": [vp, C.c_int, C.POINTER(MCParams)],
         "sgh_seed_chains": [vp, C.c_int, C.c_int, C.POINTER(GridDims), _dp, _up],
+        "sgh_fast_chains": [C.c_longlong, C.c_longlong, C.c_int, C.c_double, C.c_double, C.c_uint, _ip,
+                            C.POINTER(C.c_uint), _dp],
         "sgh_merge_chains": [C.POINTER(ChainResult), C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp, _dp,
                              _ip],
         "sg_create": [C.c_int, C.c_int, C.POINTER(vp)],
@@ -401,6 +403,15 @@ def make_chain_batch(models, model_of_chain, confs, mts, steps, num_saved, heavy
         outs[k].conf = conf[k].ctypes.data_as(_dp)
         outs[k].coords = coords[k].ctypes.data_as(_dp)
     return ChainBatch(ins, outs, keep, e, conf, coords)
+
+
+def fast_chains(tasks, capacity, chain_split=0, step_fraction=0.0, budget=0.0, steps=1):
+    """sgh_fast_chains: (split, steps per chain, fraction) of --fast's chain
+    split for `tasks` search tasks on a device holding `capacity` chains."""
+    sp, st, fr = C.c_int(), C.c_uint(), C.c_double()
+    _check_host(load().sgh_fast_chains(int(tasks), int(capacity), int(chain_split), float(step_fraction),
+                                       float(budget), int(steps), C.byref(sp), C.byref(st), C.byref(fr)))
+    return sp.value, st.value, fr.value
 
 
 def merge_chains(batch, model, first=0, n=None, min_rmsd=2.0, max_size=20):

@@ -17,10 +17,13 @@
  *     For FP64 engines these are the states the plain kernels start from, as
  *     the reference's --gpu_fp64 chains start from the host's.  FP32 engines
  *     key their counter-based streams by (seed, ligand index).
- *   - Not built, and refused at construction with a message: chain_split
- *     != 1, step_fraction != 1, early_stop (the reference's --fast search,
- *     which is not smina's), threads_per_chain above 32, and skip_visited
- *     with FP32 engines (QuickVina 2's history runs on the FP64 path only).
+ *   - The reference's --fast search (not smina's) is built in part:
+ *     chain_split and step_fraction (0: automatic) and dock_batch's first-pass
+ *     budget, planned by sgh_fast_chains; skip_visited on FP64 engines.
+ *     Refused at construction with a message: early_stop (it needs chains
+ *     that stop and resume between phases), threads_per_chain above 32, and
+ *     skip_visited with FP32 engines (QuickVina 2's history runs on the FP64
+ *     path only).
  *
  * Precision follows the reference: the search runs in FP32 (mixed
  * precision, batched) unless settings.fp64; refinement and local
@@ -51,8 +54,8 @@ struct GpuSettings {
     std::vector<int> devices{0};
     bool fp64 = false;
     int threads_per_chain = 0;  /* 0: automatic; only 32 threads per chain are built */
-    int chain_split = 1;
-    double step_fraction = 1;
+    int chain_split = 1;        /* chains per search task (0: automatic, --fast) */
+    double step_fraction = 1;   /* fraction of smina's steps (0: automatic, --fast) */
     bool skip_visited = false;
     enum { EARLY_STOP_OFF, EARLY_STOP_FULL, EARLY_STOP_ALWAYS };
     int early_stop = EARLY_STOP_OFF;
@@ -173,10 +176,11 @@ class GpuDocking {
 public:
     explicit GpuDocking(const GpuSettings& s) : settings_(s) {
         if (s.devices.empty()) throw std::runtime_error("no CUDA device given");
-        if (s.chain_split != 1) throw std::runtime_error("chain_split is not built in this engine (smina's search only)");
-        if (s.step_fraction != 1) throw std::runtime_error("step_fraction is not built in this engine (smina's search only)");
+        if (s.chain_split < 0) throw std::runtime_error("chain_split must be 0 (automatic) or positive");
+        if (!(s.step_fraction >= 0 && s.step_fraction <= 1))
+            throw std::runtime_error("step_fraction must lie in [0, 1] (0: automatic)");
         if (s.early_stop != GpuSettings::EARLY_STOP_OFF)
-            throw std::runtime_error("early_stop is not built in this engine (smina's search only)");
+            throw std::runtime_error("early_stop is not built in this engine");
         if (s.threads_per_chain != 0 && s.threads_per_chain != 32)
             throw std::runtime_error("threads_per_chain: this engine runs 32 threads per chain");
         if (s.skip_visited && !s.fp64)
@@ -235,15 +239,17 @@ public:
      * refine_structure of every pose (FP64, cap as the refinement's curl
      * cap), poses sorted by energy.  FP32 engines run all jobs of a device
      * in one persistent launch; jobs are split over the devices in
-     * contiguous ranges, one host thread per device. */
+     * contiguous ranges, one host thread per device.  budget > 0: that
+     * fraction of smina's steps (a first pass of two-pass screening). */
     void dock_batch(std::vector<DockJob*>& jobs, const sgh_tables* p, sgh_receptor* rec, const sg_grid_dims& gd,
-                    int seed, const double cap[3]) {
+                    int seed, const double cap[3], double budget = 0) {
+        if (!(budget >= 0 && budget <= 1)) throw std::runtime_error("dock_batch: budget must lie in [0, 1]");
         if (jobs.empty()) return;
         const size_t nd = std::min(dev_.size(), jobs.size());
         std::vector<std::string> errors(nd);
         auto run = [&](size_t k, size_t lo, size_t hi) {
             try {
-                dock_range(k, jobs, lo, hi, p, rec, gd, seed, cap);
+                dock_range(k, jobs, lo, hi, p, rec, gd, seed, cap, budget);
             } catch (const std::exception& ex) {
                 errors[k] = ex.what();
             }
@@ -357,12 +363,14 @@ private:
 
     /* jobs [lo, hi) on device k */
     void dock_range(size_t k, std::vector<DockJob*>& jobs, size_t lo, size_t hi, const sgh_tables* p,
-                    sgh_receptor* rec, const sg_grid_dims& gd, int seed, const double cap[3]) {
+                    sgh_receptor* rec, const sg_grid_dims& gd, int seed, const double cap[3], double budget) {
+        long long tasks = 0;  /* search tasks docked at once on this device: they set the automatic split */
+        for (size_t j = lo; j < hi; j++) tasks += jobs[j]->par.num_tasks;
         if (settings_.fp64) {
             for (size_t j = lo; j < hi; j++) {
                 DockJob& job = *jobs[j];
                 OutputContainer poses;
-                search_on(k, job.par, job.m, poses, p, rec, gd, seed);
+                search_on(k, job.par, job.m, poses, p, rec, gd, seed, tasks, budget);
                 std::vector<Pose*> ptr;
                 for (Pose& q : poses) ptr.push_back(&q);
                 MinParams mp{job.par.mc.maxiters, job.par.mc.accurate_line, job.par.mc.early_term};
@@ -386,8 +394,9 @@ private:
                 throw std::runtime_error("dock_batch: every job must keep the same number of poses");
             models[j] = detail::desc_of(job.m);
             heavy[j] = sgh_model_heavy(job.m);
-            lj[j] = sg_ligand_job{int(j), job.par.num_tasks, job.par.mc.num_steps, job.par.mc.maxiters,
-                                  uint64_t(seed), uint64_t(lo + j)};
+            const Plan f = plan(k, tasks, budget, job.par.mc.num_steps);
+            lj[j] = sg_ligand_job{int(j), job.par.num_tasks * f.split, f.steps, job.par.mc.maxiters, uint64_t(seed),
+                                  uint64_t(lo + j)};
             const int S = mc.num_saved_mins;
             e_[j].assign(S, 0.0);
             c_[j].assign(size_t(S) * models[j].conf_size, 0.0);
@@ -402,13 +411,31 @@ private:
             append(jobs[lo + j]->out, res[j].count, e_[j], c_[j], x_[j], models[j].conf_size, heavy[j]);
     }
 
+    /* --fast's chain split for `tasks` tasks docked at once on device k */
+    struct Plan {
+        int split = 1;
+        unsigned steps = 1;
+    };
+    Plan plan(size_t k, long long tasks, double budget, unsigned steps) const {
+        Plan f;
+        int sms = 0;
+        sg_device_info(dev_[k].search, nullptr, &sms, nullptr);
+        const long long capacity = (long long)sms * (settings_.fp64 ? 32 : 16);
+        detail::check_host(sgh_fast_chains(tasks, capacity, settings_.chain_split, settings_.step_fraction, budget,
+                                           steps, &f.split, &f.steps, nullptr),
+                           "chain split");
+        return f;
+    }
+
     void search_on(size_t k, const ParallelMC& par, const sgh_model* m, OutputContainer& out, const sgh_tables* p,
-                   sgh_receptor* rec, const sg_grid_dims& gd, int seed) {
+                   sgh_receptor* rec, const sg_grid_dims& gd, int seed, long long tasks = 0, double budget = 0) {
         if (par.num_tasks <= 0) throw std::runtime_error("parallel_mc: no tasks");
         sg_engine* e = prepare(k, false, p, rec, gd);
         const sg_model_desc d = detail::desc_of(m);
-        const int heavy = sgh_model_heavy(m), S = par.mc.num_saved_mins, n = par.num_tasks;
+        const Plan f = plan(k, tasks > 0 ? tasks : par.num_tasks, budget, par.mc.num_steps);
+        const int heavy = sgh_model_heavy(m), S = par.mc.num_saved_mins, n = par.num_tasks * f.split;
         sg_mc_params mc = par.mc;
+        mc.num_steps = f.steps;
         mc.visited = settings_.skip_visited ? 1 : 0;
         std::vector<double> e_(S), conf(size_t(S) * d.conf_size), xyz(size_t(S) * heavy * 3);
         int count = 0;

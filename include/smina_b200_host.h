@@ -87,6 +87,17 @@ int  sgh_finish_docking(const sgh_tables* t, const double inputs[7], int n, cons
 
 int  sgh_make_box(const double center[3], const double size[3], double granularity, sg_grid_dims* out);
 int  sgh_search_params(const sgh_model* m, int num_modes, sg_mc_params* out);
+/* --fast's chain split and step fraction (not smina's search; the
+ * reference's GpuSettings::chain_split / step_fraction and dock_batch's
+ * budget, src/gpu/gpu_docking.cpp:87-112,168-220): every search task
+ * becomes *split chains of *chain_steps steps each.  chain_split 0 picks the
+ * split from the tasks docked at once and the device's resident chain
+ * capacity (the largest power of two from 32 down to 4 within 4 waves);
+ * step_fraction 0 picks 1/2 for splits 4..31, else 1; budget > 0 (a
+ * first pass) overrides the fraction.  *fraction (may be NULL) gets the
+ * fraction used.  Host arithmetic only. */
+int  sgh_fast_chains(long long tasks, long long capacity, int chain_split, double step_fraction, double budget,
+                     unsigned steps, int* split, unsigned* chain_steps, double* fraction);
 /* confs [tasks][conf_size], mt [tasks][625] */
 int  sgh_seed_chains(const sgh_model* m, int seed, int tasks, const sg_grid_dims* box, double* confs, uint32_t* mt);
 

@@ -1,7 +1,8 @@
 // Host-side checks of the C++ interface (include/smina_b200.hpp), in the
 // manner of the reference's own C++ test programs (src/gpu/tests): settings
-// that the reference accepts but this engine does not build are refused at
-// construction with std::runtime_error, device lists parse like the
+// out of range, or that the reference accepts but this engine does not
+// build, are refused at construction with std::runtime_error; --fast's
+// chain split and step fraction are accepted; device lists parse like the
 // reference's parse_devices, and a machine without a usable device gets an
 // exception from the constructor instead of a half-built engine.
 //
@@ -54,9 +55,10 @@ int main(int argc, char** argv) {
     expect_throw([] { smina_b200::parse_devices("1a"); }, "bad device list", "trailing characters");
     expect_throw([] { smina_b200::parse_devices("-1"); }, "bad device list", "negative device");
     // settings this engine does not build
-    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.chain_split = 4; })); }, "chain_split", "chain_split");
-    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.step_fraction = 0.5; })); }, "step_fraction",
-                 "step_fraction");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.chain_split = -1; })); }, "chain_split",
+                 "negative chain_split");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.step_fraction = 1.5; })); }, "step_fraction",
+                 "step_fraction above 1");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_FULL; })); },
                  "early_stop", "early_stop");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 128; })); }, "threads_per_chain",
@@ -72,6 +74,8 @@ int main(int argc, char** argv) {
     if (mode == "host") {
         // without a usable device the constructor throws (cuda_check in the reference)
         expect_throw([] { GpuDocking g(GpuSettings{}); }, "not usable", "no device present");
+        expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.chain_split = 0; s.step_fraction = 0; })); },
+                     "not usable", "--fast settings pass validation");
         expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.fp64 = true; })); }, "not usable",
                      "no device present, fp64");
     }
