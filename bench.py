@@ -355,6 +355,100 @@ def run_redock(args):
     }), flush=True)
 
 
+REF_SEARCH_SO = os.path.join(ROOT, "baseline", "_ref", "libref_search32.so")
+
+
+def run_ref_gpu(args):
+    """The reference's own FP32 GPU search on this GPU, beside this engine's,
+    on the same screen.  baseline/_ref/libref_search32.so holds the
+    reference's device library (src/gpu/gpu_device.cu, gpu_kernels_f32.cu)
+    compiled for sm_100a from its sources (make -C baseline/ref_gpu, which
+    needs the reference tree).  Both searches get every chain of every
+    ligand at once, smina's step counts (times --step-scale), no refinement;
+    the reference's chains start from host-seeded confs and mt19937 states,
+    this engine's from its own counter-based streams.  Reported: each
+    search's time and ligands/s, and the mean best (unrefined) energy."""
+    import ctypes as C
+    if not os.path.exists(REF_SEARCH_SO):
+        print(json.dumps({"mode": "reference_gpu", "unavailable": "baseline/_ref/libref_search32.so is not built "
+                                                                   "(make -C baseline/ref_gpu needs the reference tree)"}))
+        return
+    L = C.CDLL(REF_SEARCH_SO)
+    L.refs_last_error.restype = C.c_char_p
+    L.refs_create.argtypes = [C.POINTER(sb.TablesDesc), C.POINTER(sb.ReceptorDesc), C.POINTER(sb.GridDims), sb._ip,
+                              C.c_int, C.c_double, C.POINTER(C.c_void_p)]
+    L.refs_dock.argtypes = [C.c_void_p, C.POINTER(sb.ModelDesc), C.c_int, C.POINTER(sb.ChainInput), C.c_int,
+                            C.POINTER(sb.MCParams), C.POINTER(sb.ChainResult), C.POINTER(C.c_double)]
+    L.refs_destroy.argtypes = [C.c_void_p]
+    spec = screen(args.ligands, args.seed)
+    models = build_models(spec)
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    types = np.array(sorted({t for m in models for t in m.types() if 1 < t < 27}), np.int32)
+    p = make_params(models)
+    exh = args.exhaustiveness
+
+    def ref_chains(ms):
+        confs, mts, moc, steps, its = [], [], [], [], []
+        for k, m in enumerate(ms):
+            sp = m.search_params(9)
+            c, mt = m.seed_chains(args.seed + k, exh, gd)
+            confs += list(c)
+            mts += list(mt)
+            moc += [k] * exh
+            steps += [max(1, int(sp.num_steps * args.step_scale))] * exh
+            its += [sp.maxiters] * exh
+        return sb.make_chain_batch(ms, moc, confs, mts, steps, p.num_saved_mins, [m.heavy for m in ms], its)
+
+    def ref_dock(ms, b):
+        descs = (sb.ModelDesc * len(ms))(*[m.desc for m in ms])
+        secs = C.c_double()
+        rc = L.refs_dock(h, descs, len(ms), b.inputs, len(b.e), C.byref(p), b.results, C.byref(secs))
+        if rc != 0:
+            raise RuntimeError("reference search: " + L.refs_last_error().decode())
+        return secs.value
+
+    h = C.c_void_p()
+    if L.refs_create(C.byref(T.desc), C.byref(R.desc), C.byref(gd), sb.iptr(types), len(types), 1e6, C.byref(h)):
+        raise RuntimeError("reference maps: " + L.refs_last_error().decode())
+    warm = models[:2]
+    ref_dock(warm, ref_chains(warm))  # loads the reference's kernels
+    b = ref_chains(models)
+    t_ref = ref_dock(models, b)
+    cnt = [b.results[c].count for c in range(len(b.e))]
+    best_ref = []
+    for k in range(len(models)):
+        vals = [b.e[c, :cnt[c]].min() for c in range(exh * k, exh * (k + 1)) if cnt[c] > 0]
+        best_ref.append(float(min(vals)) if vals else float("nan"))
+    L.refs_destroy(h)
+    eng = sb.Engine(0, sb.PREC_FP32)
+    eng.set_tables(T)
+    eng.set_receptor(0, R, gd)
+    eng.build_grids(0, [int(t) for t in types])
+    jobs = jobs_for(models, list(range(len(models))), exh, args.seed, 0, args.step_scale)
+    eng.dock_batch(0, models[:2], jobs_for(models[:2], [0, 1], exh, args.seed, 0, 0.001), p, refine=False)
+    t0 = time.perf_counter()
+    r = eng.dock_batch(0, models, jobs, p, refine=False)
+    t_ours_wall = time.perf_counter() - t0
+    t_ours = eng.batch_stats()["mc_ms"] / 1000.0
+    best_ours = [float(x["e"][0]) if len(x["e"]) else float("nan") for x in r]
+    n = len(models)
+    print(json.dumps({
+        "mode": "reference_gpu",
+        "config": {"workload": f"virtual screen, {n} ligands (heavy U[10,50], rotors U[0,12]), receptor 3000 heavy "
+                               f"atoms, 22 A box at 0.375 A, exhaustiveness {exh}, smina step counts"
+                               + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
+                               + ", every chain at once, search only (no merge, no refinement)"},
+        "reference_fp32": {"search_s": t_ref, "ligands_per_s": n / t_ref,
+                           "how": "run_monte_carlo<float>, 32 threads per chain, wall time of the call",
+                           "mean_best_e_unrefined": float(np.nanmean(best_ref))},
+        "this_engine_fp32": {"search_s": t_ours, "ligands_per_s": n / t_ours, "call_wall_s": t_ours_wall,
+                             "how": "k_mc32 persistent launch, CUDA-event time of the search launch",
+                             "mean_best_e_unrefined": float(np.nanmean(best_ours))},
+    }), flush=True)
+
+
 SERVE_RECEPTORS = ((2000, 22.0), (3000, 26.0), (5000, 30.0))  # (heavy atoms, box edge in A)
 
 
@@ -523,6 +617,9 @@ def main():
                     help="instead of the batched search: the same screen through the plain FP64 path")
     ap.add_argument("--visited", action="store_true",
                     help="with --plain64: QuickVina 2's history check (not smina's search)")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="instead of timing: the reference's own FP32 GPU search (built from its sources into "
+                         "baseline/_ref) beside this engine's, on the same screen")
     ap.add_argument("--redock", type=int, default=0,
                     help="instead of timing: the single-ligand redock (FP64 exhaustiveness 8, FP32 exhaustiveness "
                          "128) with this many seeds; top-pose energy and RMSD differences")
@@ -533,6 +630,9 @@ def main():
         return
     if args.redock:
         run_redock(args)
+        return
+    if args.ref_gpu:
+        run_ref_gpu(args)
         return
     if args.serve:
         run_serve(args)
