@@ -2,8 +2,9 @@
 
 The harness hands this project's models and receptors to the reference's
 own FP64 device library; before it uploads anything it converts them to the
-reference's flat structures (a restatement of src/gpu/gpu_flatten.cpp) and
-checks every index the reference's kernels read.  These tests run that
+reference's flat structures (baseline/ref_gpu/flatten.h, a restatement of
+src/gpu/gpu_flatten.cpp shared with the reference GPU baseline) and checks
+every index the reference's kernels read.  These tests run that
 conversion and those checks on the CPU for every input the golden-record
 script uses, and compare the conversion's counts with counts taken here
 from the descriptors.  The harness is built only where the reference tree
