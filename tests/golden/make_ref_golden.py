@@ -16,9 +16,10 @@ writes one compressed archive of its outputs:
 
 next to SHA-256 digests of every input, so a reader can tell that it
 rebuilds the same inputs.  It then runs the oracle on the same inputs and
-prints how many values agree bit for bit and the largest difference.
+prints how many values agree bit for bit and the largest difference; with
+--engine it does the same for this engine's FP64 path on the GPU.
 
-    python tests/golden/make_ref_golden.py --out tests/golden/ref_fp64.npz
+    python tests/golden/make_ref_golden.py --engine --out tests/golden/ref_fp64.npz
 
 Cases: default (vina) scoring and the charge-dependent ad4_scoring tables;
 a 1,500-atom receptor with a 14 A box at 0.375 A; ligands of 14/3, 24/5 and
@@ -185,7 +186,42 @@ class Ref:
         self.L.refg_destroy(self.h)
 
 
-# ---- one side's outputs (the reference's or the oracle's) ------------------------------------------------
+class EngineSide:
+    """This engine's plain FP64 path with the oracle's method names, so that
+    outputs() records it the same way (a third side of the comparison)."""
+
+    def __init__(self, T, R, gd):
+        self.e = sb.Engine(0, sb.PREC_FP64)
+        self.e.set_tables(T)
+        self.e.set_receptor(0, R, gd)
+        self.gd = gd
+
+    def build_grids(self, types):
+        self.e.build_grids(0, types)
+
+    def grid(self, t, charged):
+        return self.e.grid(0, t, self.gd, charged)
+
+    def eval(self, m, confs, v, slope):
+        return self.e.eval(0, m, confs, v=v, slope=slope)
+
+    def eval_direct(self, m, confs, slope):
+        return self.e.eval_direct(0, m, confs, slope=slope)
+
+    def bfgs(self, m, confs, v, slope, maxiters, accurate):
+        return self.e.bfgs(0, m, confs, v=v, slope=slope, maxiters=maxiters, accurate=accurate)
+
+    def dock(self, models, moc, c0, mt, p, steps):
+        return self.e.dock(0, models, moc, c0, mt, p, steps=steps)
+
+    def refine(self, models, pm, poses, cap, maxiters):
+        return self.e.refine(0, models, pm, poses, cap=cap, maxiters=maxiters)
+
+    def close(self):
+        self.e.close()
+
+
+# ---- one side's outputs (the reference's, the oracle's or this engine's) --------------------------------
 def outputs(side, T, gd, models, tag):
     """Every recorded quantity of a case, as {key: array}; `side` is a Ref
     or a tests/oracle_lib.Oracle (same method names)."""
@@ -248,6 +284,7 @@ def compare(ref, mine):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(HERE, "ref_fp64.npz"))
+    ap.add_argument("--engine", action="store_true", help="also compare this engine's FP64 path on the GPU")
     args = ap.parse_args()
     from oracle_lib import Oracle
     rec = {}
@@ -259,8 +296,15 @@ def main():
         rec[f"{name}/sha256"] = np.array(digest(T, R, gd, models))
         o = outputs(Oracle(T, R, gd, full_cells=True), T, gd, models, name)
         total, same, worst, key = compare(r, o)
-        print(f"{name}: {same}/{total} values bit-identical to the oracle; largest relative difference "
-              f"{worst:.3g} ({key or 'none'})", flush=True)
+        print(f"{name}: oracle: {same}/{total} values bit-identical to the reference; largest relative "
+              f"difference {worst:.3g} ({key or 'none'})", flush=True)
+        if args.engine:
+            eng = EngineSide(T, R, gd)
+            g = outputs(eng, T, gd, models, name)
+            eng.close()
+            total, same, worst, key = compare(r, g)
+            print(f"{name}: this engine (FP64): {same}/{total} values bit-identical to the reference; largest "
+                  f"relative difference {worst:.3g} ({key or 'none'})", flush=True)
     np.savez_compressed(args.out, **rec)
     print(f"wrote {args.out} ({os.path.getsize(args.out)} bytes)")
 
