@@ -59,6 +59,24 @@ int or_set_receptor(or_ctx* o, const sg_receptor_desc* r, const sg_grid_dims* gd
     return 0;
 }
 
+/* A user grid (--user_grid) on the same footing as the receptor: added to
+ * every map at the map point's index coordinates (cache.cpp:204-205, with
+ * the cache's slope) and to the direct sum at each atom (non_cache.cpp:
+ * 180-184).  data [(n0+1)(n1+1)(n2+1)], x fastest; NULL clears it.  Maps
+ * built before are dropped. */
+int or_set_user_grid(or_ctx* o, const sg_grid_dims* gd, const double* data, double cache_slope) {
+    o->c.ug = UserGrid();
+    if (gd && data) {
+        o->c.ug.init = true;
+        o->c.ug.geom.init_from(*gd);
+        const size_t n = (size_t)(gd->n[0] + 1) * (gd->n[1] + 1) * (gd->n[2] + 1);
+        o->c.ug.data.assign(data, data + n);
+        o->c.ug.slope = cache_slope;
+    }
+    std::fill(o->c.built.begin(), o->c.built.end(), false);
+    return 0;
+}
+
 int or_build_grids(or_ctx* o, const int* types, int n) {
     try {
         populate(o->c, types, n);

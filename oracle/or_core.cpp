@@ -267,6 +267,9 @@ static void table_eval_fast(const Tables& T, int t1, int t2, double r2, double* 
 }
 
 // ---- cache::populate (cache.cpp:116-206) ----------------------------------
+static double evaluate_aux(const GridGeom& G, const std::vector<double>& D, const V3& loc, double slope, double v,
+                           V3* deriv);
+
 void populate(Ctx& c, const int* types, int ntypes) {
     std::vector<int> needed;
     for (int k = 0; k < ntypes; k++) {
@@ -309,8 +312,13 @@ void populate(Ctx& c, const int* types, int ntypes) {
                     }
                 }
                 size_t idx = (size_t)x + (size_t)g.dim[0] * ((size_t)y + (size_t)g.dim[1] * z);
+                // the user grid is evaluated at the point's index coordinates, as
+                // cache::populate does (cache.cpp:204-205)
+                const double u = c.ug.init ? evaluate_aux(c.ug.geom, c.ug.data, V3(x, y, z), c.ug.slope, 1000, nullptr)
+                                           : 0.0;
                 for (size_t j = 0; j < needed.size(); j++) {
                     c.grids[needed[j]].data[idx] = aff[j];
+                    if (c.ug.init) c.grids[needed[j]].data[idx] += u;
                     if (charged) c.grids[needed[j]].chargedata[idx] = chg[j];
                 }
             }
@@ -511,6 +519,11 @@ double eval_direct_deriv(Ctx& c, CellLists& cl, const Model& m, const double* co
                 this_e += pe;
                 addto(deriv, dor * rba);
             }
+        }
+        if (c.ug.init) {  // non_cache.cpp:180-184: at the atom's own coordinates
+            V3 ugd(0, 0, 0);
+            this_e += evaluate_aux(c.ug.geom, c.ug.data, a, slope, 1000, &ugd);
+            deriv = deriv + ugd;
         }
         curl(this_e, deriv, v[1]);
         s.minus_forces[i] = deriv + oobd;

@@ -137,6 +137,15 @@ struct CellLists {
     const std::vector<int>& get(const V3& coord);
 };
 
+// a user grid (--user_grid; grid::init(gd, user_in, ...), grid.cpp:78-110):
+// its own geometry and values, x fastest
+struct UserGrid {
+    bool init = false;
+    GridGeom geom;
+    std::vector<double> data;
+    double slope = 1e6;  // the cache's slope, used when it is added to the maps
+};
+
 struct Ctx {
     Tables tab;
     Receptor rec;
@@ -145,6 +154,7 @@ struct Ctx {
     std::vector<bool> built;
     bool has_receptor = false;
     bool full_cells = false;  // non_cache cell semantics
+    UserGrid ug;
 };
 
 // evaluations

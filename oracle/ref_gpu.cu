@@ -128,15 +128,29 @@ int refg_check_receptor(const sg_tables_desc* t, const sg_receptor_desc* r, cons
 }
 
 /* Uploads tables and receptor and builds the reference's FP64 grid maps
- * for `types` (DeviceGrids::build, cache::populate). */
+ * for `types` (DeviceGrids::build, cache::populate).  ug_dims / ug_data
+ * (both NULL for none): a user grid over ug_dims, values x fastest, as
+ * smina holds it after reading (FlatUserGrid, gpu_flatten.cpp:506-531). */
 int refg_create(const sg_tables_desc* t, const sg_receptor_desc* r, const sg_grid_dims* gd, const int* types,
-                int ntypes, double slope, refg_ctx** out) {
+                int ntypes, double slope, const sg_grid_dims* ug_dims, const double* ug_data, refg_ctx** out) {
     refg_ctx* c = nullptr;
     try {
         need(t && r && gd && out && (ntypes == 0 || types), "create: null argument");
+        need((ug_dims == nullptr) == (ug_data == nullptr), "create: user grid needs both dims and data");
         c = new refg_ctx;
         c->ft = tables(*t);
         c->geo = geometry(*gd);
+        if (ug_dims) {
+            const FlatGridGeometry g = geometry(*ug_dims);
+            c->ug.initialized = true;
+            c->ug.geom = g;
+            for (int i = 0; i < 3; i++) {
+                c->ug.geom.gd_begin[i] = c->ug.geom.gd_end[i] = 0;
+                c->ug.geom.gd_enabled[i] = 0;
+            }
+            c->ug.data.assign(ug_data, ug_data + size_t(g.dim[0]) * g.dim[1] * g.dim[2]);
+            c->dug.upload(c->ug);
+        }
         c->rec_grid = receptor_for_grid(*r, *gd, c->geo, t->cutoff_sqr);
         c->rec_full = receptor_full(*r, t->cutoff_sqr);
         check_receptor(c->rec_grid);

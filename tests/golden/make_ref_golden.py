@@ -23,7 +23,9 @@ prints how many values agree bit for bit and the largest difference; with
 
 Cases: default (vina) scoring and the charge-dependent ad4_scoring tables;
 a 1,500-atom receptor with a 14 A box at 0.375 A; ligands of 14/3, 24/5 and
-40/10 heavy atoms/rotors, and the 24/5 ligand with flexible residues.
+40/10 heavy atoms/rotors, and the 24/5 ligand with flexible residues; and the
+24/5 ligand with a user grid (--user_grid) added to the maps and the direct
+sum.
 """
 import argparse
 import ctypes as C
@@ -54,7 +56,32 @@ def cases():
     lig = [W.ligand(14, 3, 2), W.ligand(24, 5, 11), W.ligand(40, 10, 5)]
     flex = sb.Model(sb.make_ligand_pdbqt(24, 5, 11, W.CENTER), sb.make_flex_pdbqt(4, 3, W.CENTER))
     return [("vina", W.tables(), R, gd, lig + [flex]),
-            ("ad4", sb.Tables("ad4_scoring"), R, gd, [lig[1]])]
+            ("ad4", sb.Tables("ad4_scoring"), R, gd, [lig[1]]),
+            ("vina_ug", W.tables(), R, gd, [lig[1]])]
+
+
+def user_grid_for(name, gd):
+    """(GridDims, values x fastest) of a case's user grid, or None.  Values
+    as smina holds them after reading a user grid file (grid.cpp:78-110
+    fills x, y, z < n and leaves the last plane of each axis at 0)."""
+    if name != "vina_ug":
+        return None
+    n = 16
+    g = sb.GridDims()
+    for i in range(3):
+        g.begin[i], g.end[i], g.n[i] = gd.begin[i] - 4.0, gd.end[i] + 4.0, n
+    v = 0.5 * np.random.default_rng(77).normal(size=(n + 1, n + 1, n + 1))  # [z][y][x]
+    v[n, :, :] = v[:, n, :] = v[:, :, n] = 0.0
+    return g, np.ascontiguousarray(v.ravel())
+
+
+def oracle_for(name, T, R, gd):
+    from oracle_lib import Oracle
+    o = Oracle(T, R, gd, full_cells=True)
+    ug = user_grid_for(name, gd)
+    if ug is not None:
+        o.set_user_grid(*ug)
+    return o
 
 
 def grid_types(models):
@@ -75,8 +102,11 @@ def _arr(ptr, n, dtype):
     return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype) if n else np.zeros(0, dtype)
 
 
-def digest(T, R, gd, models):
+def digest(T, R, gd, models, ug=None):
     h = hashlib.sha256()
+    if ug is not None:
+        h.update(np.array(list(ug[0].begin) + list(ug[0].end), np.float64).tobytes())
+        h.update(np.array(list(ug[0].n), np.int64).tobytes() + ug[1].tobytes())
     t = T.desc
     cells = 351 * t.n * t.num_components
     h.update(np.array([t.num_types, t.num_components, t.n], np.int64).tobytes())
@@ -114,13 +144,13 @@ def grid_sample(gd, seed):
 
 # ---- the reference (oracle/_ref/libref_gpu.so) ----------------------------------------------------------
 class Ref:
-    def __init__(self, T, R, gd, types):
+    def __init__(self, T, R, gd, types, ug=None):
         L = C.CDLL(REF_SO)
         vp, dp, ip = C.c_void_p, sb._dp, sb._ip
         L.refg_last_error.restype = C.c_char_p
         sig = {
             "refg_create": [C.POINTER(sb.TablesDesc), C.POINTER(sb.ReceptorDesc), C.POINTER(sb.GridDims), ip, C.c_int,
-                            C.c_double, C.POINTER(vp)],
+                            C.c_double, C.POINTER(sb.GridDims), dp, C.POINTER(vp)],
             "refg_get_grid": [vp, C.c_int, dp, dp],
             "refg_eval": [vp, C.POINTER(sb.ModelDesc), C.c_int, dp, C.c_double * 3, C.c_int, C.c_double, dp, dp, dp],
             "refg_bfgs": [vp, C.POINTER(sb.ModelDesc), C.c_int, dp, C.c_double * 3, C.c_int, C.c_int, C.c_int, dp],
@@ -137,7 +167,9 @@ class Ref:
         self.L, self.gd = L, gd
         self.h = vp()
         t = np.ascontiguousarray(types, np.int32)
+        self._ug = None if ug is None else np.ascontiguousarray(ug[1], np.float64)
         self._check(L.refg_create(C.byref(T.desc), C.byref(R.desc), C.byref(gd), sb.iptr(t), len(t), 1e6,
+                                  None if ug is None else C.byref(ug[0]), None if ug is None else sb.dptr(self._ug),
                                   C.byref(self.h)))
 
     def _check(self, rc):
@@ -286,19 +318,19 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "ref_fp64.npz"))
     ap.add_argument("--engine", action="store_true", help="also compare this engine's FP64 path on the GPU")
     args = ap.parse_args()
-    from oracle_lib import Oracle
     rec = {}
     for name, T, R, gd, models in cases():
-        ref = Ref(T, R, gd, grid_types(models))
+        ug = user_grid_for(name, gd)
+        ref = Ref(T, R, gd, grid_types(models), ug)
         r = outputs(ref, T, gd, models, name)
         ref.close()
         rec.update(r)
-        rec[f"{name}/sha256"] = np.array(digest(T, R, gd, models))
-        o = outputs(Oracle(T, R, gd, full_cells=True), T, gd, models, name)
+        rec[f"{name}/sha256"] = np.array(digest(T, R, gd, models, ug))
+        o = outputs(oracle_for(name, T, R, gd), T, gd, models, name)
         total, same, worst, key = compare(r, o)
         print(f"{name}: oracle: {same}/{total} values bit-identical to the reference; largest relative "
               f"difference {worst:.3g} ({key or 'none'})", flush=True)
-        if args.engine:
+        if args.engine and ug is None:  # the engine has no user grids yet
             eng = EngineSide(T, R, gd)
             g = outputs(eng, T, gd, models, name)
             eng.close()

@@ -35,6 +35,7 @@ def load():
             "or_set_tables": [vp, C.POINTER(sb.TablesDesc)],
             "or_set_receptor": [vp, C.POINTER(sb.ReceptorDesc), C.POINTER(sb.GridDims), C.c_int],
             "or_build_grids": [vp, sb._ip, C.c_int],
+            "or_set_user_grid": [vp, C.POINTER(sb.GridDims), sb._dp, C.c_double],
             "or_get_grid": [vp, C.c_int, sb._dp, sb._dp],
             "or_eval": [vp, C.POINTER(sb.ModelDesc), C.c_int, sb._dp, C.c_double * 3, C.c_double, sb._dp, sb._dp, sb._dp],
             "or_eval_direct": [vp, C.POINTER(sb.ModelDesc), C.c_int, sb._dp, C.c_double * 3, C.c_double, sb._dp, sb._dp],
@@ -81,6 +82,16 @@ class Oracle:
         self.box = box
         self._built = set()
         load().or_set_receptor(self.h, C.byref(receptor.desc), C.byref(box), int(full_cells))
+
+    def set_user_grid(self, gd, data, cache_slope=1e6):
+        """A user grid (--user_grid) over `gd`, values x fastest; None clears it."""
+        self._built = set()
+        if data is None:
+            self._check(load().or_set_user_grid(self.h, None, None, cache_slope))
+            return
+        self._ug = np.ascontiguousarray(data, dtype=np.float64).ravel(order="F") if np.ndim(data) == 3 else \
+            np.ascontiguousarray(data, dtype=np.float64)
+        self._check(load().or_set_user_grid(self.h, C.byref(gd), sb.dptr(self._ug), cache_slope))
 
     def build_grids(self, types):
         t = np.ascontiguousarray(sorted(set(int(x) for x in types)), dtype=np.int32)

@@ -7,7 +7,8 @@ written by tests/golden/make_ref_golden.py.  Here every case's inputs are
 rebuilt from their seeds, checked against the recorded SHA-256 digest, and
 the oracle's outputs are compared with the records: grid maps, eval at two
 curl caps, direct eval, BFGS with both line searches, Monte Carlo chains and
-refine_structure, for vina and ad4 tables and a model with flexible residues.
+refine_structure, for vina and ad4 tables, a model with flexible residues and a
+user grid.
 
 The bar is the reference's own for its FP64 path (gpu_eval_test.cpp:173-210,
 gpu_mc_test.cpp:44-81): relative differences of at most 1e-9 and identical
@@ -23,7 +24,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
 
 import make_ref_golden as G  # noqa: E402
-from oracle_lib import Oracle  # noqa: E402
 
 FIXTURE = os.path.join(HERE, "golden", "ref_fp64.npz")
 REL = 1e-9  # the reference's FP64 tolerance
@@ -37,12 +37,13 @@ def records():
         return {k: z[k] for k in z.files}
 
 
-@pytest.mark.parametrize("case", ["vina", "ad4"])
+@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug"])
 def test_oracle_matches_the_reference_device_library(records, case):
     name, T, R, gd, models = next(c for c in G.cases() if c[0] == case)
-    assert str(records[f"{name}/sha256"]) == G.digest(T, R, gd, models), "inputs differ from the recorded ones"
+    ug = G.user_grid_for(name, gd)
+    assert str(records[f"{name}/sha256"]) == G.digest(T, R, gd, models, ug), "inputs differ from the recorded ones"
     ref = {k: v for k, v in records.items() if k.startswith(f"{name}/") and not k.endswith("/sha256")}
-    mine = G.outputs(Oracle(T, R, gd, full_cells=True), T, gd, models, name)
+    mine = G.outputs(G.oracle_for(name, T, R, gd), T, gd, models, name)
     assert set(ref) == set(mine)
     for k, a in ref.items():
         b = np.asarray(mine[k])
