@@ -149,7 +149,6 @@ int refg_create(const sg_tables_desc* t, const sg_receptor_desc* r, const sg_gri
                 c->ug.geom.gd_enabled[i] = 0;
             }
             c->ug.data.assign(ug_data, ug_data + size_t(g.dim[0]) * g.dim[1] * g.dim[2]);
-            c->dug.upload(c->ug);
         }
         c->rec_grid = receptor_for_grid(*r, *gd, c->geo, t->cutoff_sqr);
         c->rec_full = receptor_full(*r, t->cutoff_sqr);
@@ -161,6 +160,7 @@ int refg_create(const sg_tables_desc* t, const sg_receptor_desc* r, const sg_gri
             tl.push_back(types[i]);
         }
         c->slope = slope;
+        if (c->ug.initialized) c->dug.upload(c->ug);
         c->tables.upload(c->ft);
         c->receptor.upload(c->rec_full);
         c->grids.build(c->rec_grid, c->geo, c->ft, tl, c->ug, slope);
