@@ -38,7 +38,8 @@ inline void need(bool ok, const char* what) {
 inline FlatGridGeometry geometry(const sg_grid_dims& gd) {
     FlatGridGeometry g;
     for (int i = 0; i < 3; i++) {
-        need(gd.n[i] >= 0 && gd.end[i] > gd.begin[i], "grid: bad dimensions");
+        // at least two points per axis: evaluate_aux reads corners a and a + 1 with a <= dim - 2
+        need(gd.n[i] >= 1 && gd.end[i] > gd.begin[i], "grid: bad dimensions");
         g.dim[i] = gd.n[i] + 1;
         g.init[i] = gd.begin[i];
         const double range = gd.end[i] - gd.begin[i];
