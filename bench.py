@@ -355,6 +355,48 @@ def run_redock(args):
     }), flush=True)
 
 
+def run_fast(args):
+    """The reference's --fast search (not smina's) on the same screen: chain
+    split and step fraction chosen automatically by sgh_fast_chains for the
+    screen's tasks on this device (16 resident chains per SM), then merge and
+    FP64 refinement as in the headline.  Reports ligands/s of the call and
+    the mean best refined energy, beside the same for smina's search."""
+    spec = screen(args.ligands, args.seed)
+    models = build_models(spec)
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina")
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    eng = sb.Engine(0, sb.PREC_FP32)
+    eng.set_tables(T)
+    eng.set_receptor(0, R, gd)
+    eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
+    p = make_params(models)
+    cap = 16 * eng.device_info()["num_sms"]
+    runs = {}
+    for name, jobs in (("smina", jobs_for(models, list(range(len(models))), args.exhaustiveness, args.seed, 0)),
+                       ("fast", sb.fast_jobs(models, args.exhaustiveness, args.seed, cap))):
+        eng.dock_batch(0, models[:2], [sb.LigandJob(model=k, num_chains=2, num_steps=5, maxiters=j.maxiters,
+                                                    seed=j.seed, ligand_key=j.ligand_key)
+                                       for k, j in enumerate(jobs[:2])], p)  # warm
+        with Clocks(0) as clk:
+            t0 = time.perf_counter()
+            r = eng.dock_batch(0, models, jobs, p)
+            wall = time.perf_counter() - t0
+        st = eng.batch_stats()
+        runs[name] = {"ligands_per_s": len(models) / wall, "wall_s": wall, "search_ms": st["mc_ms"],
+                      "refine_ms": st["refine_ms"], "chains_per_ligand": jobs[0].num_chains,
+                      "steps_of_first_ligand": jobs[0].num_steps,
+                      "mean_best_e": float(np.mean([x["e"][0] for x in r if len(x["e"])])),
+                      "clocks": {k_: clk.summary()[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")}}
+    print(json.dumps({
+        "mode": "fast", "metric": "ligands docked/sec, --fast search (not smina's)", "unit": UNIT, "n_gpus": 1,
+        "config": {"workload": f"virtual screen, {args.ligands} ligands (heavy U[10,50], rotors U[0,12]), receptor "
+                               f"3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness {args.exhaustiveness}; "
+                               "automatic chain split and step fraction; merge + FP64 refine"},
+        "runs": runs,
+    }), flush=True)
+
+
 REF_SEARCH_SO = os.path.join(ROOT, "baseline", "_ref", "libref_search32.so")
 
 
@@ -617,6 +659,8 @@ def main():
                     help="instead of the batched search: the same screen through the plain FP64 path")
     ap.add_argument("--visited", action="store_true",
                     help="with --plain64: QuickVina 2's history check (not smina's search)")
+    ap.add_argument("--fast", action="store_true",
+                    help="instead of timing: the reference's --fast search (not smina's) beside smina's, same screen")
     ap.add_argument("--ref-gpu", action="store_true",
                     help="instead of timing: the reference's own FP32 GPU search (built from its sources into "
                          "baseline/_ref) beside this engine's, on the same screen")
@@ -633,6 +677,9 @@ def main():
         return
     if args.ref_gpu:
         run_ref_gpu(args)
+        return
+    if args.fast:
+        run_fast(args)
         return
     if args.serve:
         run_serve(args)

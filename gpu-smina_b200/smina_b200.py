@@ -414,6 +414,22 @@ def fast_chains(tasks, capacity, chain_split=0, step_fraction=0.0, budget=0.0, s
     return sp.value, st.value, fr.value
 
 
+def fast_jobs(models, num_tasks, seed, capacity, chain_split=0, step_fraction=0.0, budget=0.0, key_base=0,
+              num_modes=9):
+    """LigandJobs of the reference's --fast search (not smina's): every
+    ligand's num_tasks tasks become `split` chains each, with the steps
+    sgh_fast_chains plans for all the screen's tasks on a device holding
+    `capacity` chains; BFGS iterations stay smina's."""
+    tasks = num_tasks * len(models)
+    jobs = []
+    for k, m in enumerate(models):
+        p = m.search_params(num_modes)
+        split, steps, _ = fast_chains(tasks, capacity, chain_split, step_fraction, budget, p.num_steps)
+        jobs.append(LigandJob(model=k, num_chains=num_tasks * split, num_steps=steps, maxiters=p.maxiters, seed=seed,
+                              ligand_key=key_base + k))
+    return jobs
+
+
 def merge_chains(batch, model, first=0, n=None, min_rmsd=2.0, max_size=20):
     """merge_output_containers over chains [first, first + n) of a ChainBatch."""
     n = len(batch.count) - first if n is None else n

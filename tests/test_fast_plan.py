@@ -53,3 +53,17 @@ def test_automatic_split_follows_the_load():
 def test_bad_arguments_are_refused(args):
     with pytest.raises(sb.SminaError):
         sb.fast_chains(*args)
+
+
+def test_fast_jobs_shape_the_screen():
+    import workloads as W
+    models = [W.ligand(14, 3, 2), W.ligand(24, 5, 11)]
+    jobs = sb.fast_jobs(models, 8, 42, capacity=16 * 148)
+    for m, j in zip(models, jobs):
+        p = m.search_params()
+        assert j.num_chains == 8 * 32  # two ligands leave the device idle: 32 chains per task
+        assert j.num_steps == max(1, math.ceil(p.num_steps / 32))
+        assert j.maxiters == p.maxiters and j.seed == 42
+    plain = sb.fast_jobs(models, 8, 42, capacity=16 * 148, chain_split=1, step_fraction=1.0)
+    assert [j.num_chains for j in plain] == [8, 8]
+    assert [j.num_steps for j in plain] == [m.search_params().num_steps for m in models]
