@@ -52,3 +52,13 @@ def test_host_errors_are_reported():
         sb.Tables("no_such_function")
     with pytest.raises(sb.SminaError):
         sb.Tables("vina", custom_text="1.0 bogus_term(x=1)\n")
+
+
+@pytest.mark.gpu
+def test_device_info_reports_the_engine_device():
+    e = sb.Engine(0, sb.PREC_FP32)
+    try:
+        info = e.device_info()
+        assert info["device"] == 0 and info["num_sms"] > 0 and info["smem_optin"] >= 48 * 1024
+    finally:
+        e.close()
