@@ -222,10 +222,12 @@ class EngineSide:
     """This engine's plain FP64 path with the oracle's method names, so that
     outputs() records it the same way (a third side of the comparison)."""
 
-    def __init__(self, T, R, gd):
+    def __init__(self, T, R, gd, ug=None):
         self.e = sb.Engine(0, sb.PREC_FP64)
         self.e.set_tables(T)
         self.e.set_receptor(0, R, gd)
+        if ug is not None:
+            self.e.set_user_grid(0, *ug)
         self.gd = gd
 
     def build_grids(self, types):

@@ -1,4 +1,5 @@
-"""The oracle against the reference's own FP64 device library.
+"""The oracle, and this engine's FP64 path, against the reference's own FP64
+device library.
 
 tests/golden/ref_fp64.npz holds what the reference's FP64 validation path
 (src/gpu/gpu_device.cu, src/gpu/gpu_kernels_f64.cu, behind
@@ -37,13 +38,8 @@ def records():
         return {k: z[k] for k in z.files}
 
 
-@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug"])
-def test_oracle_matches_the_reference_device_library(records, case):
-    name, T, R, gd, models = next(c for c in G.cases() if c[0] == case)
-    ug = G.user_grid_for(name, gd)
-    assert str(records[f"{name}/sha256"]) == G.digest(T, R, gd, models, ug), "inputs differ from the recorded ones"
+def _check(records, name, mine):
     ref = {k: v for k, v in records.items() if k.startswith(f"{name}/") and not k.endswith("/sha256")}
-    mine = G.outputs(G.oracle_for(name, T, R, gd), T, gd, models, name)
     assert set(ref) == set(mine)
     for k, a in ref.items():
         b = np.asarray(mine[k])
@@ -55,3 +51,30 @@ def test_oracle_matches_the_reference_device_library(records, case):
             assert np.array_equal(a, b), k
     total, same, worst, key = G.compare(ref, mine)
     assert same == total, f"{total - same} of {total} values differ in the last bits (largest {worst:.3g} at {key})"
+
+
+def _case(records, case):
+    name, T, R, gd, models = next(c for c in G.cases() if c[0] == case)
+    ug = G.user_grid_for(name, gd)
+    assert str(records[f"{name}/sha256"]) == G.digest(T, R, gd, models, ug), "inputs differ from the recorded ones"
+    return name, T, R, gd, models, ug
+
+
+@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug"])
+def test_oracle_matches_the_reference_device_library(records, case):
+    name, T, R, gd, models, _ = _case(records, case)
+    _check(records, name, G.outputs(G.oracle_for(name, T, R, gd), T, gd, models, name))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["vina", "ad4"])
+def test_engine_matches_the_reference_device_library(records, case):
+    """This engine's FP64 path (grid maps, eval at both curl caps, direct
+    eval, both line searches, 40-step chains, refine; the vina case includes
+    a model with flexible residues) against the same records."""
+    name, T, R, gd, models, ug = _case(records, case)
+    side = G.EngineSide(T, R, gd, ug)
+    try:
+        _check(records, name, G.outputs(side, T, gd, models, name))
+    finally:
+        side.close()
