@@ -84,7 +84,7 @@ static void add_pose(std::vector<HostPose>& out, HostPose&& t, double min_rmsd, 
 
 // launch shape: chains (warps) per block with the most resident chains per
 // SM (ties: more chains per block, so fewer model copies)
-static void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ) {
+void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ) {
     const int cands[4] = {8, 4, 2, 1};
     int best_w = 0, best_occ = 0, best_res = 0;
     for (int c : cands) {

@@ -667,11 +667,16 @@ static cudaError_t prep32(const void* fn, size_t smem) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-// resident blocks per SM of k_mc32 with `wpb` chains (warps) per block
+// resident blocks per SM of k_mc32 with `wpb` chains (warps) per block; 0
+// when the shape does not fit (the failed call's error is cleared, so the
+// next launch's check does not see it)
 int mc32_occupancy(int wpb, size_t smem) {
-    if (prep32((const void*)k_mc32, smem) != cudaSuccess) return 0;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_mc32, 32 * wpb, smem) != cudaSuccess) return 0;
+    if (prep32((const void*)k_mc32, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_mc32, 32 * wpb, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
     return blocks;
 }
 
@@ -686,11 +691,21 @@ cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G,
     return cudaGetLastError();
 }
 
-// Serving launches: many launches of k_mc32 run at once, so they all take the
-// same dynamic shared memory (set once here), which keeps every SM's
-// shared-memory configuration the same for all of them and sets no function
-// attribute while earlier launches run.
-cudaError_t serve_prepare32(size_t smem_fixed) { return prep32((const void*)k_mc32, smem_fixed); }
+// Raises k_mc32's dynamic shared-memory limit ahead of time, so that later
+// launches (serving's many concurrent ones, the no-allocation entry point's)
+// set no function attribute while other launches of the kernel run.  The
+// first use also loads the kernel's module.
+cudaError_t mc32_reserve_smem(size_t smem) { return prep32((const void*)k_mc32, smem); }
+
+// the largest dynamic shared memory a k_mc32 block can take: the device's
+// opt-in limit less the kernel's static shared memory
+cudaError_t mc32_max_dynamic_smem(size_t optin, size_t* out) {
+    cudaFuncAttributes fa{};
+    cudaError_t rc = cudaFuncGetAttributes(&fa, (const void*)k_mc32);
+    if (rc != cudaSuccess) return rc;
+    *out = optin > fa.sharedSizeBytes ? optin - fa.sharedSizeBytes : 0;
+    return cudaSuccess;
+}
 
 cudaError_t launch_mc32_fixed(const DModel* dms, const DTables32& T, const DMaps32& G, const DMaps32* maps_tab,
                               const Chain32* chains, const Item32* items, int nitems, const MCParams32& P,

@@ -32,8 +32,10 @@ namespace sg {
 constexpr size_t kScratchBytes = size_t(8) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of the fixed array, looked up once per device (the first
-// call on a device does it, with that device current).
+// Device address of the fixed array, looked up once per device with that
+// device current.  The lookup also loads this file's module, and with it the
+// array: under lazy module loading that is the moment the 8 MiB is taken from
+// the device, so engine creation does it (noalloc_claim), not a call.
 static std::mutex g_scratch_mu;
 static unsigned char* g_scratch_ptr[64] = {};
 
@@ -46,6 +48,17 @@ static unsigned char* scratch_on(int device) {
         g_scratch_ptr[device] = static_cast<unsigned char*>(p);
     }
     return g_scratch_ptr[device];
+}
+
+// At engine creation (mixed-precision engines): claim the fixed array and
+// load the search kernel with its shared-memory limit raised to the device's
+// maximum, so that a later call neither loads a module nor sets a kernel
+// attribute.
+void noalloc_claim(sg_engine* e) {
+    scratch_on(e->device);
+    size_t dyn = 0;
+    cuda_check(mc32_max_dynamic_smem((size_t)e->max_smem, &dyn), "search kernel attributes");
+    cuda_check(mc32_reserve_smem(dyn), "search kernel shared-memory limit");
 }
 
 // bump placement inside the fixed array
@@ -130,11 +143,10 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
         }
         ws_stride = (ws_stride + 15) & ~(size_t)15;
         const int S = p->num_saved_mins;
-        // chains and their result slots
-        std::vector<Chain32> hc;
-        std::vector<int> chain_job;
-        std::vector<size_t> cres_off, xres_off;
-        size_t nconf_res = 0, nxyz_res = 0;
+        // first pass: check the jobs and count what the batch needs, so that
+        // a batch too large for the array is refused before any per-chain
+        // host table is built
+        size_t nchains = 0, nconf_res = 0, nxyz_res = 0;
         int max_chains = 1;
         for (int j = 0; j < njobs; j++) {
             const sg_ligand_job& J = jobs[j];
@@ -144,52 +156,19 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
             require(out[j].e && out[j].conf && out[j].coords, "dock_batch32_noalloc: null result arrays");
             max_chains = std::max(max_chains, J.num_chains);
             const DModel& h = img.host[J.model];
-            for (int c = 0; c < J.num_chains; c++) {
-                Chain32 ch{};
-                ch.model = J.model;
-                ch.steps = J.num_steps;
-                ch.maxiters = J.maxiters > 0 ? J.maxiters : p->maxiters;
-                ch.key0 = (uint32_t)J.seed;
-                ch.key1 = (uint32_t)(J.seed >> 32) ^ (uint32_t)(J.ligand_key >> 32);
-                ch.lig = (uint32_t)J.ligand_key;
-                ch.chain = (uint32_t)c;
-                hc.push_back(ch);
-                chain_job.push_back(j);
-                cres_off.push_back(nconf_res);
-                xres_off.push_back(nxyz_res);
-                nconf_res += (size_t)S * h.conf_size;
-                nxyz_res += (size_t)S * h.nheavy * 3;
-            }
+            nchains += (size_t)J.num_chains;
+            nconf_res += (size_t)J.num_chains * S * h.conf_size;
+            nxyz_res += (size_t)J.num_chains * S * h.nheavy * 3;
         }
-        const size_t nchains = hc.size();
-        // launch shape: the most resident chains per SM
-        int wpb = 0, occ = 0;
-        for (int c : {8, 4, 2, 1}) {
-            if (c > 1 && c / 2 >= max_chains) continue;
-            const size_t smem = stage_stride + (size_t)c * ws_stride;
-            if (smem > (size_t)e->max_smem) continue;
-            const int o = mc32_occupancy(c, smem);
-            if (o * c > occ * wpb) { wpb = c; occ = o; }
-        }
-        require(wpb > 0, "model too large for the mixed-precision path's shared memory");
-        std::vector<Item32> items;
-        std::vector<double> item_cost;
-        for (size_t k = 0; k < nchains;) {
-            const int j = chain_job[k];
-            int n = 0;
-            while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
-            items.push_back(Item32{hc[k].model, (int)k, n, 0});
-            item_cost.push_back((double)hc[k].steps * img.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
-            k += n;
-        }
-        std::vector<int> order(items.size());
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_cost[a] > item_cost[b]; });
-        std::vector<Item32> queue(items.size());
-        for (size_t k = 0; k < items.size(); k++) queue[k] = items[order[k]];
-        // everything else the kernel writes
+        require(nchains <= (size_t(1) << 24), "dock_batch32_noalloc: at most 2^24 chains per call");
+        // launch shape as sg_dock_batch32 picks it (a shape set by
+        // sg_set_chains_per_block or sg_autotune32 included)
+        int wpb = 1, occ = 1;
+        choose_launch(e, stage_stride, ws_stride, max_chains, wpb, occ);
+        size_t nitems_sz = 0;
+        for (int j = 0; j < njobs; j++) nitems_sz += (size_t)(jobs[j].num_chains + wpb - 1) / wpb;
         const size_t chains_at = at.take(nchains * sizeof(Chain32));
-        const size_t items_at = at.take(queue.size() * sizeof(Item32));
+        const size_t items_at = at.take(nitems_sz * sizeof(Item32));
         const size_t queue_at = at.take(sizeof(unsigned));
         const size_t e_at = at.take(nchains * S * sizeof(double));
         const size_t conf_at = at.take(nconf_res * sizeof(double));
@@ -202,6 +181,51 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
             throw EngineError(SG_ERR_ARG, "dock_batch32_noalloc: this batch needs " + std::to_string(at.used) +
                                               " bytes of scratch but the fixed array holds " +
                                               std::to_string(kScratchBytes) + "; dock fewer ligands per call");
+        // second pass: the chains and their result slots
+        std::vector<Chain32> hc;
+        std::vector<int> chain_job;
+        std::vector<size_t> cres_off, xres_off;
+        hc.reserve(nchains);
+        chain_job.reserve(nchains);
+        cres_off.reserve(nchains);
+        xres_off.reserve(nchains);
+        size_t conf_cur = 0, xyz_cur = 0;
+        for (int j = 0; j < njobs; j++) {
+            const sg_ligand_job& J = jobs[j];
+            const DModel& h = img.host[J.model];
+            for (int c = 0; c < J.num_chains; c++) {
+                Chain32 ch{};
+                ch.model = J.model;
+                ch.steps = J.num_steps;
+                ch.maxiters = J.maxiters > 0 ? J.maxiters : p->maxiters;
+                ch.key0 = (uint32_t)J.seed;
+                ch.key1 = (uint32_t)(J.seed >> 32) ^ (uint32_t)(J.ligand_key >> 32);
+                ch.lig = (uint32_t)J.ligand_key;
+                ch.chain = (uint32_t)c;
+                hc.push_back(ch);
+                chain_job.push_back(j);
+                cres_off.push_back(conf_cur);
+                xres_off.push_back(xyz_cur);
+                conf_cur += (size_t)S * h.conf_size;
+                xyz_cur += (size_t)S * h.nheavy * 3;
+            }
+        }
+        std::vector<Item32> items;
+        std::vector<double> item_cost;
+        for (size_t k = 0; k < nchains;) {
+            const int j = chain_job[k];
+            int n = 0;
+            while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
+            items.push_back(Item32{hc[k].model, (int)k, n, 0});
+            item_cost.push_back((double)hc[k].steps * img.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
+            k += n;
+        }
+        require(items.size() == nitems_sz, "dock_batch32_noalloc: work item count");
+        std::vector<int> order(items.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_cost[a] > item_cost[b]; });
+        std::vector<Item32> queue(items.size());
+        for (size_t k = 0; k < items.size(); k++) queue[k] = items[order[k]];
         for (size_t k = 0; k < nchains; k++) {
             Chain32& ch = hc[k];
             ch.out_e = reinterpret_cast<double*>(base + e_at) + k * S;
@@ -240,10 +264,14 @@ int sg_dock_batch32_noalloc(sg_engine* e, int rid, const sg_model_desc* models, 
         P.early_term = p->early_term;
         const int nitems = (int)queue.size();
         const int blocks = (int)std::min<long long>((long long)occ * e->num_sms, nitems);
-        cuda_check(launch_mc32(reinterpret_cast<const DModel*>(base + models_at + img.dmodel_off), tables32(e),
-                               maps32(e, r), nullptr, reinterpret_cast<const Chain32*>(base + chains_at),
-                               reinterpret_cast<const Item32*>(base + items_at), nitems, P,
-                               reinterpret_cast<unsigned*>(base + queue_at), blocks, wpb, stage_stride, ws_stride, s),
+        // the kernel's shared-memory limit was raised at engine creation, so
+        // this launch sets no kernel attribute (a serving loop's launches may
+        // be running on other streams)
+        cuda_check(launch_mc32_fixed(reinterpret_cast<const DModel*>(base + models_at + img.dmodel_off), tables32(e),
+                                     maps32(e, r), nullptr, reinterpret_cast<const Chain32*>(base + chains_at),
+                                     reinterpret_cast<const Item32*>(base + items_at), nitems, P,
+                                     reinterpret_cast<unsigned*>(base + queue_at), blocks, wpb, stage_stride,
+                                     ws_stride, stage_stride + (size_t)wpb * ws_stride, s),
                    "search launch");
         std::vector<double> he(nchains * S), hconf(nconf_res);
         std::vector<float> hxyz(nxyz_res);

@@ -787,7 +787,7 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
         // memory and the 1 KB the driver keeps per block), which leaves L1 room
         // for the gathers; bigger models run fewer chains per block.
         s->smem_block = std::min<size_t>((size_t)e->max_smem, 82048);
-        cuda_check(serve_prepare32(s->smem_block), "serve: kernel attributes");
+        cuda_check(mc32_reserve_smem(s->smem_block), "serve: kernel attributes");
         cuda_check(cudaStreamCreateWithFlags(&s->refine_stream, cudaStreamNonBlocking), "serve: stream");
         cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "serve: stream");
         unsigned* hf = nullptr;
