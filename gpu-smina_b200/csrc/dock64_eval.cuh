@@ -8,7 +8,7 @@
 // cache.cpp:69-90; non_cache.cpp:109-191; tree.h:108-243;
 // precalculate.h:111-151,245-293.
 #pragma once
-#include "sg_dev.cuh"
+#include "grid64.cuh"
 
 namespace sg {
 
@@ -72,46 +72,6 @@ __device__ void set_conf64(W64& w, const double* conf) {
         st3(S + w.L.coords + 3 * i, c);
     }
     __syncwarp();
-}
-
-// grid::evaluate_aux
-__device__ double grid_aux64(const DGeom& G, const double* D, V3<double> loc, double slope, double v,
-                             V3<double>& deriv) {
-    double s[3] = {(loc.x - G.init[0]) * G.factor[0], (loc.y - G.init[1]) * G.factor[1],
-                   (loc.z - G.init[2]) * G.factor[2]};
-    double miss[3] = {0, 0, 0};
-    int region[3];
-    int a[3];
-    for (int i = 0; i < 3; i++) {
-        if (s[i] < 0) {
-            miss[i] = -s[i]; region[i] = -1; a[i] = 0; s[i] = 0;
-        } else if (s[i] >= G.dim_fl_minus_1[i]) {
-            miss[i] = s[i] - G.dim_fl_minus_1[i]; region[i] = 1; a[i] = G.dim[i] - 2; s[i] = 1;
-        } else {
-            region[i] = 0; a[i] = (int)(unsigned long long)s[i]; s[i] -= (double)a[i];
-        }
-    }
-    const double penalty = slope * (miss[0] * G.factor_inv[0] + miss[1] * G.factor_inv[1] + miss[2] * G.factor_inv[2]);
-    const size_t d0 = G.dim[0], d01 = (size_t)G.dim[0] * G.dim[1];
-    const double* b = D + a[0] + d0 * a[1] + d01 * a[2];
-    const double f000 = b[0], f100 = b[1], f010 = b[d0], f110 = b[d0 + 1];
-    const double f001 = b[d01], f101 = b[d01 + 1], f011 = b[d01 + d0], f111 = b[d01 + d0 + 1];
-    const double x = s[0], y = s[1], z = s[2];
-    const double mx = 1 - x, my = 1 - y, mz = 1 - z;
-    double f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
-               f001 * mx * my * z + f101 * x * my * z + f011 * mx * y * z + f111 * x * y * z;
-    const double xg = -(f000 * my * mz) + f100 * my * mz + -(f010 * y * mz) + f110 * y * mz + -(f001 * my * z) +
-                      f101 * my * z + -(f011 * y * z) + f111 * y * z;
-    const double yg = -(f000 * mx * mz) + -(f100 * x * mz) + f010 * mx * mz + f110 * x * mz + -(f001 * mx * z) +
-                      -(f101 * x * z) + f011 * mx * z + f111 * x * z;
-    const double zg = -(f000 * mx * my) + -(f100 * x * my) + -(f010 * mx * y) + -(f110 * x * y) + f001 * mx * my +
-                      f101 * x * my + f011 * mx * y + f111 * x * y;
-    V3<double> grad{xg, yg, zg};
-    curl_ed(f, grad, v);
-    deriv.x = G.factor[0] * (region[0] == 0 ? grad.x : 0.0) + slope * region[0];
-    deriv.y = G.factor[1] * (region[1] == 0 ? grad.y : 0.0) + slope * region[1];
-    deriv.z = G.factor[2] * (region[2] == 0 ? grad.z : 0.0) + slope * region[2];
-    return f + penalty;
 }
 
 // precalculate_linear::eval_deriv (type-ordered lookup, charge-weighted components)
@@ -218,6 +178,11 @@ __device__ void direct_atoms64(W64& w, double v, double slope) {
             }
         } else {
             atomicExch(w.err, kDevBadModel);
+        }
+        if (R.ugrid) {  // the user grid at the atom's own coordinates (non_cache.cpp:180-184)
+            V3<double> ugd;
+            this_e += grid_aux64(R.ug, R.ugrid, V3<double>{a[0], a[1], a[2]}, slope, 1000.0, ugd);
+            add_to(deriv, ugd);
         }
         curl_ed(this_e, deriv, v);
         mf[0] = deriv.x + oobd[0];

@@ -32,7 +32,13 @@ void DevBuf::upload(const void* src, size_t n, cudaStream_t s) {
 }
 
 void cuda_check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw EngineError(SG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        // a failed call that does not poison the context still stays the
+        // thread's last error, which the next launch's check would report
+        // again; clear it
+        cudaGetLastError();
+        throw EngineError(SG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
 }
 
 DGeom make_geom(const sg_grid_dims& gd) {
@@ -94,6 +100,7 @@ int sg_create(int device, int precision, sg_engine** out) {
         cuda_check(cudaGetDeviceProperties(&prop, device), "device properties");
         e->num_sms = prop.multiProcessorCount;
         e->max_smem = (int)prop.sharedMemPerBlockOptin;
+        if (precision != SG_PREC_FP64) noalloc_claim(e.get());
     });
     if (rc != SG_OK) return rc;
     *out = e.release();
@@ -185,6 +192,8 @@ void refresh_header(sg_engine* e, RecState& r) {
         h.cmap32[t] = r.cmap32[t].as<float4>();
         h.map16[t] = r.map16[t].as<uint4>();
     }
+    h.ugrid = r.ugrid.as<double>();
+    h.ug = r.ug;
     if (!r.dhdr.p) r.dhdr.alloc(sizeof(DReceptor));
     cuda_check(cudaMemcpyAsync(r.dhdr.p, &h, sizeof(DReceptor), cudaMemcpyHostToDevice, e->stream), "receptor header");
     cuda_check(cudaStreamSynchronize(e->stream), "receptor header");
@@ -284,7 +293,8 @@ void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes) {
     dcmaps.upload(cmaps.data(), cmaps.size() * sizeof(double*), e->stream);
     cuda_check(launch_grid_map64(r.geom, r.natoms, r.xyz.as<double>(), r.type.as<int>(), r.charge.as<double>(),
                                  r.pop_start.as<int>(), r.pop_atoms.as<int>(), e->tables, dtypes.as<int>(), (int)need.size(),
-                                 dmaps.as<double*>(), dcmaps.as<double*>(), e->stream),
+                                 dmaps.as<double*>(), dcmaps.as<double*>(), r.ugrid.as<double>(), r.ug, r.ug_slope,
+                                 e->stream),
                "grid maps");
     if (e->precision != SG_PREC_FP64) {
         const size_t ncells = (size_t)(r.geom.dim[0] - 1) * (r.geom.dim[1] - 1) * (r.geom.dim[2] - 1);
@@ -325,6 +335,8 @@ int sg_set_receptor(sg_engine* e, int rid, const sg_receptor_desc* r, const sg_g
         RecState& s = e->rec[rid];
         s.clear_maps();
         s.pop_start.reset(); s.pop_atoms.reset(); s.full_start.reset(); s.full_atoms.reset();
+        s.ugrid.reset();  // a new receptor starts without a user grid
+        s.ug = DGeom{};
         s.gd = *gd;
         s.geom = make_geom(*gd);
         s.natoms = r->num_atoms;
@@ -362,13 +374,36 @@ int sg_get_grid(sg_engine* e, int rid, int type, double* data, double* chargedat
     });
 }
 
+int sg_set_user_grid(sg_engine* e, int rid, const sg_grid_dims* gd, const double* data, double cache_slope) {
+    return guarded(e, [&] {
+        RecState& r = receptor_for(e, rid);
+        if (gd && data) {
+            for (int i = 0; i < 3; i++) {
+                require(gd->n[i] >= 1 && gd->n[i] <= 4096, "user grid: n must be in [1, 4096]");
+                require(gd->end[i] > gd->begin[i], "user grid: end must exceed begin");
+            }
+            require(std::isfinite(cache_slope), "user grid: non-finite slope");
+            const size_t n = (size_t)(gd->n[0] + 1) * (gd->n[1] + 1) * (gd->n[2] + 1);
+            for (size_t k = 0; k < n; k++) require(std::isfinite(data[k]), "user grid: non-finite value");
+            r.ugrid.upload(data, n * sizeof(double), e->stream);
+            r.ug = make_geom(*gd);
+            r.ug_slope = cache_slope;
+        } else {
+            r.ugrid.reset();
+            r.ug = DGeom{};
+        }
+        r.clear_maps();
+        refresh_header(e, r);
+    });
+}
+
 int sg_drop_receptor(sg_engine* e, int rid) {
     return guarded(e, [&] {
         require(rid >= 0 && rid < SG_MAX_RECEPTORS, "receptor id out of range");
         RecState& s = e->rec[rid];
         s.clear_maps();
         s.pop_start.reset(); s.pop_atoms.reset(); s.full_start.reset(); s.full_atoms.reset();
-        s.xyz.reset(); s.type.reset(); s.charge.reset(); s.dhdr.reset();
+        s.xyz.reset(); s.type.reset(); s.charge.reset(); s.dhdr.reset(); s.ugrid.reset();
         s.set = false;
     });
 }

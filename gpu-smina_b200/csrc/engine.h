@@ -45,6 +45,9 @@ struct RecState {
     DevBuf xyz, type, charge, pop_start, pop_atoms, full_start, full_atoms;
     DevBuf map64[kNumTypes], cmap64[kNumTypes], map32[kNumTypes], cmap32[kNumTypes], map16[kNumTypes];
     bool built[kNumTypes] = {};
+    DevBuf ugrid;  // user grid values, or empty
+    DGeom ug{};
+    double ug_slope = 1e6;
     DevBuf dhdr;  // device copy of the DReceptor header
     DReceptor hdr{};
     void clear_maps() {
@@ -117,7 +120,8 @@ int guarded(sg_engine* e, F f) {
 cudaError_t launch_cell_lists(int, const double*, const int*, const DGeom&, double, const double*, const double*, int*,
                               const int*, int*, int, cudaStream_t);
 cudaError_t launch_grid_map64(const DGeom&, int, const double*, const int*, const double*, const int*, const int*,
-                              const DTables&, const int*, int, double**, double**, cudaStream_t);
+                              const DTables&, const int*, int, double**, double**, const double* ugrid,
+                              const DGeom& ug, double ug_slope, cudaStream_t);
 cudaError_t launch_grid_pack(const DGeom&, const double*, float4*, uint4*, cudaStream_t);
 size_t ws64_bytes(const DModel& hm);
 cudaError_t launch_eval64(const DModel*, size_t, const DTables&, const DReceptor*, int, const double*, const double[3],
@@ -134,7 +138,8 @@ cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DRecept
                             double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
 int mc32_occupancy(int wpb, size_t smem);
-cudaError_t serve_prepare32(size_t smem_fixed);
+cudaError_t mc32_reserve_smem(size_t smem);
+cudaError_t mc32_max_dynamic_smem(size_t optin, size_t* out);
 cudaError_t launch_mc32_fixed(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
                               const Item32*, int nitems, const MCParams32&, unsigned* queue, int blocks, int wpb,
                               size_t stage_stride, size_t ws_stride, size_t smem_fixed, cudaStream_t s);
@@ -160,4 +165,8 @@ void ensure_maps(sg_engine* e, RecState& r, const int* types, int ntypes);
 void ensure_model_maps(sg_engine* e, RecState& r, const PackedModels& pm, const sg_model_desc* models, int nmodels);
 void refresh_header(sg_engine* e, RecState& r);
 void serve_shutdown(sg_engine* e);  // stops the engine's request loop, if one runs
+// chains per block and resident blocks per SM of a k_mc32 launch (honours
+// e->force_wpb)
+void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ);
+void noalloc_claim(sg_engine* e);  // the no-allocation entry point's set-up, at engine creation
 }  // namespace sg

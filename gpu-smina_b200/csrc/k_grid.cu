@@ -11,8 +11,12 @@
 // 2. k_grid_map64: one thread per grid point, FP64 sums over the point's
 //    cell list in receptor order for a chunk of ligand types; identical
 //    rounding to the CPU's loop (each type's sum is independent).
+//    A user grid (--user_grid) is added to every map at the point's index
+//    coordinates (x, y, z), with the cache's slope, as cache::populate does
+//    (cache.cpp:204-205).
 // 3. k_grid_pack: packed-corner FP32 / FP16 copies for the mixed-precision path.
-#include "sg_dev.cuh"
+// Built without FMA contraction, like the CPU code it reproduces.
+#include "grid64.cuh"
 
 namespace sg {
 
@@ -63,7 +67,8 @@ __global__ void k_cell_lists(int natoms, const double* xyz, const int* type, DGe
 __global__ void __launch_bounds__(256) k_grid_map64(DGeom g, int natoms, const double* xyz, const int* rtype,
                                                     const double* rcharge, const int* cstart, const int* catoms,
                                                     const double* fast, int nc, int n, double factor, double cutoff_sqr,
-                                                    const int* types, int ntypes, double** maps, double** cmaps) {
+                                                    const int* types, int ntypes, double** maps, double** cmaps,
+                                                    const double* ugrid, DGeom ug, double ug_slope) {
     const int x = blockIdx.x * 8 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     const int z = blockIdx.z * 4 + threadIdx.z;
@@ -76,6 +81,8 @@ __global__ void __launch_bounds__(256) k_grid_map64(DGeom g, int natoms, const d
     const int cell = cell_ok ? cx + g.cell_dim[0] * (cy + g.cell_dim[1] * cz) : 0;
     const int b = cell_ok ? cstart[cell] : 0, e = cell_ok ? cstart[cell + 1] : 0;
     const size_t idx = (size_t)x + (size_t)g.dim[0] * ((size_t)y + (size_t)g.dim[1] * z);
+    const double u = ugrid ? grid_value64(ug, ugrid, V3<double>{(double)x, (double)y, (double)z}, ug_slope, 1000.0)
+                           : 0.0;
     constexpr int CH = 8;
     for (int t0 = 0; t0 < ntypes; t0 += CH) {
         double aff[CH], chg[CH];
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(256) k_grid_map64(DGeom g, int natoms, const d
             }
         }
         for (int j = 0; j < nt; j++) {
-            maps[t0 + j][idx] = aff[j];
+            maps[t0 + j][idx] = ugrid ? aff[j] + u : aff[j];
             if (nc > 1) cmaps[t0 + j][idx] = chg[j];
         }
     }
@@ -150,11 +157,12 @@ cudaError_t launch_cell_lists(int natoms, const double* xyz, const int* type, co
 
 cudaError_t launch_grid_map64(const DGeom& g, int natoms, const double* xyz, const int* rtype, const double* rcharge,
                               const int* cstart, const int* catoms, const DTables& T, const int* types, int ntypes,
-                              double** maps, double** cmaps, cudaStream_t s) {
+                              double** maps, double** cmaps, const double* ugrid, const DGeom& ug, double ug_slope,
+                              cudaStream_t s) {
     dim3 block(8, 8, 4);
     dim3 grid((g.dim[0] + 7) / 8, (g.dim[1] + 7) / 8, (g.dim[2] + 3) / 4);
     k_grid_map64<<<grid, block, 0, s>>>(g, natoms, xyz, rtype, rcharge, cstart, catoms, T.fast, T.nc, T.n, T.factor,
-                                        T.cutoff_sqr, types, ntypes, maps, cmaps);
+                                        T.cutoff_sqr, types, ntypes, maps, cmaps, ugrid, ug, ug_slope);
     return cudaGetLastError();
 }
 

@@ -50,6 +50,9 @@ struct DReceptor {
     const float4* map32[kNumTypes];      // packed-corner FP32 copies
     const float4* cmap32[kNumTypes];
     const uint4* map16[kNumTypes];       // packed-corner FP16 copies
+    // user grid (--user_grid): its own geometry, values x fastest; null: none
+    const double* ugrid;
+    DGeom ug;
 };
 
 // A docking model packed for the device.  Arrays index into three pools

@@ -136,6 +136,7 @@ def _declare(L):
         "sg_build_grids": [vp, C.c_int, _ip, C.c_int],
         "sg_get_grid": [vp, C.c_int, C.c_int, _dp, _dp],
         "sg_drop_receptor": [vp, C.c_int],
+        "sg_set_user_grid": [vp, C.c_int, C.POINTER(GridDims), _dp, C.c_double],
         "sg_eval": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, _dp, _dp, _dp],
         "sg_eval_direct": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, _dp, C.c_double * 3, C.c_double, _dp, _dp],
         "sg_dock": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(ChainInput), C.c_int,
@@ -465,6 +466,19 @@ class Engine:
 
     def set_receptor(self, rid: int, r: Receptor, gd: GridDims):
         self._check(load().sg_set_receptor(self._h, rid, C.byref(r.desc), C.byref(gd)))
+
+    def set_user_grid(self, rid: int, gd, data, cache_slope=1e6):
+        """sg_set_user_grid: a user grid (--user_grid) over ``gd``, values x
+        fastest; ``data`` None clears it.  Maps built before are dropped."""
+        if data is None or gd is None:
+            self._ug = None
+            self._check(load().sg_set_user_grid(self._h, rid, None, None, cache_slope))
+            return
+        self._ug = np.ascontiguousarray(data, dtype=np.float64).ravel()
+        need = (gd.n[0] + 1) * (gd.n[1] + 1) * (gd.n[2] + 1)
+        if self._ug.size != need:
+            raise ValueError(f"user grid holds {self._ug.size} values, its box needs {need}")
+        self._check(load().sg_set_user_grid(self._h, rid, C.byref(gd), dptr(self._ug), cache_slope))
 
     def build_grids(self, rid: int, types):
         t = np.ascontiguousarray(sorted(set(int(x) for x in types)), dtype=np.int32)

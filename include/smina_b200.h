@@ -14,6 +14,8 @@
  *   sg_set_receptor              ensure_receptor / DeviceGrids::build   src/gpu/gpu_device.cu:199-250
  *                                (cache::populate                       src/lib/cache.cpp:116-206)
  *   sg_build_grids               build_grids_kernel                     src/gpu/gpu_device.cu:133-186
+ *   sg_set_user_grid             the user_grid argument of GpuDocking    src/gpu/gpu_docking.h:71,77,93,107
+ *                                (FlatUserGrid                          src/gpu/gpu_flatten_data.h:90-96)
  *   sg_eval                      eval_confs (model::eval_deriv)          src/gpu/gpu_kernels.h:22-126,
  *                                                                        src/lib/model.cpp:969-985
  *   sg_dock                      run_monte_carlo (monte_carlo::operator()) src/gpu/gpu_kernels_impl.cuh:659-885,
@@ -209,6 +211,17 @@ int sg_build_grids(sg_engine* e, int receptor_id, const int* types, int ntypes);
 int sg_get_grid(sg_engine* e, int receptor_id, int type, double* data, double* chargedata);
 /* Drop a receptor and its maps. */
 int sg_drop_receptor(sg_engine* e, int receptor_id);
+/* A user grid (--user_grid) for receptor `receptor_id`: its own box `gd`
+ * and values data [(n0+1)(n1+1)(n2+1)], x fastest, as smina holds them
+ * after reading the grid file.  It is added to every map at the map point's
+ * index coordinates with `cache_slope` (cache::populate, cache.cpp:204-205),
+ * and to the direct receptor sum at each atom with its derivative
+ * (non_cache::eval_deriv, non_cache.cpp:180-184), so refinement and
+ * sg_minimize see it; the rescoring of sg_score does not (non_cache::eval
+ * has no user-grid term).  gd == NULL or data == NULL clears it.  Maps built
+ * before are dropped and rebuilt on demand. */
+int sg_set_user_grid(sg_engine* e, int receptor_id, const sg_grid_dims* gd, const double* data,
+                     double cache_slope);
 
 /* model::eval_deriv for nconfs confs of one model against receptor maps
  * (cache) of `receptor_id`.  out_e [nconfs], out_g [nconfs][dof],
@@ -328,7 +341,13 @@ int sg_dock_batch32(sg_engine* e, int receptor_id, const sg_model_desc* models, 
  *     (for example 16 ligands of 50 heavy atoms x 8 chains fit);
  *   - the receptor's maps for the ligands' atom types must already be
  *     built (sg_build_grids), since building them allocates;
- *   - the first call on a device looks up the array's device address;
+ *   - the array is claimed when a mixed-precision engine is created
+ *     (sg_create with SG_PREC_FP32 or SG_PREC_FP32_H16): 8 MiB of device
+ *     memory per device, held until the process exits.  Engine creation
+ *     also loads the search kernel and raises its shared-memory limit, so a
+ *     call loads no module and sets no kernel attribute;
+ *   - the launch shape is the one sg_dock_batch32 would pick, including a
+ *     shape set by sg_set_chains_per_block or sg_autotune32;
  *   - every call reuses the same array, so calls that overlap on one GPU
  *     (two engines, or two host threads) corrupt each other: keep them
  *     apart.

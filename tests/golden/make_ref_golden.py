@@ -23,9 +23,10 @@ prints how many values agree bit for bit and the largest difference; with
 
 Cases: default (vina) scoring and the charge-dependent ad4_scoring tables;
 a 1,500-atom receptor with a 14 A box at 0.375 A; ligands of 14/3, 24/5 and
-40/10 heavy atoms/rotors, and the 24/5 ligand with flexible residues; and the
+40/10 heavy atoms/rotors, and the 24/5 ligand with flexible residues; the
 24/5 ligand with a user grid (--user_grid) added to the maps and the direct
-sum.
+sum; and ad4_scoring with seeded partial charges on the receptor, the ligand
+and the flexible residues (ad4_q).
 """
 import argparse
 import ctypes as C
@@ -55,9 +56,14 @@ def cases():
     gd = W.box(14.0)
     lig = [W.ligand(14, 3, 2), W.ligand(24, 5, 11), W.ligand(40, 10, 5)]
     flex = sb.Model(sb.make_ligand_pdbqt(24, 5, 11, W.CENTER), sb.make_flex_pdbqt(4, 3, W.CENTER))
+    # charge-dependent terms with non-zero charges on both sides
+    Rq = W.charged_receptor(1500, 3, 2)
+    flex_q = sb.Model(W.with_charges(sb.make_ligand_pdbqt(24, 5, 11, W.CENTER), 1),
+                      W.with_charges(sb.make_flex_pdbqt(4, 3, W.CENTER), 3))
     return [("vina", W.tables(), R, gd, lig + [flex]),
             ("ad4", sb.Tables("ad4_scoring"), R, gd, [lig[1]]),
-            ("vina_ug", W.tables(), R, gd, [lig[1]])]
+            ("vina_ug", W.tables(), R, gd, [lig[1]]),
+            ("ad4_q", sb.Tables("ad4_scoring"), Rq, gd, [W.charged_ligand(24, 5, 11, 1), flex_q])]
 
 
 def user_grid_for(name, gd):
@@ -332,8 +338,8 @@ def main():
         total, same, worst, key = compare(r, o)
         print(f"{name}: oracle: {same}/{total} values bit-identical to the reference; largest relative "
               f"difference {worst:.3g} ({key or 'none'})", flush=True)
-        if args.engine and ug is None:  # the engine has no user grids yet
-            eng = EngineSide(T, R, gd)
+        if args.engine:
+            eng = EngineSide(T, R, gd, ug)
             g = outputs(eng, T, gd, models, name)
             eng.close()
             total, same, worst, key = compare(r, g)

@@ -237,12 +237,12 @@ def test_score_bit_exact(setup):
 
 @pytest.mark.gpu
 def test_score_charge_dependent_tables_bit_exact():
-    T4, R, gd = sb.Tables("ad4_scoring"), W.receptor(), W.box()
+    T4, R, gd = sb.Tables("ad4_scoring"), W.charged_receptor(), W.box()
     eng = sb.Engine(0, sb.PREC_FP64)
     eng.set_tables(T4)
     eng.set_receptor(0, R, gd)
     orc = Oracle(T4, R, gd, full_cells=True)
-    m = W.ligand(24, 5, 11)
+    m = W.charged_ligand(24, 5, 11)
     confs = W.random_confs(m, gd, 16, 9)
     e1, i1, _ = eng.score(0, [m], [0] * 16, confs)
     e0, i0, _ = orc.score([m], [0] * 16, confs)

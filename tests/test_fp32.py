@@ -38,12 +38,12 @@ def base():
     orc = Oracle(T, R, gd, full_cells=True)
     engines = {}
 
-    def engine(prec, tables=T):
-        key = (prec, id(tables))
+    def engine(prec, tables=T, receptor=R):
+        key = (prec, id(tables), id(receptor))
         if key not in engines:
             e = sb.Engine(0, prec)
             e.set_tables(tables)
-            e.set_receptor(0, R, gd)
+            e.set_receptor(0, receptor, gd)
             engines[key] = e
         return engines[key]
     return engine, orc, gd, R
@@ -103,10 +103,11 @@ def test_eval_fp32_charge_dependent_tables(base):
     """nc = 4 tables (charge-weighted components, charge maps)."""
     engine, _, gd, R = base
     T4 = sb.Tables("ad4_scoring")
-    orc = Oracle(T4, R, gd, full_cells=True)
-    m = W.ligand(24, 5, 11)
+    Rq = W.charged_receptor()
+    orc = Oracle(T4, Rq, gd, full_cells=True)
+    m = W.charged_ligand(24, 5, 11)
     confs = W.random_confs(m, gd, 128, 7)
-    eng = engine(sb.PREC_FP32, T4)
+    eng = engine(sb.PREC_FP32, T4, Rq)
     e32, g32 = eng.eval(0, m, confs)
     e64, g64, x64 = orc.eval(m, confs, coords=True)
     check_fp32(e32, g32, e64, g64, at_discontinuity(m, gd, x64, T4.desc.cutoff_sqr))

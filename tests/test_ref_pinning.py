@@ -8,8 +8,8 @@ written by tests/golden/make_ref_golden.py.  Here every case's inputs are
 rebuilt from their seeds, checked against the recorded SHA-256 digest, and
 the oracle's outputs are compared with the records: grid maps, eval at two
 curl caps, direct eval, BFGS with both line searches, Monte Carlo chains and
-refine_structure, for vina and ad4 tables, a model with flexible residues and a
-user grid.
+refine_structure, for vina and ad4 tables (ad4 also with non-zero partial
+charges), a model with flexible residues and a user grid.
 
 The bar is the reference's own for its FP64 path (gpu_eval_test.cpp:173-210,
 gpu_mc_test.cpp:44-81): relative differences of at most 1e-9 and identical
@@ -60,18 +60,19 @@ def _case(records, case):
     return name, T, R, gd, models, ug
 
 
-@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug"])
+@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug", "ad4_q"])
 def test_oracle_matches_the_reference_device_library(records, case):
     name, T, R, gd, models, _ = _case(records, case)
     _check(records, name, G.outputs(G.oracle_for(name, T, R, gd), T, gd, models, name))
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["vina", "ad4"])
+@pytest.mark.parametrize("case", ["vina", "ad4", "vina_ug", "ad4_q"])
 def test_engine_matches_the_reference_device_library(records, case):
     """This engine's FP64 path (grid maps, eval at both curl caps, direct
     eval, both line searches, 40-step chains, refine; the vina case includes
-    a model with flexible residues) against the same records."""
+    a model with flexible residues, vina_ug a user grid) against the same
+    records."""
     name, T, R, gd, models, ug = _case(records, case)
     side = G.EngineSide(T, R, gd, ug)
     try:

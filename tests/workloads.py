@@ -62,3 +62,40 @@ def random_confs(m, gd, n, seed, spread=None):
         out[k, 3:7] = q
         out[k, 7:] = tors
     return out
+
+
+def with_charges(pdbqt, seed, sd=0.25):
+    """The PDBQT text with seeded partial charges (normal, s.d. `sd`, within
+    +-0.9) in the charge columns of its ATOM lines, so charge-dependent terms
+    see non-zero charges through the reader."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for line in pdbqt.splitlines():
+        if line.startswith(("ATOM", "HETATM")):
+            q = float(np.clip(rng.normal(scale=sd), -0.9, 0.9))
+            line = line[:66] + "    " + f"{q:+6.3f}" + line[76:]
+        out.append(line)
+    return "\n".join(out) + "\n"
+
+
+@functools.lru_cache(maxsize=None)
+def charged_ligand(heavy=24, rotors=5, seed=11, qseed=1):
+    return sb.Model(with_charges(sb.make_ligand_pdbqt(heavy, rotors, seed, CENTER), qseed))
+
+
+class ChargedReceptor:
+    """A synthetic receptor with seeded partial charges (normal, s.d. 0.3,
+    within +-0.9) in place of its zero charges; `desc` is what the engine and
+    the oracle take."""
+
+    def __init__(self, n, seed, qseed):
+        self.base = sb.Receptor(n, seed, CENTER)
+        d = self.base.desc
+        self.q = np.clip(np.random.default_rng(qseed).normal(scale=0.3, size=d.num_atoms), -0.9, 0.9)
+        self.desc = sb.ReceptorDesc(d.num_atoms, d.coords, d.type, sb.dptr(self.q))
+        self.coords, self.types = self.base.coords, self.base.types
+
+
+@functools.lru_cache(maxsize=None)
+def charged_receptor(n=3000, seed=7, qseed=2):
+    return ChargedReceptor(n, seed, qseed)
