@@ -80,6 +80,16 @@ int type_from_ad_name(const std::string& ad) {
     return NumTypes;
 }
 
+// string_to_smina_type (atom_constants.h:294-327): two characters or fewer
+// name an AD4 type, longer names a smina type (atom_type_* scoring terms)
+int type_from_name(const std::string& name) {
+    if (name.size() <= 2) return type_from_ad_name(name);
+    ensure_table();
+    for (int t = 0; t < NumTypes; t++)
+        if (name == g_active[t].name) return t;
+    return NumTypes;
+}
+
 int adjust_type(int t, bool hb, bool het) {
     switch (t) {
         case AliphaticCarbonXSHydrophobe:
@@ -284,10 +294,11 @@ void Scoring::add(const std::string& desc, double w) {
     } else if (name == "non_dir_h_bond") {
         need(3); auto* g = new HBondT; g->g = argval(a[0]); g->b = argval(a[1]); g->cutoff = argval(a[2]); t.reset(g);
     } else if (name == "vdw") {
-        need(5); auto* g = new VdwT; g->i = (int)argval(a[0]); g->j = (int)argval(a[1]); g->s = argval(a[2]);
-        g->cap = argval(a[3]); g->cutoff = argval(a[4]);
-        if (!((g->i == 4 && g->j == 8) || (g->i == 6 && g->j == 12)))
+        need(5); auto* g = new VdwT;
+        const double vi = argval(a[0]), vj = argval(a[1]);
+        if (!((vi == 4 && vj == 8) || (vi == 6 && vj == 12)))
             throw std::runtime_error("Unsupported LJ exponents: try <4,8> or <6,12>.");
+        g->i = (int)vi; g->j = (int)vj; g->s = argval(a[2]); g->cap = argval(a[3]); g->cutoff = argval(a[4]);
         t.reset(g);
     } else if (name == "non_dir_h_bond_lj") {
         need(3); auto* g = new HBondLJT; g->o = argval(a[0]); g->cap = argval(a[1]); g->cutoff = argval(a[2]); t.reset(g);
@@ -296,20 +307,28 @@ void Scoring::add(const std::string& desc, double w) {
         need(2); auto* g = new QuadT; g->o = argval(a[0]); g->cutoff = argval(a[1]);
         g->kind = name[0] == 'n' ? 0 : name[0] == 'd' ? 1 : 2; t.reset(g);
     } else if (name == "electrostatic") {
-        need(3); auto* g = new ElectroT; g->p = (int)argval(a[0]); g->cap = argval(a[1]); g->cutoff = argval(a[2]);
-        if (g->p != 1 && g->p != 2) throw std::runtime_error("Invalid exponent: 1 or 2 only");
+        need(3); auto* g = new ElectroT;
+        const double i = argval(a[0]);
+        if (i != 1 && i != 2) throw std::runtime_error("Invalid exponent: 1 or 2 only");
+        g->p = (int)i; g->cap = argval(a[1]); g->cutoff = argval(a[2]);
         t.reset(g);
     } else if (name == "ad4_solvation") {
         need(3); auto* g = new SolvT; g->sigma = argval(a[0]); g->q = argval(a[1]); g->cutoff = argval(a[2]); t.reset(g);
     } else if (name.rfind("atom_type_", 0) == 0) {
         auto* g = new PairTypeT;
         std::string n1 = argstr(a.at(0)), n2 = argstr(a.at(1));
-        g->a = type_from_ad_name(n1); g->b = type_from_ad_name(n2);
+        g->a = type_from_name(n1); g->b = type_from_name(n2);
         if (g->a == NumTypes || g->b == NumTypes) throw std::runtime_error("Invalid atom type: " + desc);
         if (name == "atom_type_gaussian") { need(5); g->kind = 0; g->p1 = argval(a[2]); g->p2 = argval(a[3]); g->cutoff = argval(a[4]); }
         else if (name == "atom_type_linear") { need(5); g->kind = 1; g->p1 = argval(a[2]); g->p2 = argval(a[3]); g->cutoff = argval(a[4]); }
         else if (name == "atom_type_quadratic") { need(4); g->kind = 2; g->p1 = argval(a[2]); g->cutoff = argval(a[3]); }
-        else if (name == "atom_type_inverse_power") { need(5); g->kind = 3; g->power = (int)argval(a[2]); g->cap = argval(a[3]); g->cutoff = argval(a[4]); }
+        else if (name == "atom_type_inverse_power") {
+            need(5);
+            g->kind = 3;
+            const double i = argval(a[2]);
+            if (i != 1 && i != 2) throw std::runtime_error("Invalid exponent: 1 or 2 only");
+            g->power = (int)i; g->cap = argval(a[3]); g->cutoff = argval(a[4]);
+        }
         else throw std::runtime_error("Unknown term " + desc);
         t.reset(g);
     } else {
@@ -343,6 +362,11 @@ bool builtin_scoring(const std::string& name, Scoring& s) {
         add("ad4_solvation(d-sigma=3.6,_s/q=0.01097,_c=8)", 0.048934);
         add("num_tors_sqr", 0.317267);
         add("constant_term", -2.469020);
+    } else if (name == "dkoes_scoring_old") {
+        add("vdw(i=4,_j=8,_s=0,_^=100,_c=8)", 0.010607);
+        add("non_dir_h_bond(g=-0.7,_b=0,_c=8)", 0.197201);
+        add("num_tors_sqr", .285035);
+        add("constant_term", -2.585651);
     } else if (name == "dkoes_fast") {
         add("vdw(i=4,_j=8,_s=0,_^=100,_c=8)", 0.008962);
         add("non_dir_h_bond(g=-0.7,_b=0,_c=8)", 0.387739);

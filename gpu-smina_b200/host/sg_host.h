@@ -37,6 +37,7 @@ struct TypeInfo {
 const TypeInfo& type_info(int t);
 void use_type_table(bool vinardo);
 int type_from_ad_name(const std::string& ad);  // string_to_smina_type for <= 2 chars
+int type_from_name(const std::string& name);   // string_to_smina_type
 int adjust_type(int t, bool h_bonded, bool hetero_bonded);  // adjust_smina_type
 inline bool is_hydrogen(int t) { return t == Hydrogen || t == PolarHydrogen; }
 

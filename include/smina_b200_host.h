@@ -63,7 +63,7 @@ int  sgh_make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double ce
  * 0 when written, -1 on error. */
 int  sgh_make_flex_pdbqt(int residues, uint64_t seed, const double center[3], double shell, char* buf, int buflen);
 
-/* builtin_name: "vina"/"default", "vinardo", "dkoes_scoring", "dkoes_fast",
+/* builtin_name: "vina"/"default", "vinardo", "dkoes_scoring", "dkoes_scoring_old", "dkoes_fast",
  * "ad4_scoring"; custom_text (if non-empty) takes precedence */
 int  sgh_tables_create(const char* builtin_name, const char* custom_text, double factor, sgh_tables** out);
 void sgh_tables_free(sgh_tables* t);
