@@ -221,94 +221,123 @@ __device__ void bfgs_update64(W64& w, double* h, const double* p, const double* 
 }
 
 // ---- QuickVina 2 history (not smina's search) ----------------------------------------------
-// Follows the reference's restatement of QuickVina 2 (gpu_mc.cuh:144-264;
-// Alhossary et al., Bioinformatics 2015): each chain keeps the last 5n points
-// its local optimisations visited.  A local optimisation runs only if one of
-// the 4n history points nearest its start passes the first-order consistency
-// check; until the history is full every start passes.
-__device__ inline Vis64 vis64_view(double* d, uint32_t* u, int n) {
-    Vis64 v;
-    v.x = d;
-    v.f = v.x + (size_t)5 * n * n;
-    v.now = v.f + 5 * n;
-    v.dist = v.now + n;
-    v.bits = u;
-    v.state = reinterpret_cast<int*>(u + 20 * n);
-    return v;
-}
-__device__ inline bool vis_bit(const uint32_t* b, int i) { return ((i < 32 ? b[0] >> i : b[1] >> (i - 32)) & 1u) != 0; }
+// QuickVina 2 (Alhossary, Handoko, Mu and Kwoh, Bioinformatics 31:2214, 2015)
+// skips a local optimisation whose start the chain's recent history already
+// accounts for.  The history holds the last 5n points (n = dof) that local
+// optimisations visited, with their energies and gradient signs.  A stored
+// point e is consistent with a start (x, f, g) when, in every coordinate in
+// which both gradients have the same nonzero sign, "gradient positive" equals
+// "x_i > e_i" xor "f > f_e".  A start is worth optimising when a consistent
+// point is among its 4n nearest (squared distance in change coordinates,
+// ties to the lower slot); until 5n points are stored, every start is.  The
+// decisions are those of the reference's gpu_mc.cuh:144-264, which the
+// checker restates and this path matches bit for bit.
+//
+// The device layout and the check are this file's own:
+//  - coordinates are stored coordinate-major, so for one coordinate the
+//    lanes read consecutive slots;
+//  - lane l owns slots l, l + 32, ...; their squared distances and "start
+//    above the point" bits build up in registers while the coordinates
+//    stream past (the start's coordinate comes by shuffle), so nothing is
+//    written back but the new point;
+//  - the sign test is mask algebra on 64-bit words: it applies where
+//    nz_e & nz_x & ~(pos_e ^ pos_x), and a point fails when any of those
+//    coordinates has pos_x ^ above ^ uphill set.
+constexpr int kHistSlotsPerLane = (5 * kHistMaxN + 31) / 32;
 
-// visited::add (gpu_mc.cuh:163-205)
-__device__ void vis64_add(W64& w, const Vis64& V, const double* x, double f, const double* g) {
-    const DModel& m = *w.m;
-    const int n = m.dof, cap = 5 * n;
-    int slot = 0;
-    if (w.lane == 0) {
-        int* st = V.state;  // size, next slot, full
-        if (!st[2]) {
-            slot = st[0]++;
-            if (st[0] >= cap) { st[2] = 1; st[1] = 0; }
-        } else {
-            slot = st[1];
-            st[1] = (st[1] + 1) % cap;
-        }
-        V.f[slot] = f;
-        uint32_t zero[2] = {0, 0}, pos[2] = {0, 0};
-        for (int i = 0; i < n; i++)
-            if (g[i] == 0) zero[i >> 5] |= 1u << (i & 31);
-            else if (g[i] > 0) pos[i >> 5] |= 1u << (i & 31);
-        uint32_t* b = V.bits + 4 * slot;
-        b[0] = zero[0]; b[1] = zero[1]; b[2] = pos[0]; b[3] = pos[1];
+__device__ __forceinline__ Hist64 hist64_view(double* d, unsigned long long* u, int n) {
+    const size_t cap = (size_t)5 * n;
+    return Hist64{d, d + (size_t)n * cap, u, u + 2 * cap};
+}
+
+// (nonzero, positive) masks of the gradient's n coordinates, on every lane
+__device__ __forceinline__ ulonglong2 grad_signs64(const W64& w, const double* g, int n) {
+    unsigned nz[2], pos[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int i = 32 * h + w.lane;
+        const double v = i < n ? g[i] : 0.0;
+        nz[h] = __ballot_sync(kFull, !(v == 0));
+        pos[h] = __ballot_sync(kFull, v > 0);
     }
-    slot = __shfl_sync(kFull, slot, 0);
-    for (int i = w.lane; i < n; i += 32) V.x[(size_t)slot * n + i] = conf_value64(m, x, i);
+    return make_ulonglong2(nz[0] | (unsigned long long)nz[1] << 32, pos[0] | (unsigned long long)pos[1] << 32);
+}
+
+// stores (x, f, sign(g)) in the next slot (the oldest point once the ring is full)
+__device__ void hist64_add(W64& w, const Hist64& H, const double* x, double f, const double* g) {
+    const DModel& m = *w.m;
+    const int n = m.dof, cap = 5 * n;
+    const unsigned long long adds = __shfl_sync(kFull, w.lane == 0 ? *H.adds : 0ull, 0);
+    const int slot = (int)(adds % (unsigned long long)cap);
+    const ulonglong2 sg = grad_signs64(w, g, n);
+    for (int i = w.lane; i < n; i += 32) H.x[(size_t)i * cap + slot] = conf_value64(m, x, i);
+    if (w.lane == 0) {
+        H.f[slot] = f;
+        H.mask[2 * slot] = sg.x;
+        H.mask[2 * slot + 1] = sg.y;
+        *H.adds = adds + 1;
+    }
     __syncwarp();
 }
 
-// visited::interesting (gpu_mc.cuh:207-264): the nearest history point that
-// passes the check (lowest index on ties) must rank below 4n by distance
-__device__ bool vis64_interesting(W64& w, const Vis64& V, const double* x, double f, const double* g) {
+// true when a local optimisation from (x, f, g) should run
+__device__ bool hist64_interesting(W64& w, const Hist64& H, const double* x, double f, const double* g) {
     const DModel& m = *w.m;
     const int n = m.dof, cap = 5 * n;
-    const int full = __shfl_sync(kFull, w.lane == 0 ? V.state[2] : 0, 0);
-    if (!full) return true;
-    for (int i = w.lane; i < n; i += 32) V.now[i] = conf_value64(m, x, i);
-    __syncwarp();
+    const unsigned long long adds = __shfl_sync(kFull, w.lane == 0 ? *H.adds : 0ull, 0);
+    if (adds < (unsigned long long)cap) return true;
+    const double x_lo = w.lane < n ? conf_value64(m, x, w.lane) : 0.0;
+    const double x_hi = w.lane + 32 < n ? conf_value64(m, x, w.lane + 32) : 0.0;
+    const ulonglong2 sx = grad_signs64(w, g, n);
+    double d2[kHistSlotsPerLane];
+    unsigned long long above[kHistSlotsPerLane];
+#pragma unroll
+    for (int k = 0; k < kHistSlotsPerLane; k++) { d2[k] = 0; above[k] = 0; }
+    for (int i = 0; i < n; i++) {
+        const double xi = __shfl_sync(kFull, i < 32 ? x_lo : x_hi, i & 31);
+        const double* row = H.x + (size_t)i * cap;
+#pragma unroll
+        for (int k = 0; k < kHistSlotsPerLane; k++) {
+            const int e = w.lane + 32 * k;
+            if (e < cap) {
+                const double dx = row[e] - xi;  // summed in coordinate order
+                d2[k] += dx * dx;
+                if (dx < 0) above[k] |= 1ull << i;
+            }
+        }
+    }
+    // nearest consistent point, in (distance, slot) order
     double best = kMaxFl;
     int besti = cap;
-    for (int e = w.lane; e < cap; e += 32) {
-        const double* xe = V.x + (size_t)e * n;
-        const uint32_t* b = V.bits + 4 * e;
-        const bool newY = f - V.f[e] > 0;
-        double d2 = 0;
-        bool pass = true;
-        for (int i = 0; i < n; i++) {
-            const double dx = xe[i] - V.now[i];
-            d2 += dx * dx;
-            if (vis_bit(b, i) || g[i] == 0) continue;
-            const bool nowPos = g[i] > 0;
-            if (nowPos != vis_bit(b + 2, i)) continue;
-            const bool newX = V.now[i] - xe[i] > 0;
-            if (nowPos ^ newX ^ newY) pass = false;
+#pragma unroll
+    for (int k = 0; k < kHistSlotsPerLane; k++) {
+        const int e = w.lane + 32 * k;
+        if (e < cap) {
+            const unsigned long long nz = H.mask[2 * e], pos = H.mask[2 * e + 1];
+            const unsigned long long uphill = f - H.f[e] > 0 ? ~0ull : 0ull;
+            const unsigned long long applies = nz & sx.x & ~(pos ^ sx.y);
+            if ((applies & (sx.y ^ above[k] ^ uphill)) == 0 && d2[k] < best) { best = d2[k]; besti = e; }
         }
-        V.dist[e] = d2;
-        if (pass && d2 < best) { best = d2; besti = e; }
     }
-    for (int o = 16; o > 0; o >>= 1) {  // argmin of (best, index)
+    for (int o = 16; o > 0; o >>= 1) {
         const double ob = __shfl_xor_sync(kFull, best, o);
         const int oi = __shfl_xor_sync(kFull, besti, o);
         if (ob < best || (ob == best && oi < besti)) { best = ob; besti = oi; }
     }
     if (besti >= cap) return false;
-    __syncwarp();
+    // its rank: the points strictly before it in (distance, slot) order
     int ahead = 0;
-    for (int e = w.lane; e < cap; e += 32) ahead += (V.dist[e] < best || (V.dist[e] == best && e < besti));
+#pragma unroll
+    for (int k = 0; k < kHistSlotsPerLane; k++) {
+        const int e = w.lane + 32 * k;
+        if (e < cap) ahead += d2[k] < best || (d2[k] == best && e < besti);
+    }
     for (int o = 16; o > 0; o >>= 1) ahead += __shfl_xor_sync(kFull, ahead, o);
     return ahead < 4 * n;
 }
 
 __device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int early, const EvalMode& em,
-                         const Vis64* vis = nullptr) {
+                         const Hist64* vis = nullptr) {
     const DModel& m = *w.m;
     const int n = m.dof;
     double* S = w.s;
@@ -321,8 +350,8 @@ __device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int earl
     __syncwarp();
     double f0 = feval(w, x, g, em);
     if (vis) {
-        if (!vis64_interesting(w, *vis, x, f0, g)) return f0;
-        vis64_add(w, *vis, x, f0, g);
+        if (!hist64_interesting(w, *vis, x, f0, g)) return f0;
+        hist64_add(w, *vis, x, f0, g);
     }
     const double f_orig = f0;
     vcopy(w, g_orig, g, n);
@@ -351,7 +380,7 @@ __device__ double bfgs64(W64& w, double* x, int maxiters, int accurate, int earl
             }
         }
         bfgs_update64(w, h, p, y, alpha, n);
-        if (vis) vis64_add(w, *vis, x, f0, g);
+        if (vis) hist64_add(w, *vis, x, f0, g);
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;

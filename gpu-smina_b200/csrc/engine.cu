@@ -895,26 +895,27 @@ int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, con
             nxyz_res += (size_t)S * h.nheavy * 3;
             require(out[k].e && out[k].conf && out[k].coords, "dock: null result arrays");
         }
-        Staged<double> d_conf0, d_e, d_conf, d_xyz, d_vis;
-        Staged<uint32_t> d_mt, d_visw;
+        Staged<double> d_conf0, d_e, d_conf, d_xyz, d_hist;
+        Staged<uint32_t> d_mt;
+        Staged<unsigned long long> d_histw;
         Staged<int> d_order, d_count;
         Staged<unsigned long long> d_evals;
         // QuickVina 2 histories (MCParams::visited), one block per chain whose dof fits
-        std::vector<size_t> vis_off(nchains, SIZE_MAX), visw_off(nchains, SIZE_MAX);
-        size_t nvis = 0, nvisw = 0;
+        std::vector<size_t> hist_off(nchains, SIZE_MAX), histw_off(nchains, SIZE_MAX);
+        size_t nhist = 0, nhistw = 0;
         if (p->visited)
             for (int k = 0; k < nchains; k++) {
                 const int n = pm.host[chains[k].model].dof;
-                if (n > kVisMaxN) continue;
-                vis_off[k] = nvis;
-                visw_off[k] = nvisw;
-                nvis += vis64_doubles(n);
-                nvisw += vis64_words(n);
+                if (n > kHistMaxN) continue;
+                hist_off[k] = nhist;
+                histw_off[k] = nhistw;
+                nhist += hist64_doubles(n);
+                nhistw += hist64_words(n);
             }
-        if (nvis) {
-            d_vis.make(nvis, e->stream);
-            d_visw.make(nvisw, e->stream);
-            d_visw.zero(e->stream);  // empty histories
+        if (nhist) {
+            d_hist.make(nhist, e->stream);
+            d_histw.make(nhistw, e->stream);
+            d_histw.zero(e->stream);  // empty histories
         }
         d_conf0.make(conf0.size(), e->stream, conf0.data());
         d_mt.make(mt.size(), e->stream, mt.data());
@@ -937,8 +938,8 @@ int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, con
             hc[k].out_order = d_order.p() + (size_t)k * S;
             hc[k].out_count = d_count.p() + k;
             hc[k].evals = d_evals.p() + k;
-            hc[k].vis = vis_off[k] == SIZE_MAX ? nullptr : d_vis.p() + vis_off[k];
-            hc[k].vis_words = visw_off[k] == SIZE_MAX ? nullptr : d_visw.p() + visw_off[k];
+            hc[k].hist = hist_off[k] == SIZE_MAX ? nullptr : d_hist.p() + hist_off[k];
+            hc[k].hist_words = histw_off[k] == SIZE_MAX ? nullptr : d_histw.p() + histw_off[k];
         }
         DevBuf d_chains;
         d_chains.upload(hc.data(), hc.size() * sizeof(Chain64), e->stream);
@@ -954,7 +955,7 @@ int sg_dock(sg_engine* e, int rid, const sg_model_desc* models, int nmodels, con
         P.early_term = p->early_term;
         P.slope = p->cache_slope;
         cuda_check(launch_mc64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(),
-                               d_chains.as<Chain64>(), nchains, P, nvis > 0, e->d_err.as<int>(), e->stream),
+                               d_chains.as<Chain64>(), nchains, P, nhist > 0, e->d_err.as<int>(), e->stream),
                    "dock launch");
         std::vector<double> he((size_t)nchains * S), hconf(nconf_res), hxyz(nxyz_res);
         std::vector<int> horder((size_t)nchains * S), hcount(nchains);

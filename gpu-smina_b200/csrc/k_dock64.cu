@@ -90,11 +90,11 @@ __global__ void __launch_bounds__(32) k_mc64(const DModel* models, DTables T, co
     __syncwarp();
     const EvalMode hunt{{P.hunt[0], P.hunt[1], P.hunt[2]}, P.slope, false};
     const EvalMode auth{{P.auth[0], P.auth[1], P.auth[2]}, P.slope, false};
-    Vis64 vis_store{};
-    const Vis64* vis = nullptr;
-    if (VIS && ch.vis && m.dof <= kVisMaxN) {
-        vis_store = vis64_view(ch.vis, ch.vis_words, m.dof);
-        vis = &vis_store;
+    Hist64 hist_store{};
+    const Hist64* vis = nullptr;
+    if (VIS && ch.hist && m.dof <= kHistMaxN) {
+        hist_store = hist64_view(ch.hist, ch.hist_words, m.dof);
+        vis = &hist_store;
     }
     double tmp_e = 0, best_e = kMaxFl;
     for (unsigned step = 0; step < ch.steps; step++) {

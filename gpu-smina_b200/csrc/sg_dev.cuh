@@ -273,28 +273,28 @@ SG_HD Ws64 ws64_layout(int natoms, int nframes, int npairs, int conf, int dof) {
 }
 
 // Chain bookkeeping for the plain path (global memory)
-// A chain's QuickVina 2 history (plain path, MCParams::visited): 5n points
-// of n change coordinates, their energies, the zero and positive bits of their
-// gradients, and the ring state (size, next slot, full); scratch for the
-// point being checked and the distances.  n <= kVisMaxN.
-constexpr int kVisMaxN = 64;
-struct Vis64 {
-    double* x;        // [5n][n]
-    double* f;        // [5n]
-    double* now;      // [n]
-    double* dist;     // [5n]
-    uint32_t* bits;   // [5n][4]: zero bits (2 words), positive bits (2 words)
-    int* state;       // [3]
+// A chain's QuickVina 2 history (plain path, MCParams::visited) over n <=
+// kHistMaxN change coordinates: the last 5n points, stored coordinate-major
+// (coordinate i of slot e at x[i * 5n + e]), their energies, two gradient-sign
+// masks per point (bit i: gradient i nonzero / positive) and the count of
+// points added so far (the next slot is that count mod 5n; the ring is full
+// once it reaches 5n).  Only the count needs zeroing before a chain starts.
+constexpr int kHistMaxN = 64;
+struct Hist64 {
+    double* x;                 // [n][5n]
+    double* f;                 // [5n]
+    unsigned long long* mask;  // [5n][2]: nonzero, positive
+    unsigned long long* adds;  // [1]
 };
-SG_HD size_t vis64_doubles(int n) { return (size_t)5 * n * n + 5 * n + n + 5 * n; }
-SG_HD size_t vis64_words(int n) { return (size_t)20 * n + 4; }
+SG_HD size_t hist64_doubles(int n) { return (size_t)5 * n * (n + 1); }
+SG_HD size_t hist64_words(int n) { return (size_t)10 * n + 1; }
 
 struct Chain64 {
     int model;
     unsigned steps;
     int maxiters;
-    double* vis;         // history doubles (vis64_doubles(dof)), or null: no history
-    uint32_t* vis_words; // history words (vis64_words(dof), zeroed)
+    double* hist;                    // history doubles (hist64_doubles(dof)), or null: no history
+    unsigned long long* hist_words;  // history masks and count (hist64_words(dof), zeroed)
     const double* conf0;
     uint32_t* mt;        // [625] state (read + written)
     double* out_e;       // [num_saved]
