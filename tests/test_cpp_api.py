@@ -30,3 +30,14 @@ def test_cpp_interface_without_a_device(tmp_path):
     r = subprocess.run([exe, "host"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "0 failure(s)" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cpp_interface_on_the_device(tmp_path):
+    """parallel_mc (FP32 and FP64 engines), dock_batch, refine and
+    minimize_batch through the GpuDocking-shaped class give, bit for bit,
+    what the same work gives through the C ABI directly."""
+    exe = _build(tmp_path)
+    r = subprocess.run([exe, "device"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "device: 0 failure(s)" in r.stdout
