@@ -145,9 +145,12 @@ def cpu_sample(models, gd, receptor, tables, exh, seed, nlig, threads, parallel=
 def run_accuracy(args):
     """Top-score agreement of the batched FP32 search with the plain FP64
     search on a sample of the screen (smina's full step counts, exhaustiveness
-    8, merge + FP64 refinement on both sides).  Reports the spread of
-    best-energy differences FP32 - FP64 next to the seed-to-seed spread of
-    FP64 itself (two FP64 runs with different seeds)."""
+    8, merge + FP64 refinement on both sides), each path run with
+    --acc-seeds seeds.  Reports the spread of best-energy differences FP32 -
+    FP64 (every FP32 run against every FP64 run) next to the seed-to-seed
+    spreads of FP64 and of FP32 (every pair of runs of one path), per-ligand
+    spreads over the seeds with a Wilcoxon signed-rank test, and ligand
+    bootstrap intervals of the spread ratios."""
     spec = screen(args.ligands, args.seed)
     idx = [int(i) for i in np.linspace(0, len(spec) - 1, args.accuracy)]
     models = build_models([spec[i] for i in idx])
@@ -190,31 +193,70 @@ def run_accuracy(args):
             out.append(float(np.min(er)))
         return np.array(out), time.perf_counter() - t0
 
-    a64, t_a = best64(args.seed)
-    b64, t_b = best64(args.seed + 7919)
-    jobs = jobs_for(models, list(range(len(models))), exh, args.seed, 0)
-    t0 = time.perf_counter()
-    r32 = e32.dock_batch(0, models, jobs, p, refine=True)
-    t32 = time.perf_counter() - t0
-    a32 = np.array([float(r["e"][0]) for r in r32])
-    r32b = e32.dock_batch(0, models, jobs_for(models, list(range(len(models))), exh, args.seed + 7919, 0), p,
-                          refine=True)
-    b32 = np.array([float(r["e"][0]) for r in r32b])
-    d32, d64, d3232 = a32 - a64, b64 - a64, b32 - a32
+    K = max(2, args.acc_seeds)
+    seeds = [args.seed + 7919 * k for k in range(K)]
+    A64, t64 = [], []
+    for sd in seeds:
+        v, t = best64(sd)
+        A64.append(v)
+        t64.append(t)
+    A32, t32 = [], []
+    for sd in seeds:
+        jobs = jobs_for(models, list(range(len(models))), exh, sd, 0)
+        t0 = time.perf_counter()
+        r32 = e32.dock_batch(0, models, jobs, p, refine=True)
+        t32.append(time.perf_counter() - t0)
+        A32.append(np.array([float(r["e"][0]) for r in r32]))
+    A64, A32 = np.array(A64), np.array(A32)
+
+    def spread(X, Y, pairs):
+        d = np.concatenate([X[k] - Y[l] for k, l in pairs])
+        return {"mean": float(d.mean()), "sd": float(d.std(ddof=1)), "median_abs": float(np.median(np.abs(d))),
+                "pairs": len(pairs)}
+
+    within = [(k, l) for k in range(K) for l in range(K) if k < l]
+    cross = [(k, l) for k in range(K) for l in range(K)]
+    s64 = A64.std(axis=0, ddof=1)  # per-ligand spread over seeds
+    s32 = A32.std(axis=0, ddof=1)
+    rng = np.random.default_rng(1)
+    boot_w, boot_c = [], []
+    for _ in range(2000):  # ligands resampled with replacement
+        i = rng.integers(0, len(models), len(models))
+        ww64 = np.concatenate([A64[k, i] - A64[l, i] for k, l in within]).std(ddof=1)
+        ww32 = np.concatenate([A32[k, i] - A32[l, i] for k, l in within]).std(ddof=1)
+        cc = np.concatenate([A32[k, i] - A64[l, i] for k, l in cross]).std(ddof=1)
+        boot_w.append(ww32 / ww64)
+        boot_c.append(cc / ww64)
+    try:
+        from scipy.stats import wilcoxon
+        p_w = float(wilcoxon(s32, s64).pvalue)
+    except Exception:
+        p_w = None
     print(json.dumps({
         "accuracy": f"top-score agreement, {len(models)} ligands spread over the screen, full smina steps, "
-                    f"exhaustiveness {exh}, merge + FP64 refine on both sides",
+                    f"exhaustiveness {exh}, merge + FP64 refine on both sides, {K} seeds per path",
         "precision": args.precision,
-        "fp32_minus_fp64": {"mean": float(d32.mean()), "sd": float(d32.std(ddof=1)),
-                            "median_abs": float(np.median(np.abs(d32)))},
-        "fp64_seed_to_seed": {"mean": float(d64.mean()), "sd": float(d64.std(ddof=1)),
-                              "median_abs": float(np.median(np.abs(d64)))},
-        "fp32_seed_to_seed": {"mean": float(d3232.mean()), "sd": float(d3232.std(ddof=1)),
-                              "median_abs": float(np.median(np.abs(d3232)))},
-        "fp32_seed_b_minus_fp64": {"mean": float((b32 - a64).mean()), "sd": float((b32 - a64).std(ddof=1))},
-        "best_energy_mean": {"fp32": float(a32.mean()), "fp64": float(a64.mean())},
-        "wall_s": {"fp64_run": t_a, "fp64_run_2": t_b, "fp32_batched": t32},
-        "ligands_per_s": {"fp64_plain": len(models) / t_a, "fp32_batched": len(models) / t32},
+        "target_sd_kcal_mol": 0.08,
+        "fp32_minus_fp64": spread(A32, A64, cross),
+        "fp64_seed_to_seed": spread(A64, A64, within),
+        "fp32_seed_to_seed": spread(A32, A32, within),
+        "sd_ratio_fp32_seed_to_seed_over_fp64": {
+            "value": float(spread(A32, A32, within)["sd"] / spread(A64, A64, within)["sd"]),
+            "ci95_ligand_bootstrap": [float(np.percentile(boot_w, 2.5)), float(np.percentile(boot_w, 97.5))]},
+        "sd_ratio_fp32_minus_fp64_over_fp64_seed_to_seed": {
+            "value": float(spread(A32, A64, cross)["sd"] / spread(A64, A64, within)["sd"]),
+            "ci95_ligand_bootstrap": [float(np.percentile(boot_c, 2.5)), float(np.percentile(boot_c, 97.5))]},
+        "per_ligand_sd_over_seeds": {"fp64_median": float(np.median(s64)), "fp32_median": float(np.median(s32)),
+                                     "fp64_mean": float(s64.mean()), "fp32_mean": float(s32.mean()),
+                                     "fraction_fp32_above": float((s32 > s64).mean()),
+                                     "wilcoxon_p": p_w},
+        "per_ligand_mean_fp32_minus_fp64": {"mean": float((A32.mean(0) - A64.mean(0)).mean()),
+                                            "sd": float((A32.mean(0) - A64.mean(0)).std(ddof=1))},
+        "best_energy_mean": {"fp32": float(A32.mean()), "fp64": float(A64.mean())},
+        "wall_s": {"fp64_runs": t64, "fp32_runs": t32},
+        "ligands_per_s": {"fp64_plain": len(models) / float(np.mean(t64)),
+                          "fp32_batched": len(models) / float(np.mean(t32))},
+        "best_energies": {"fp64": A64.round(4).tolist(), "fp32": A32.round(4).tolist()},
     }), flush=True)
 
 
@@ -272,6 +314,112 @@ def run_plain64(args):
                                f"3000 heavy atoms, 22 A box at 0.375 A, exhaustiveness {exh}, smina step counts"
                                + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
                                + ", all chains in one launch, merge + FP64 refine per ligand"},
+        "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }), flush=True)
+
+
+# config 5's custom scoring: the five distance terms of vina with user weights
+CUSTOM_FLEX = ("-0.0400 gauss(o=0,_w=0.5,_c=8)\n-0.0060 gauss(o=3,_w=2,_c=8)\n0.8000 repulsion(o=0,_c=8)\n"
+               "-0.0300 hydrophobic(g=0.5,_b=1.5,_c=8)\n-0.5500 non_dir_h_bond(g=-0.7,_b=0,_c=8)\n"
+               "1.923 num_tors_div\n")
+
+
+def run_flex(args):
+    """Flexible residues, custom scoring and FP16 maps: ligands drawn from the
+    20,000-ligand screen (heavy atoms U[10,50], rotors U[0,12]) docked with
+    4 synthetic flexible side chains (2-4 chi torsions each) next to the
+    cavity of the 3,000-atom receptor, a custom scoring file (vina's five
+    distance terms with user weights), grid maps stored in FP16 and
+    interpolated in FP32.  Times ``args.flex_screen`` evenly spaced ligands
+    of that screen through the batched search (merge + FP64 refinement) and
+    extrapolates to 20,000; then, on the first ``args.flex_acc`` of them,
+    compares the top refined energies of the FP16 search with the plain FP64
+    search (two seeds each, so FP64's own seed-to-seed spread stands beside
+    the difference)."""
+    spec = screen(20000, args.seed)
+    idx = [int(i) for i in np.linspace(0, len(spec) - 1, args.flex_screen)]
+    flex = sb.make_flex_pdbqt(4, args.seed, CENTER)
+    models = [sb.Model(sb.make_ligand_pdbqt(*spec[i][:2], spec[i][2], CENTER), flex) for i in idx]
+    R = sb.Receptor(3000, 7, CENTER)
+    T = sb.Tables("vina", CUSTOM_FLEX)
+    gd = sb.make_box(CENTER, (22.0, 22.0, 22.0))
+    types = sorted({t for m in models for t in m.types() if 1 < t < 27})
+    e16 = sb.Engine(0, sb.PREC_FP32_H16)
+    e16.set_tables(T)
+    e16.set_receptor(0, R, gd)
+    e16.build_grids(0, types)
+    p = make_params(models)
+    exh = args.exhaustiveness
+    jobs = jobs_for(models, list(range(len(models))), exh, args.seed, 0, args.step_scale)
+    e16.dock_batch(0, models[:2], jobs_for(models, [0, 1], exh, args.seed, 0, 0.01), p, refine=True)  # warm-up
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        r16 = e16.dock_batch(0, models, jobs, p, refine=True)
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+    lps = len(models) / wall
+    # accuracy on a subsample: FP16 batched (two seeds) against plain FP64 (two seeds)
+    na = min(args.flex_acc, len(models))
+    sub = models[:na]
+    e64 = sb.Engine(0, sb.PREC_FP64)
+    e64.set_tables(T)
+    e64.set_receptor(0, R, gd)
+    e64.build_grids(0, types)
+    cmax = max(m.conf_size for m in sub)
+
+    def best64(seed):
+        confs, mts, moc, steps, its = [], [], [], [], []
+        for k, m in enumerate(sub):
+            sp = m.search_params(9)
+            c, mt = m.seed_chains(seed + k, exh, gd)
+            cm = np.zeros((exh, cmax))
+            cm[:, :m.conf_size] = c
+            confs += list(cm)
+            mts += list(mt)
+            moc += [k] * exh
+            n = max(1, int(sp.num_steps * args.step_scale)) if args.step_scale != 1.0 else sp.num_steps
+            steps += [n] * exh
+            its += [sp.maxiters] * exh
+        b = e64.dock(0, sub, moc, confs, mts, p, steps=steps, maxiters=its)
+        out = []
+        for k, m in enumerate(sub):
+            sp = m.search_params(9)
+            e, conf, _ = sb.merge_chains(b, m, first=exh * k, n=exh, max_size=p.num_saved_mins)
+            _, er, _ = e64.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v),
+                                  maxiters=sp.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
+            out.append(float(np.min(er)))
+        return np.array(out)
+
+    t1 = time.perf_counter()
+    a64, b64 = best64(args.seed), best64(args.seed + 7919)
+    t64 = (time.perf_counter() - t1) / 2
+    a16 = np.array([float(r["e"][0]) for r in r16[:na]])
+    r16b = e16.dock_batch(0, sub, jobs_for(sub, list(range(na)), exh, args.seed + 7919, 0, args.step_scale), p,
+                          refine=True)
+    b16 = np.array([float(r["e"][0]) for r in r16b])
+    d_cross = np.concatenate([a16 - a64, a16 - b64, b16 - a64, b16 - b64])
+
+    def st(d):
+        return {"mean": float(d.mean()), "sd": float(d.std(ddof=1)), "median_abs": float(np.median(np.abs(d)))}
+
+    evals = int(sum(r["evals"] for r in r16))
+    print(json.dumps({
+        "mode": "flex_fp16_custom", "metric": "ligands docked/sec, flexible residues + custom scoring + FP16 maps",
+        "value": lps, "unit": UNIT, "n_gpus": 1, "dtype": "f32 (f16 maps)", "data": "synthetic",
+        "ligands_timed": len(models), "wall_s": wall, "evals_per_s": evals / wall,
+        "extrapolated_20000_ligands_s": 20000 / lps,
+        "flex": {"residues": 4, "torsions_added": int(models[0].dof - 6 - models[0].torsdof)},
+        "accuracy": {"ligands": na, "seeds_per_path": 2,
+                     "fp16_minus_fp64": st(d_cross), "fp64_seed_to_seed": st(b64 - a64),
+                     "fp16_seed_to_seed": st(b16 - a16), "target_sd_kcal_mol": 0.08,
+                     "best_energy_mean": {"fp16": float(np.concatenate([a16, b16]).mean()),
+                                          "fp64": float(np.concatenate([a64, b64]).mean())},
+                     "fp64_wall_s_per_run": t64},
+        "config": {"workload": f"{len(models)} of a 20,000-ligand screen (heavy U[10,50], rotors U[0,12]) with 4 "
+                               "flexible side chains (2-4 chi each), receptor 3000 heavy atoms, 22 A box at 0.375 A, "
+                               f"custom scoring (vina's five terms, user weights), FP16 maps, exhaustiveness {exh}, "
+                               "smina step counts" + (f" x {args.step_scale}" if args.step_scale != 1.0 else "")
+                               + ", one persistent launch, merge + FP64 refine"},
         "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
     }), flush=True)
 
@@ -652,6 +800,7 @@ def main():
                     help="scale every ligand's Monte Carlo step count (profiling cases; 1 = smina's counts)")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="instead of timing: top-score agreement FP32 vs FP64 on this many ligands")
+    ap.add_argument("--acc-seeds", type=int, default=4, help="with --accuracy: seeds per path (at least 2)")
     ap.add_argument("--serve", type=int, default=0,
                     help="instead of the screen: this many requests through the serving loop (p50/p99 latency)")
     ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
@@ -664,6 +813,10 @@ def main():
     ap.add_argument("--ref-gpu", action="store_true",
                     help="instead of timing: the reference's own FP32 GPU search (built from its sources into "
                          "baseline/_ref) beside this engine's, on the same screen")
+    ap.add_argument("--flex-screen", type=int, default=0,
+                    help="instead of timing the screen: this many ligands of the 20,000-ligand screen with 4 flexible "
+                         "residues, custom scoring and FP16 maps, plus an accuracy check against FP64")
+    ap.add_argument("--flex-acc", type=int, default=24, help="with --flex-screen: ligands in the FP64 comparison")
     ap.add_argument("--redock", type=int, default=0,
                     help="instead of timing: the single-ligand redock (FP64 exhaustiveness 8, FP32 exhaustiveness "
                          "128) with this many seeds; top-pose energy and RMSD differences")
@@ -674,6 +827,9 @@ def main():
         return
     if args.redock:
         run_redock(args)
+        return
+    if args.flex_screen:
+        run_flex(args)
         return
     if args.ref_gpu:
         run_ref_gpu(args)
