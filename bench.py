@@ -667,8 +667,8 @@ def run_serve(args):
     for j in jobs:
         j.model = 0
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
-    eng.serve_start()
-    lat, evals = {}, 0
+    eng.serve_start(block_smem_bytes=args.serve_block_smem)
+    lat, evals, dev = {}, 0, {}
     k = 0
     occupancy = []  # (queued, ligands in flight) sampled every 100 ms
     next_sample = 0.0
@@ -684,21 +684,27 @@ def run_serve(args):
                 occupancy.append((st["queued"], st["inflight"]))
                 next_sample = now + 0.1
             wait = 1 if k < n else 20
-            for (t, st, cnt, ms, ev, cs, nh) in eng.serve_poll(256, wait_ms=wait):
+            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1) in eng.serve_poll(256, wait_ms=wait, spans=True):
                 if st != 0:
                     raise RuntimeError(f"request {t} failed with status {st}")
                 eng.serve_fetch(t, cnt, cs, nh)
                 lat[t] = ms
+                dev[t] = (launch, d0, d1)
                 evals += ev
         wall = time.perf_counter() - t0
     eng.serve_stop()
     v = np.array(list(lat.values()))
+    dms = np.array([(d1 - d0) / 1e6 for (_, d0, d1) in dev.values()])
+    launches = len({l for (l, _, _) in dev.values()})
     clocks = clk.summary()
     print(json.dumps({
         "mode": "serve", "metric": "request latency (p50/p99) and ligands/s under Poisson arrivals",
         "value": n / wall, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
         "latency_ms": {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
                        "max": float(v.max()), "mean": float(v.mean())},
+        "device_search_ms": {"p50": float(np.percentile(dms, 50)), "p99": float(np.percentile(dms, 99)),
+                             "mean": float(dms.mean())},
+        "launches": launches,
         "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
         "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),
                              "max": int(max(o[1] for o in occupancy))},
@@ -708,7 +714,8 @@ def run_serve(args):
                                f"{[r[0] for r in SERVE_RECEPTORS]} heavy atoms in {[r[1] for r in SERVE_RECEPTORS]} A "
                                f"boxes at 0.375 A, exhaustiveness {args.exhaustiveness}, smina step counts"
                                + (f" x {args.step_scale}" if args.step_scale != 1.0 else ""),
-                   "precision": args.precision, "arrivals": f"Poisson, seed {args.seed}"},
+                   "precision": args.precision, "arrivals": f"Poisson, seed {args.seed}",
+                   "block_smem_bytes": args.serve_block_smem or "automatic"},
         "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
     }), flush=True)
 
@@ -804,6 +811,8 @@ def main():
     ap.add_argument("--serve", type=int, default=0,
                     help="instead of the screen: this many requests through the serving loop (p50/p99 latency)")
     ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
+    ap.add_argument("--serve-block-smem", type=int, default=0,
+                    help="with --serve: dynamic shared memory per search block (0: the server's default)")
     ap.add_argument("--plain64", action="store_true",
                     help="instead of the batched search: the same screen through the plain FP64 path")
     ap.add_argument("--visited", action="store_true",
@@ -920,6 +929,10 @@ def main():
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get("bytes_per_launch")
     evals = sum(r[2]["evals"] for r in recs)
+    accuracy = None  # top-score agreement with the FP64 search, measured by the command it names
+    af = os.path.join(ROOT, "profiles", "accuracy_fp32_vs_fp64_screen120.json")
+    if os.path.exists(af):
+        accuracy = json.load(open(af))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = args.exhaustiveness
@@ -951,6 +964,7 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k_mc32"},
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "evals_per_s": evals / mc_s,
             "search_ms_per_step": 1000 * mc_s / args.steps,
         }), flush=True)
