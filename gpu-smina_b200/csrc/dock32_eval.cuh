@@ -113,6 +113,13 @@ __device__ __forceinline__ W32 here() {
     return W32{sWs0 + (int)(threadIdx.x >> 5) * sWsStride, (int)(threadIdx.x & 31)};
 }
 
+// the device's nanosecond clock (%globaltimer), comparable across launches
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }

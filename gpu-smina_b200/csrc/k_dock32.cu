@@ -474,6 +474,7 @@ __device__ __forceinline__ int add_output32(const W32& w, const Chain32& ch, con
 __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P) {
     SG_T0(t_chain);
     const W32 w = here();
+    if (ch.span && w.lane == 0) ch.span[0] = global_ns();
     const SModel& m = smodel();
     const Ws32& L = m.L;
     unsigned* C = w.counters();
@@ -523,6 +524,7 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
         *ch.evals = C[64];
         ch.hits[0] = gh;
         ch.hits[1] = ph;
+        if (ch.span) ch.span[1] = global_ns();
         if (ch.done_count) {
             __threadfence();  // this chain's results, before its count
             if (atomicAdd(ch.done_count, 1u) + 1 == (unsigned)ch.lig_chains) {
@@ -652,6 +654,30 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
         }
 }
 
+// quasi_newton for a batch of confs of one model with the search's own
+// mixed-precision BFGS (one warp per conf); confs are optimised in place
+__global__ void __launch_bounds__(32) k_bfgs32(const DModel* model, DTables32 T, DMaps32 G, int n, double* confs,
+                                               float v0, float v1, float v2, float slope, int maxiters, int accurate,
+                                               int early, double* out_e, int ws_at) {
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = 0; }
+    stage_model(model, threadIdx.x, 32);
+    const W32 w = here();
+    const SModel& m = smodel();
+    const Ws32& L = m.L;
+    unsigned* C = w.counters();
+    for (int i = w.lane; i < 65; i += 32) C[i] = 0;
+    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);  // inflex atoms stay here
+    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
+    double* c = confs + (size_t)k * m.conf_size;
+    copyd(w, w.d(L.x_tmp), c, m.conf_size);
+    const double e = bfgs32(w.at(L.x_tmp), maxiters, accurate, early, Mode32{make_float3(v0, v1, v2), slope});
+    const double* x = w.d(L.x_tmp);
+    for (int i = w.lane; i < m.conf_size; i += 32) c[i] = x[i];
+    if (w.lane == 0) out_e[k] = e;
+}
+
 // ---- host launchers -----------------------------------------------------------------------
 size_t ws32_bytes(const DModel& hm) {
     return (size_t)ws32_layout(hm.natoms, hm.nframes, hm.conf_size, hm.dof).total;
@@ -725,6 +751,17 @@ cudaError_t launch_eval32(const DModel* dm, size_t stage, size_t ws, const DTabl
     if (rc != cudaSuccess) return rc;
     k_eval32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, e, g, coords,
                                  (int)stage);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bfgs32(const DModel* dm, size_t stage, size_t ws, const DTables32& T, const DMaps32& G, int n,
+                          double* confs, const double v[3], double slope, int maxiters, int accurate, int early,
+                          double* e, cudaStream_t s) {
+    const size_t smem = stage + ws;
+    cudaError_t rc = prep32((const void*)k_bfgs32, smem);
+    if (rc != cudaSuccess) return rc;
+    k_bfgs32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, maxiters,
+                                 accurate, early, e, (int)stage);
     return cudaGetLastError();
 }
 

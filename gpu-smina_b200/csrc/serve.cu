@@ -110,6 +110,9 @@ struct SvLig {
     int model = 0, first = 0, nchains = 0, flag = -1;
     int state = 0;  // 0 searching, 1 refining, 2 published
     uint64_t evals = 0;
+    uint64_t dev_start = 0, dev_end = 0;  // device clock (ns): first chain's start, last chain's end
+    uint64_t launch = 0;                  // its batch's launch number
+    Clock::time_point t_launch;           // when its batch was launched
     std::vector<SvPose> poses;
     size_t conf_off = 0, xyz_off = 0;
     struct SvBatch* batch = nullptr;
@@ -122,8 +125,9 @@ struct SvBatch {
     ModelImage img;
     std::vector<SvLig> ligs;
     std::vector<Chain32> hc;
-    size_t e_at = 0, conf_at = 0, xyz_at = 0, order_at = 0, count_at = 0, evals_at = 0;
+    size_t e_at = 0, conf_at = 0, xyz_at = 0, order_at = 0, count_at = 0, evals_at = 0, span_at = 0;
     int S = 20;
+    uint64_t seq = 0;  // launch number (1, 2, ... per server)
     cudaEvent_t kdone = nullptr;  // recorded once every ligand's chains are done (see worker)
     int flagged = 0;               // ligands whose completion flag has been seen
     int published = 0;
@@ -140,6 +144,7 @@ struct Server {
     std::deque<uint64_t> done_order;  // not yet reported by poll
     std::vector<std::unique_ptr<SvBatch>> inflight;
     size_t inflight_bytes = 0;
+    uint64_t launches = 0;
     uint64_t next_ticket = 1;
     bool stopping = false;
     int error = SG_OK;
@@ -235,7 +240,9 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     b->count_at = at; at = r16(at + nchains * sizeof(int));
     b->evals_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
     const size_t hits_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
+    b->span_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
     b->bytes = std::max(at, need);
+    b->seq = ++s.launches;
     cuda_check(cudaMallocAsync((void**)&b->dmem, b->bytes, b->stream), "serve: batch memory");
     pack_models_image(descs.data(), (int)descs.size(), b->dmem, b->img);
     // map sets and search boxes of every receptor
@@ -287,6 +294,8 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
         L.conf_off = conf_off;
         L.xyz_off = xyz_off;
         L.batch = b.get();
+        L.launch = b->seq;
+        L.t_launch = Clock::now();
         const sg_ligand_job& J = L.req.job;
         for (int c = 0; c < J.num_chains; c++) {
             Chain32 ch{};
@@ -309,6 +318,7 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
             ch.host_flag = s.dflags + L.flag;
             ch.lig_chains = J.num_chains;
             ch.box = reinterpret_cast<const double*>(b->dmem + boxes_at) + 6 * L.req.rid;
+            ch.span = reinterpret_cast<unsigned long long*>(b->dmem + b->span_at) + 2 * kc;
             b->hc.push_back(ch);
             conf_off += (size_t)S * h.conf_size;
             xyz_off += (size_t)S * h.nheavy * 3;
@@ -397,9 +407,9 @@ static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
     auto r16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
     const size_t eb = nc * S * sizeof(double), cb = (size_t)nc * S * cs * sizeof(double),
                  xb = (size_t)nc * S * H * 3 * sizeof(float), ob = nc * S * sizeof(int), nb = nc * sizeof(int),
-                 vb = nc * sizeof(unsigned long long);
+                 vb = nc * sizeof(unsigned long long), sb = 2 * vb;
     const size_t c_at = r16(eb), x_at = c_at + r16(cb), o_at = x_at + r16(xb), n_at = o_at + r16(ob),
-                 v_at = n_at + r16(nb), total = v_at + r16(vb);
+                 v_at = n_at + r16(nb), s_at = v_at + r16(vb), total = s_at + r16(sb);
     size_t cap = 0;
     char* hb = pin_get(s, total, cap);
     const double* he = reinterpret_cast<const double*>(hb);
@@ -408,6 +418,7 @@ static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
     const int* horder = reinterpret_cast<const int*>(hb + o_at);
     const int* hcount = reinterpret_cast<const int*>(hb + n_at);
     const unsigned long long* hev = reinterpret_cast<const unsigned long long*>(hb + v_at);
+    const unsigned long long* hspan = reinterpret_cast<const unsigned long long*>(hb + s_at);
     cudaStream_t cp = s.copy_stream;
     auto get = [&](size_t to, size_t from, size_t bytes) {
         if (bytes)
@@ -419,11 +430,14 @@ static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
     get(o_at, b.order_at + (size_t)L.first * S * sizeof(int), ob);
     get(n_at, b.count_at + (size_t)L.first * sizeof(int), nb);
     get(v_at, b.evals_at + (size_t)L.first * sizeof(unsigned long long), vb);
+    get(s_at, b.span_at + (size_t)L.first * 2 * sizeof(unsigned long long), sb);
     const cudaError_t rc = cudaStreamSynchronize(cp);
     if (rc != cudaSuccess) pin_put(s, hb, cap);
     cuda_check(rc, "serve: fetch");
     for (size_t k = 0; k < nc; k++) {
         L.evals += hev[k];
+        L.dev_start = k == 0 ? hspan[0] : std::min<uint64_t>(L.dev_start, hspan[2 * k]);
+        L.dev_end = std::max<uint64_t>(L.dev_end, hspan[2 * k + 1]);
         const int cnt = std::min(std::max(hcount[k], 0), S);
         for (int i = 0; i < cnt; i++) {
             const int slot = horder[k * S + i];
@@ -554,6 +568,10 @@ static void publish(Server& s, const RefineGroup& g, size_t k) {
     d.info.conf_size = L.req.m->d.conf_size;
     d.info.num_heavy = H;
     d.info.evals = L.evals;
+    d.info.launch = L.launch;
+    d.info.queue_ms = std::chrono::duration<double, std::milli>(L.t_launch - L.req.t_submit).count();
+    d.info.device_start_ns = L.dev_start;
+    d.info.device_end_ns = L.dev_end;
     for (int i = 0; i < np; i++) {
         const size_t q = (size_t)g.first[k] + i;
         L.poses[i].e = g.out_e[q];
@@ -614,26 +632,33 @@ static void worker(Server* sp) {
         try {
             // 1. launch.  At most max_inflight_ligands ligands are on the device;
             // the rest wait here, so a launch never queues on the GPU behind
-            // resident work.  A launch holds one of at most kMaxStreams concurrent
-            // kernels until its last ligand is done, so the launches still
-            // possible must carry the ligands the device can still take: a launch
-            // goes out once that share has queued, or when the oldest request has
-            // waited max_wait_ms scaled by how scarce launches have become.  Same
-            // search parameters per launch; device memory held for requests in
-            // flight stays under the budget.
+            // resident work.  A launch holds one of at most kMaxStreams
+            // concurrent kernels until its last ligand is done, so launches
+            // must carry several ligands each for the device to fill: while
+            // more requests wait than the device can take, a launch waits
+            // until a batch of `full` ligands fits (twice the ligands in
+            // flight per launch slot).  When everything queued fits, it goes
+            // at once if a full batch has queued, else after the oldest
+            // request has waited max_wait_ms (scaled up as launch slots run
+            // out) for others to share it.  Same search parameters per
+            // launch; device memory held for requests in flight stays under
+            // the budget.
             const int in_use = (int)(s.streams.size() - s.free_streams.size());
             if (!s.queue.empty() && in_use < Server::kMaxStreams) {
                 const double waited =
                     std::chrono::duration<double, std::milli>(Clock::now() - s.queue.front().t_submit).count();
                 const int slots = Server::kMaxStreams - in_use;
                 const int open = std::max(0, s.o.max_inflight_ligands - s.inflight_ligs);
-                const int share = std::max(1, (open + slots - 1) / slots);
+                const int q = (int)s.queue.size();
+                const int want = std::min({q, open, s.o.max_batch_ligands, (int)s.free_flags.size()});
+                const int full = std::min(s.o.max_batch_ligands,
+                                          2 * ((s.o.max_inflight_ligands + Server::kMaxStreams - 1) / Server::kMaxStreams));
                 const double gather_ms = s.o.max_wait_ms * (double)Server::kMaxStreams / slots;
-                const bool go = open > 0 && ((int)s.queue.size() >= share || waited >= gather_ms || s.stopping);
+                const bool go = want > 0 && (want >= full || s.stopping || (q <= open && waited >= gather_ms));
                 if (go) {
                     std::vector<ServeReq> take;
                     size_t bytes = 0;
-                    const int cap = std::min({s.o.max_batch_ligands, (int)s.free_flags.size(), open});
+                    const int cap = want;
                     size_t t_stage = 0, t_ws = 0;
                     int t_chains = 1, t_shape = 0;
                     while (!s.queue.empty() && (int)take.size() < cap) {
@@ -782,11 +807,25 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
             cuda_check(cudaMemGetInfo(&fr, &tot), "serve: memory info");
             s->o.hbm_budget_bytes = fr / 4;
         }
-        // Every search launch takes the same shared memory per block: two blocks
-        // fit an SM's 164 KB configuration (with the kernel's static shared
-        // memory and the 1 KB the driver keeps per block), which leaves L1 room
-        // for the gathers; bigger models run fewer chains per block.
-        s->smem_block = std::min<size_t>((size_t)e->max_smem, 82048);
+        // Every search launch takes the same shared memory per block, set once
+        // here so that no kernel attribute changes while launches run.  By
+        // default it is the most that still fits two blocks per SM (the SM's
+        // shared memory, less per block the kernel's static shared memory and
+        // the driver's reserve), so that the largest ligands also run eight
+        // chains per block; block_smem_bytes overrides it.
+        size_t dyn_max = 0, two_per_sm = 0;
+        cuda_check(mc32_max_dynamic_smem((size_t)e->max_smem, &dyn_max), "serve: kernel attributes");
+        int per_sm = 0, reserved = 0;
+        cuda_check(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, e->device), "serve");
+        cuda_check(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, e->device), "serve");
+        cuda_check(mc32_max_dynamic_smem((size_t)std::max(0, per_sm / 2 - reserved), &two_per_sm), "serve");
+        if (s->o.block_smem_bytes > 0) {
+            require((size_t)s->o.block_smem_bytes <= dyn_max, "serve: block_smem_bytes above the device's limit");
+            s->smem_block = (size_t)s->o.block_smem_bytes;
+        } else {
+            s->smem_block = std::min(dyn_max, two_per_sm & ~(size_t)1023);
+        }
+        require(s->smem_block >= 4096, "serve: too little shared memory per block");
         cuda_check(mc32_reserve_smem(s->smem_block), "serve: kernel attributes");
         cuda_check(cudaStreamCreateWithFlags(&s->refine_stream, cudaStreamNonBlocking), "serve: stream");
         cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "serve: stream");

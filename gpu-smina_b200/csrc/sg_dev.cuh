@@ -157,6 +157,7 @@ struct Chain32 {
     volatile unsigned* host_flag;
     int lig_chains;
     const double* box;  // search box (lo xyz, hi xyz) of this chain's receptor; null: the launch's
+    unsigned long long* span;  // [2] device clock (ns) at the chain's start and end; null: not recorded
 };
 
 // A block's unit of work: chains [first, first + count) of one model

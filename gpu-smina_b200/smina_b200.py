@@ -83,12 +83,13 @@ class LigandResult(C.Structure):
 
 class ServeOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_ligands", C.c_int), ("max_wait_ms", C.c_double),
-                ("max_inflight_ligands", C.c_int)]
+                ("max_inflight_ligands", C.c_int), ("block_smem_bytes", C.c_int)]
 
 
 class ServeDone(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("status", C.c_int), ("count", C.c_int), ("conf_size", C.c_int),
-                ("num_heavy", C.c_int), ("evals", C.c_uint64), ("latency_ms", C.c_double)]
+                ("num_heavy", C.c_int), ("evals", C.c_uint64), ("latency_ms", C.c_double), ("launch", C.c_uint64),
+                ("device_start_ns", C.c_uint64), ("device_end_ns", C.c_uint64), ("queue_ms", C.c_double)]
 
 
 _lib = None
@@ -170,6 +171,7 @@ def _declare(L):
         "sg_serve_fetch": [vp, C.c_uint64, C.POINTER(LigandResult)],
         "sg_serve_stats": [vp, _ip, _ip, C.POINTER(C.c_uint64)],
         "sg_serve_stop": [vp],
+        "sg_probe_gather": [vp, C.c_uint64, C.c_int, C.POINTER(C.c_double)],
     }.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -606,8 +608,15 @@ class Engine:
                 "h2d_bytes": ctr[3].value, "d2h_bytes": ctr[4].value}
 
     # ---- serving (continuous batching) ----------------------------------------
-    def serve_start(self, hbm_budget_bytes=0, max_batch_ligands=0, max_wait_ms=0.0, max_inflight_ligands=0):
-        o = ServeOpts(hbm_budget_bytes, max_batch_ligands, max_wait_ms, max_inflight_ligands)
+    def probe_gather(self, working_set_bytes, bytes_per_lookup):
+        """GB/s of random gathers of bytes_per_lookup bytes over a working set of that size."""
+        g = C.c_double()
+        self._check(load().sg_probe_gather(self._h, int(working_set_bytes), int(bytes_per_lookup), C.byref(g)))
+        return g.value
+
+    def serve_start(self, hbm_budget_bytes=0, max_batch_ligands=0, max_wait_ms=0.0, max_inflight_ligands=0,
+                    block_smem_bytes=0):
+        o = ServeOpts(hbm_budget_bytes, max_batch_ligands, max_wait_ms, max_inflight_ligands, block_smem_bytes)
         self._check(load().sg_serve_start(self._h, C.byref(o)))
 
     def serve_submit(self, rid, m: Model, job: LigandJob, params: MCParams) -> int:
@@ -616,13 +625,18 @@ class Engine:
         self._check(load().sg_serve_submit(self._h, rid, C.byref(m.desc), C.byref(job), C.byref(params), C.byref(t)))
         return t.value
 
-    def serve_poll(self, max_n=256, wait_ms=0):
-        """Finished requests as (ticket, status, count, latency_ms, evals, conf_size, num_heavy) tuples."""
+    def serve_poll(self, max_n=256, wait_ms=0, spans=False):
+        """Finished requests as (ticket, status, count, latency_ms, evals, conf_size, num_heavy) tuples;
+        with spans, each tuple also carries (launch, device_start_ns, device_end_ns, queue_ms)."""
         buf = (ServeDone * max_n)()
         n = C.c_int()
         self._check(load().sg_serve_poll(self._h, buf, max_n, wait_ms, C.byref(n)))
-        return [(buf[i].ticket, buf[i].status, buf[i].count, buf[i].latency_ms, buf[i].evals, buf[i].conf_size,
-                 buf[i].num_heavy) for i in range(n.value)]
+        out = []
+        for i in range(n.value):
+            d = buf[i]
+            t = (d.ticket, d.status, d.count, d.latency_ms, d.evals, d.conf_size, d.num_heavy)
+            out.append(t + (d.launch, d.device_start_ns, d.device_end_ns, d.queue_ms) if spans else t)
+        return out
 
     def serve_fetch(self, ticket, count, conf_size, num_heavy):
         e, conf, xyz = np.zeros(max(count, 1)), np.zeros((max(count, 1), conf_size)), np.zeros((max(count, 1), num_heavy, 3))

@@ -243,7 +243,10 @@ int sg_dock(sg_engine* e, int receptor_id, const sg_model_desc* models, int nmod
             sg_chain_result* out);
 
 /* quasi_newton (BFGS, bfgs.h:202-282) of each conf against the maps;
- * confs [n][conf_size] updated in place, out_e [n]. */
+ * confs [n][conf_size] updated in place, out_e [n].  FP32 engines run the
+ * batched search's mixed-precision BFGS (FP32 energies and gradients; FP64
+ * conf, inverse Hessian and acceptance tests), so its local optimisations
+ * can be compared with the plain path's from the same starts. */
 int sg_bfgs(sg_engine* e, int receptor_id, const sg_model_desc* m, int nconfs, double* confs,
             const double v[3], double slope, int maxiters, int accurate_line, int early_term,
             double* out_e);
@@ -356,6 +359,15 @@ int sg_dock_batch32_noalloc(sg_engine* e, int receptor_id, const sg_model_desc* 
                             const sg_ligand_job* jobs, int njobs, const sg_mc_params* p,
                             sg_ligand_result* out);
 
+/* The gather bandwidth the search kernel's roofline divides by (no
+ * counterpart in the reference): independent random loads of
+ * bytes_per_lookup (16: a pair table entry, 32: a packed grid cell) bytes,
+ * aligned to their size, over a zero-filled device buffer of
+ * working_set_bytes (1 MiB .. 64 GiB) with every SM full; the best of three
+ * passes after one that brings the buffer into cache.  *out_gbs gets GB/s
+ * (1e9 bytes per second).  Allocates and frees the buffer itself. */
+int sg_probe_gather(sg_engine* e, uint64_t working_set_bytes, int bytes_per_lookup, double* out_gbs);
+
 /* Timing and launch shape of the last sg_dock_batch32 call. */
 int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
                    int* chains_per_block, int* blocks);
@@ -411,6 +423,9 @@ typedef struct sg_serve_opts {
                                    (0: two per SM, what the device holds at
                                    once with 8 chains per ligand, less 16
                                    kept for refinements)                     */
+    int block_smem_bytes;       /* dynamic shared memory of every search
+                                   launch's blocks (0: the most that keeps two
+                                   blocks per SM)                            */
 } sg_serve_opts;
 
 typedef struct sg_serve_done {
@@ -420,6 +435,14 @@ typedef struct sg_serve_done {
     int conf_size, num_heavy;  /* sizes for sg_serve_fetch's arrays         */
     uint64_t evals;            /* eval_deriv calls of the search            */
     double latency_ms;         /* submit to result                          */
+    uint64_t launch;           /* the search launch it ran in (1, 2, ...)   */
+    uint64_t device_start_ns;  /* device clock (%globaltimer, ns) when its
+                                  first chain started ...                   */
+    uint64_t device_end_ns;    /* ... and when its last chain ended; two
+                                  requests of different launches whose
+                                  spans overlap were on the device at once  */
+    double queue_ms;           /* submit to launch (waiting in the server's
+                                  queue)                                    */
 } sg_serve_done;
 
 int sg_serve_start(sg_engine* e, const sg_serve_opts* opts);

@@ -21,10 +21,11 @@ def _job(seed, key, chains=4, steps=25):
 def _collect(eng, tickets, timeout_s=120):
     got, t0 = {}, time.time()
     while len(got) < len(tickets) and time.time() - t0 < timeout_s:
-        for (t, status, count, lat, evals, cs, nh) in eng.serve_poll(64, wait_ms=50):
+        for (t, status, count, lat, evals, cs, nh, launch, d0, d1, qms) in eng.serve_poll(64, wait_ms=50, spans=True):
             assert status == sb.SG_OK
             got[t] = eng.serve_fetch(t, count, cs, nh)
-            got[t]["latency_ms"] = lat
+            got[t].update(latency_ms=lat, launch=launch, span=(d0, d1), queue_ms=qms)
+            assert 0 <= qms <= lat
     assert len(got) == len(tickets), "requests did not finish"
     return got
 
@@ -87,3 +88,32 @@ def test_serving_rejects_requests_over_budget(setup):
             eng.serve_submit(0, models[2], _job(1, 1, chains=64), p)
     finally:
         eng.serve_stop()
+
+
+def test_serving_launches_overlap_on_the_device(setup):
+    """Requests that arrive while others run go out in launches of their own
+    and share the device with them: the device-clock spans of requests from
+    different launches overlap, and every result still equals the batched
+    entry point's."""
+    eng, models = setup
+    p = models[0].search_params()
+    work = [(k % 2, models[k % 4], _job(11, 200 + k, chains=4, steps=60)) for k in range(6)]
+    refs = [_reference(eng, rid, m, j, p) for rid, m, j in work]
+    eng.serve_start(max_batch_ligands=1, max_wait_ms=0.5)
+    try:
+        tickets = []
+        for rid, m, j in work:
+            tickets.append(eng.serve_submit(rid, m, j, p))
+            time.sleep(0.005)
+        got = _collect(eng, tickets)
+    finally:
+        eng.serve_stop()
+    for t, ref in zip(tickets, refs):
+        _same(got[t], ref)
+        d0, d1 = got[t]["span"]
+        assert 0 < d0 < d1
+    res = [got[t] for t in tickets]
+    assert len({r["launch"] for r in res}) >= 2
+    overlapping = [(a["launch"], b["launch"]) for a in res for b in res
+                   if a["launch"] < b["launch"] and b["span"][0] < a["span"][1] and a["span"][0] < b["span"][1]]
+    assert overlapping, "no two launches were on the device at the same time"
