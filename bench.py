@@ -668,7 +668,7 @@ def run_serve(args):
         j.model = 0
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
     eng.serve_start(block_smem_bytes=args.serve_block_smem)
-    lat, evals, dev = {}, 0, {}
+    lat, evals, dev, queue = {}, 0, {}, {}
     k = 0
     occupancy = []  # (queued, ligands in flight) sampled every 100 ms
     next_sample = 0.0
@@ -684,12 +684,13 @@ def run_serve(args):
                 occupancy.append((st["queued"], st["inflight"]))
                 next_sample = now + 0.1
             wait = 1 if k < n else 20
-            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1) in eng.serve_poll(256, wait_ms=wait, spans=True):
+            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1, qms) in eng.serve_poll(256, wait_ms=wait, spans=True):
                 if st != 0:
                     raise RuntimeError(f"request {t} failed with status {st}")
                 eng.serve_fetch(t, cnt, cs, nh)
                 lat[t] = ms
                 dev[t] = (launch, d0, d1)
+                queue[t] = qms
                 evals += ev
         wall = time.perf_counter() - t0
     eng.serve_stop()
@@ -704,10 +705,14 @@ def run_serve(args):
                        "max": float(v.max()), "mean": float(v.mean())},
         "device_search_ms": {"p50": float(np.percentile(dms, 50)), "p99": float(np.percentile(dms, 99)),
                              "mean": float(dms.mean())},
+        "queue_ms": {"p50": float(np.percentile(list(queue.values()), 50)),
+                     "p99": float(np.percentile(list(queue.values()), 99)), "mean": float(np.mean(list(queue.values())))},
         "launches": launches,
         "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
         "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),
-                             "max": int(max(o[1] for o in occupancy))},
+                             "max": int(max(o[1] for o in occupancy)),
+                             "mean_while_requests_wait": float(np.mean([o[1] for o in occupancy if o[0] > 0]))
+                             if any(o[0] > 0 for o in occupancy) else None},
         "queued": {"mean": float(np.mean([o[0] for o in occupancy])), "max": int(max(o[0] for o in occupancy))},
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{n} requests, ligands heavy U[10,60] rotors U[0,15], receptors "
@@ -868,7 +873,8 @@ def main():
     eng = sb.Engine(local, prec)
     eng.set_tables(T)
     eng.set_receptor(0, R, gd)
-    eng.build_grids(0, sorted({t for m in models for t in m.types() if 1 < t < 27}))
+    types = sorted({t for m in models for t in m.types() if 1 < t < 27})
+    eng.build_grids(0, types)
     p = make_params(models)
     B = args.batch or args.ligands
     tuned = None
@@ -926,8 +932,27 @@ def main():
     peak, peak_src = (peaks["hbm_gbs"], "measured") if "hbm_gbs" in peaks else (6650.0, "fallback")
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k_mc32_traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("bytes_per_launch")
+    if os.path.exists(tf):  # DRAM bytes of short-case ncu captures, extended to this launch by eval_deriv calls
+        t = json.load(open(tf))
+        if t.get("bytes_per_eval"):
+            traffic = t.get("fixed_bytes", 0) + t["bytes_per_eval"] * sum(r[2]["evals"] for r in recs) / len(recs)
+    # The gathers hit L2 (the maps of the screen's types and the table fit in
+    # it), so their bound is the measured rate of random 32 B / 16 B gathers
+    # over a working set of the same size, mixed in the kernel's proportion.
+    roof_l2 = None
+    if rank == 0:
+        ncells = int(np.prod([gd.n[i] for i in range(3)]))
+        ws = len(types) * ncells * G_BYTES[prec] + T.desc.n * 378 * T_BYTES
+        g32 = eng.probe_gather(ws, 32) if G_BYTES[prec] == 32 else eng.probe_gather(ws, 16)
+        g16 = eng.probe_gather(ws, 16)
+        gb = sum(r[2]["grid_lookups"] * G_BYTES[prec] for r in recs)
+        tb = sum(r[2]["pair_lookups"] * T_BYTES for r in recs)
+        peak_l2 = (gb + tb) / (gb / g32 + tb / g16)
+        roof_l2 = {"bound": "l2 gathers", "achieved": achieved, "peak": peak_l2, "unit": "GB/s",
+                   "frac": achieved / peak_l2,
+                   "peak_source": f"measured in this run: random {G_BYTES[prec]} B gathers {g32:.0f} GB/s and 16 B "
+                                  f"gathers {g16:.0f} GB/s over {ws / 1e6:.0f} MB (sg_probe_gather), weighted by the "
+                                  f"kernel's grid / table bytes"}
     evals = sum(r[2]["evals"] for r in recs)
     accuracy = None  # top-score agreement with the FP64 search, measured by the command it names
     af = os.path.join(ROOT, "profiles", "accuracy_fp32_vs_fp64_screen120.json")
@@ -963,9 +988,11 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k_mc32"},
+            "roofline_l2": roof_l2,
             "cpu_baseline": cpu,
             "accuracy": accuracy,
             "evals_per_s": evals / mc_s,
+            "evals_per_step": evals / args.steps,
             "search_ms_per_step": 1000 * mc_s / args.steps,
         }), flush=True)
     if pg is not None:

@@ -842,19 +842,42 @@ int sg_eval_direct(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, co
     return eval_common(e, rid, m, nconfs, confs, v, slope, out_e, out_g, nullptr, 1);
 }
 
+int sg_probe_gather(sg_engine* e, uint64_t working_set_bytes, int bytes_per_lookup, double* out_gbs) {
+    return guarded(e, [&] {
+        require(out_gbs && (bytes_per_lookup == 16 || bytes_per_lookup == 32) && working_set_bytes >= (1u << 20) &&
+                    working_set_bytes <= (64ull << 30),
+                "probe_gather: bad arguments");
+        cuda_check(gather_probe(working_set_bytes, bytes_per_lookup, e->num_sms, out_gbs, e->stream), "gather probe");
+    });
+}
+
 int sg_bfgs(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, double* confs, const double v[3], double slope,
             int maxiters, int accurate_line, int early_term, double* out_e) {
     return guarded(e, [&] {
-        require(m && confs && v && out_e && nconfs > 0 && maxiters >= 0, "bfgs: bad arguments");
+        require(m && confs && v && out_e && nconfs > 0 && nconfs <= (1 << 24) && maxiters >= 0, "bfgs: bad arguments");
         RecState& r = receptor_for(e, rid);
         PackedModels pm;
         pack_models(e, m, 1, pm);
         ensure_model_maps(e, r, pm, m, 1);
-        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
         const DModel& h = pm.host[0];
         Staged<double> dc, de;
         dc.make((size_t)nconfs * h.conf_size, e->stream, confs);
         de.make(nconfs, e->stream);
+        if (e->precision != SG_PREC_FP64) {  // the batched search's mixed-precision BFGS
+            require(h.npchunks >= 0, "mixed-precision path: at most 255 atoms per model");
+            const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
+            const size_t stage =
+                (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
+            require(stage + ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
+            cuda_check(launch_bfgs32(pm.dmodels.as<DModel>(), stage, ws, tables32(e), maps32(e, r), nconfs, dc.p(), v,
+                                     slope, maxiters, accurate_line, early_term, de.p(), e->stream),
+                       "bfgs launch");
+            dc.fetch(confs, e->stream);
+            de.fetch(out_e, e->stream);
+            e->check_device_errors();
+            return;
+        }
+        require(pm.max_ws64 <= (size_t)e->max_smem, "model too large for the plain path's shared memory");
         cuda_check(launch_bfgs64(pm.dmodels.as<DModel>(), pm.max_ws64, e->tables, r.dhdr.as<DReceptor>(), nconfs, dc.p(), v,
                                  slope, maxiters, accurate_line, early_term, de.p(), e->d_err.as<int>(), e->stream),
                    "bfgs launch");

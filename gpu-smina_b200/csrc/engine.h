@@ -148,6 +148,10 @@ cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const D
                         size_t stage_stride, size_t ws_stride, cudaStream_t);
 cudaError_t launch_eval32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, const double*,
                           const double[3], double, double*, double*, double*, cudaStream_t);
+cudaError_t gather_probe(size_t working_set, int bytes_per_lookup, int num_sms, double* gbs, cudaStream_t s);
+cudaError_t launch_bfgs32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, double*,
+                          const double v[3], double slope, int maxiters, int accurate, int early, double* e,
+                          cudaStream_t);
 
 // FP32 views of the engine's tables and of a receptor's packed maps
 DTables32 tables32(const sg_engine* e);

@@ -247,3 +247,28 @@ def test_batch_rejects_fp64_engine(base):
     m = W.ligand(24, 5, 11)
     with pytest.raises(sb.SminaError):
         engine(sb.PREC_FP64).dock_batch(0, [m], _jobs([m]), _params(m))
+
+
+@pytest.mark.parametrize("heavy,rotors,seed", [(24, 5, 11), (40, 10, 5)])
+def test_mixed_precision_bfgs(base, heavy, rotors, seed):
+    """sg_bfgs on an FP32 engine runs the batched search's own BFGS (FP32
+    energies and gradients; FP64 conf, inverse Hessian and acceptance
+    tests): it never returns an energy above its starting energy, it lowers
+    the energy of some of the random starts (many start far outside the box
+    or in clashes that its line search cannot leave within the iterations), the energy it returns for a pose is that
+    pose's energy (FP64 evaluation of the returned conf, within the FP32
+    rule), and a second run gives the same bits."""
+    engine, _, gd, _ = base
+    m = W.ligand(heavy, rotors, seed)
+    e64, e32 = engine(sb.PREC_FP64), engine(sb.PREC_FP32)
+    starts = W.random_confs(m, gd, 128, 23)
+    maxit = m.search_params().maxiters
+    c32, f32 = e32.bfgs(0, m, starts, maxiters=maxit)
+    e0, _ = e32.eval(0, m, starts)
+    assert (f32 <= e0).all()
+    assert (f32 < e0).mean() >= 0.1
+    ev64, _ = e64.eval(0, m, c32)
+    rel = np.abs(f32 - ev64) / np.maximum(np.abs(ev64), 1.0)
+    assert (rel <= TOL).mean() >= FRAC, np.percentile(rel, [50, 99, 100])
+    c32b, f32b = e32.bfgs(0, m, starts, maxiters=maxit)
+    assert np.array_equal(c32b, c32) and np.array_equal(f32b, f32)
