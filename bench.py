@@ -668,7 +668,7 @@ def run_serve(args):
         j.model = 0
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
     eng.serve_start(block_smem_bytes=args.serve_block_smem)
-    lat, evals, dev, queue = {}, 0, {}, {}
+    lat, evals, dev, queue, searched = {}, 0, {}, {}, {}
     k = 0
     occupancy = []  # (queued, ligands in flight) sampled every 100 ms
     next_sample = 0.0
@@ -684,18 +684,25 @@ def run_serve(args):
                 occupancy.append((st["queued"], st["inflight"]))
                 next_sample = now + 0.1
             wait = 1 if k < n else 20
-            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1, qms) in eng.serve_poll(256, wait_ms=wait, spans=True):
+            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1, qms, sms) in eng.serve_poll(256, wait_ms=wait, spans=True):
                 if st != 0:
                     raise RuntimeError(f"request {t} failed with status {st}")
                 eng.serve_fetch(t, cnt, cs, nh)
                 lat[t] = ms
                 dev[t] = (launch, d0, d1)
                 queue[t] = qms
+                searched[t] = sms
                 evals += ev
         wall = time.perf_counter() - t0
     eng.serve_stop()
     v = np.array(list(lat.values()))
     dms = np.array([(d1 - d0) / 1e6 for (_, d0, d1) in dev.values()])
+    tk = list(lat)
+    launch_to_done = np.array([searched[t] - queue[t] for t in tk])
+    after_search = np.array([lat[t] - searched[t] for t in tk])
+    d0s = [d[1] for d in dev.values()]
+    busy_s = (max(d[2] for d in dev.values()) - min(d0s)) / 1e9
+    concurrency = float(dms.sum() / 1e3 / busy_s) if busy_s > 0 else None
     launches = len({l for (l, _, _) in dev.values()})
     clocks = clk.summary()
     print(json.dumps({
@@ -707,6 +714,10 @@ def run_serve(args):
                              "mean": float(dms.mean())},
         "queue_ms": {"p50": float(np.percentile(list(queue.values()), 50)),
                      "p99": float(np.percentile(list(queue.values()), 99)), "mean": float(np.mean(list(queue.values())))},
+        "launch_to_chains_done_ms": {"p50": float(np.percentile(launch_to_done, 50)),
+                                     "mean": float(launch_to_done.mean())},
+        "merge_refine_ms": {"p50": float(np.percentile(after_search, 50)), "mean": float(after_search.mean())},
+        "ligands_searching_at_once": concurrency,
         "launches": launches,
         "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
         "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),

@@ -113,6 +113,7 @@ struct SvLig {
     uint64_t dev_start = 0, dev_end = 0;  // device clock (ns): first chain's start, last chain's end
     uint64_t launch = 0;                  // its batch's launch number
     Clock::time_point t_launch;           // when its batch was launched
+    Clock::time_point t_flag;             // when the worker saw its chains done
     std::vector<SvPose> poses;
     size_t conf_off = 0, xyz_off = 0;
     struct SvBatch* batch = nullptr;
@@ -400,6 +401,7 @@ static void pin_put(Server& s, char* p, size_t cap) {
 
 // A ligand's chains are done: copy their containers back and merge them.
 static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
+    L.t_flag = Clock::now();
     const DModel& h = b.img.host[L.model];
     const int S = b.S, cs = h.conf_size, H = h.nheavy;
     const size_t nc = L.nchains;
@@ -570,6 +572,7 @@ static void publish(Server& s, const RefineGroup& g, size_t k) {
     d.info.evals = L.evals;
     d.info.launch = L.launch;
     d.info.queue_ms = std::chrono::duration<double, std::milli>(L.t_launch - L.req.t_submit).count();
+    d.info.searched_ms = std::chrono::duration<double, std::milli>(L.t_flag - L.req.t_submit).count();
     d.info.device_start_ns = L.dev_start;
     d.info.device_end_ns = L.dev_end;
     for (int i = 0; i < np; i++) {

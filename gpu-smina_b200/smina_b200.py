@@ -89,7 +89,8 @@ class ServeOpts(C.Structure):
 class ServeDone(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("status", C.c_int), ("count", C.c_int), ("conf_size", C.c_int),
                 ("num_heavy", C.c_int), ("evals", C.c_uint64), ("latency_ms", C.c_double), ("launch", C.c_uint64),
-                ("device_start_ns", C.c_uint64), ("device_end_ns", C.c_uint64), ("queue_ms", C.c_double)]
+                ("device_start_ns", C.c_uint64), ("device_end_ns", C.c_uint64), ("queue_ms", C.c_double),
+                ("searched_ms", C.c_double)]
 
 
 _lib = None
@@ -627,7 +628,7 @@ class Engine:
 
     def serve_poll(self, max_n=256, wait_ms=0, spans=False):
         """Finished requests as (ticket, status, count, latency_ms, evals, conf_size, num_heavy) tuples;
-        with spans, each tuple also carries (launch, device_start_ns, device_end_ns, queue_ms)."""
+        with spans, each tuple also carries (launch, device_start_ns, device_end_ns, queue_ms, searched_ms)."""
         buf = (ServeDone * max_n)()
         n = C.c_int()
         self._check(load().sg_serve_poll(self._h, buf, max_n, wait_ms, C.byref(n)))
@@ -635,7 +636,7 @@ class Engine:
         for i in range(n.value):
             d = buf[i]
             t = (d.ticket, d.status, d.count, d.latency_ms, d.evals, d.conf_size, d.num_heavy)
-            out.append(t + (d.launch, d.device_start_ns, d.device_end_ns, d.queue_ms) if spans else t)
+            out.append(t + (d.launch, d.device_start_ns, d.device_end_ns, d.queue_ms, d.searched_ms) if spans else t)
         return out
 
     def serve_fetch(self, ticket, count, conf_size, num_heavy):

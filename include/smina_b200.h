@@ -443,6 +443,8 @@ typedef struct sg_serve_done {
                                   spans overlap were on the device at once  */
     double queue_ms;           /* submit to launch (waiting in the server's
                                   queue)                                    */
+    double searched_ms;        /* submit to the worker seeing its chains
+                                  done (then merge and FP64 refinement)     */
 } sg_serve_done;
 
 int sg_serve_start(sg_engine* e, const sg_serve_opts* opts);

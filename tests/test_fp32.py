@@ -224,22 +224,28 @@ def test_batch_counters(base):
 
 def test_batch_pose_quality_vs_fp64(base):
     """Same ligand, same chains and steps: the FP32 batched search reaches the
-    plain FP64 search's best refined energy (different random streams, so
-    within a margin)."""
+    plain FP64 search's best refined energy.  The streams differ, and one
+    short search lands in one of several near-degenerate minima, so each side
+    runs 4 independent searches of 8 chains and their best results are
+    compared, within a margin."""
     engine, orc, gd, _ = base
     m = W.ligand(24, 5, 11)
     p = _params(m)
-    chains, steps = 8, 400
+    chains, steps, runs = 8, 400, 4
     eng64 = engine(sb.PREC_FP64)
-    confs, mts = m.seed_chains(5, chains, gd)
-    b = eng64.dock(0, [m], np.zeros(chains, np.int32), confs, mts, p, steps=steps)
-    e, conf, _ = merge(b, m)
-    _, e64, _ = eng64.refine(0, [m], np.zeros(len(e), np.int32), conf, cap=tuple(p.authentic_v),
-                             maxiters=p.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
-    r32 = engine(sb.PREC_FP32).dock_batch(0, [m], [sb.LigandJob(model=0, num_chains=chains, num_steps=steps,
-                                                                maxiters=0, seed=5, ligand_key=1)], p)
-    best64, best32 = float(np.min(e64)), float(r32[0]["e"][0])
-    assert best32 <= best64 + 0.5, (best32, best64)
+    confs, mts = m.seed_chains(5, chains * runs, gd)
+    b = eng64.dock(0, [m], np.zeros(chains * runs, np.int32), confs, mts, p, steps=steps)
+    best64 = []
+    for k in range(runs):
+        sub = sb.merge_chains(b, m, first=chains * k, n=chains, max_size=p.num_saved_mins)
+        _, e64, _ = eng64.refine(0, [m], np.zeros(len(sub[0]), np.int32), sub[1], cap=tuple(p.authentic_v),
+                                 maxiters=p.maxiters, accurate_line=p.accurate_line, early_term=p.early_term)
+        best64.append(float(np.min(e64)))
+    jobs = [sb.LigandJob(model=0, num_chains=chains, num_steps=steps, maxiters=0, seed=5, ligand_key=1 + k)
+            for k in range(runs)]
+    r32 = engine(sb.PREC_FP32).dock_batch(0, [m], jobs, p)
+    best32 = [float(r["e"][0]) for r in r32]
+    assert min(best32) <= min(best64) + 0.5, (best32, best64)
 
 
 def test_batch_rejects_fp64_engine(base):
