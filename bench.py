@@ -666,9 +666,23 @@ def run_serve(args):
     jobs = jobs_for(models, list(range(n)), args.exhaustiveness, args.seed, 0, args.step_scale)
     for j in jobs:
         j.model = 0
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    if args.rates:  # piecewise-constant Poisson rates, cycling every rate_period seconds
+        rates = [float(x) for x in args.rates.split(",")]
+        arrivals, t = [], 0.0
+        while len(arrivals) < n:
+            seg = int(t // args.rate_period) % len(rates)
+            t_next = t + rng.exponential(1.0 / rates[seg])
+            seg_end = (t // args.rate_period + 1) * args.rate_period
+            if t_next > seg_end:  # memoryless: restart at the segment boundary with the next rate
+                t = seg_end
+                continue
+            t = t_next
+            arrivals.append(t)
+        arrivals = np.array(arrivals)
+    else:
+        arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
     eng.serve_start(block_smem_bytes=args.serve_block_smem)
-    lat, evals, dev, queue, searched = {}, 0, {}, {}, {}
+    lat, evals, dev, queue, searched, done_at = {}, 0, {}, {}, {}, {}
     k = 0
     occupancy = []  # (queued, ligands in flight) sampled every 100 ms
     next_sample = 0.0
@@ -689,6 +703,7 @@ def run_serve(args):
                     raise RuntimeError(f"request {t} failed with status {st}")
                 eng.serve_fetch(t, cnt, cs, nh)
                 lat[t] = ms
+                done_at[t] = time.perf_counter() - t0
                 dev[t] = (launch, d0, d1)
                 queue[t] = qms
                 searched[t] = sms
@@ -703,6 +718,12 @@ def run_serve(args):
     d0s = [d[1] for d in dev.values()]
     busy_s = (max(d[2] for d in dev.values()) - min(d0s)) / 1e9
     concurrency = float(dms.sum() / 1e3 / busy_s) if busy_s > 0 else None
+    # completions per second over the middle 80 % of them (the ramp-up and the
+    # drain of the last, longest ligands left out), and the device spans
+    # inside that window
+    tdone = np.sort(np.array(list(done_at.values())))
+    t10, t90 = np.percentile(tdone, 10), np.percentile(tdone, 90)
+    mid_rate = float(((tdone >= t10) & (tdone <= t90)).sum() / (t90 - t10)) if t90 > t10 else None
     launches = len({l for (l, _, _) in dev.values()})
     clocks = clk.summary()
     print(json.dumps({
@@ -718,8 +739,9 @@ def run_serve(args):
                                      "mean": float(launch_to_done.mean())},
         "merge_refine_ms": {"p50": float(np.percentile(after_search, 50)), "mean": float(after_search.mean())},
         "ligands_searching_at_once": concurrency,
+        "completions_per_s_middle_80pct": mid_rate,
         "launches": launches,
-        "requests": n, "offered_rate_per_s": args.rate, "wall_s": wall, "evals_per_s": evals / wall,
+        "requests": n, "offered_rate_per_s": args.rates or args.rate, "wall_s": wall, "evals_per_s": evals / wall,
         "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),
                              "max": int(max(o[1] for o in occupancy)),
                              "mean_while_requests_wait": float(np.mean([o[1] for o in occupancy if o[0] > 0]))
@@ -730,7 +752,9 @@ def run_serve(args):
                                f"{[r[0] for r in SERVE_RECEPTORS]} heavy atoms in {[r[1] for r in SERVE_RECEPTORS]} A "
                                f"boxes at 0.375 A, exhaustiveness {args.exhaustiveness}, smina step counts"
                                + (f" x {args.step_scale}" if args.step_scale != 1.0 else ""),
-                   "precision": args.precision, "arrivals": f"Poisson, seed {args.seed}",
+                   "precision": args.precision,
+                   "arrivals": (f"Poisson at rates {args.rates} per second, each for {args.rate_period} s in turn"
+                                if args.rates else f"Poisson at {args.rate} per second") + f", seed {args.seed}",
                    "block_smem_bytes": args.serve_block_smem or "automatic"},
         "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
     }), flush=True)
@@ -827,6 +851,9 @@ def main():
     ap.add_argument("--serve", type=int, default=0,
                     help="instead of the screen: this many requests through the serving loop (p50/p99 latency)")
     ap.add_argument("--rate", type=float, default=20.0, help="offered request rate for --serve (per second)")
+    ap.add_argument("--rates", default="",
+                    help="with --serve: comma-separated Poisson rates (per second), each held for --rate-period s in turn")
+    ap.add_argument("--rate-period", type=float, default=60.0)
     ap.add_argument("--serve-block-smem", type=int, default=0,
                     help="with --serve: dynamic shared memory per search block (0: the server's default)")
     ap.add_argument("--plain64", action="store_true",

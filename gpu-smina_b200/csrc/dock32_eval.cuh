@@ -185,8 +185,8 @@ __device__ __noinline__ void set_frames_by_level(W32 w, const double* conf) {
     float4* Q = w.quat();
     float4* R = w.rot();
     for (int lv = 0; lv < m.nlevels; lv++) {
-        for (int idx = __ldg(m.level_start + lv) + w.lane; idx < __ldg(m.level_start + lv + 1); idx += 32) {
-            const int f = __ldg(m.level_frames + idx);
+        for (int idx = __ldcg(m.level_start + lv) + w.lane; idx < __ldcg(m.level_start + lv + 1); idx += 32) {
+            const int f = __ldcg(m.level_frames + idx);
             const int kind = fkind[f];
             float4 q;
             if (kind == SG_FRAME_RIGID) {

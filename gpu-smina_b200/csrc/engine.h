@@ -138,6 +138,11 @@ cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DRecept
                             double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
 int mc32_occupancy(int wpb, size_t smem);
+cudaError_t launch_mc32_feed(const DTables32& T, const FeedItem32* ring, unsigned cap, FeedCtrl32* ctrl,
+                             long long idle_ns, int blocks, int wpb, size_t smem, cudaStream_t s);
+cudaError_t mc32_feed_reserve_smem(size_t smem);
+cudaError_t mc32_feed_occupancy(int wpb, size_t smem, int* blocks);
+cudaError_t mc32_feed_max_dynamic_smem(size_t optin, size_t* out);
 cudaError_t mc32_reserve_smem(size_t smem);
 cudaError_t mc32_max_dynamic_smem(size_t optin, size_t* out);
 cudaError_t launch_mc32_fixed(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,

@@ -394,7 +394,7 @@ __device__ __forceinline__ void randomize32(const W32& w, Philox& rng, double* x
         double* c = x + blk_conf[b];
         if (blk_rigid[b]) {
             double v[7];
-            for (int k = 0; k < 3; k++) v[k] = ph_range(rng, box[k], box[3 + k]);
+            for (int k = 0; k < 3; k++) v[k] = ph_range(rng, __ldcg(box + k), __ldcg(box + 3 + k));
             double q[4], nq = 0;
             for (int k = 0; k < 4; k++) { q[k] = ph_normal(rng); nq += q[k] * q[k]; }
             nq = sqrt(nq);
@@ -481,8 +481,10 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
     for (int i = w.lane; i < 65; i += 32) C[i] = 0;
     const int cs = m.conf_size;
     // model state as read (mutation may read it before the first set)
-    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);
-    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
+    // (L2-only loads: a serving grid may read a ligand placed where an earlier
+    // one was, and this SM's L1 may still hold the earlier one's lines)
+    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldcg(m.lab32 + i);
+    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldcg(m.finit32 + f);
     __syncwarp();
     Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
     const int tmp_at = w.at(L.x_tmp), cand_at = w.at(L.x_cand);
@@ -541,17 +543,25 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
 // Copies a model's counts and the arrays the search reads into smem32 at
 // offset 0 (an SModel, then the arrays); every thread of the block takes
 // part.  Ends with a block barrier.
+// Loads go through L2 only (ld.global.cg): a serving grid stages ligands
+// that the host placed, while it runs, where earlier ones were.
 template <typename T>
 __device__ __forceinline__ int stage_arr(const T* src, int n, int& o, int tid, int nthr) {
     const int at = o;
     T* d = sp<T>(at);
     o += (n * (int)sizeof(T) + 15) & ~15;
-    for (int i = tid; i < n; i += nthr) d[i] = src[i];
+    for (int i = tid; i < n; i += nthr) d[i] = __ldcg(src + i);
     return at;
 }
 
+__shared__ __align__(16) DModel s_dmodel;  // the staged model's descriptor (its pointers)
+
 __device__ void stage_model(const DModel* gm, int tid, int nthr) {
-    const DModel& g = *gm;
+    static_assert(sizeof(DModel) % 16 == 0, "DModel is read in 16-byte pieces");
+    for (int k = tid; k < (int)(sizeof(DModel) / 16); k += nthr)
+        reinterpret_cast<int4*>(&s_dmodel)[k] = __ldcg(reinterpret_cast<const int4*>(gm) + k);
+    __syncthreads();
+    const DModel& g = s_dmodel;
     int o = ((int)sizeof(SModel) + 15) & ~15;
     SModel s;
     s.natoms = g.natoms; s.nmov = g.nmov; s.nframes = g.nframes; s.nlig = g.nlig; s.conf_size = g.conf_size;
@@ -623,6 +633,91 @@ __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DM
         __syncthreads();  // the staged model is in use until every warp is done
         SG_T1(t_bar, 8);
     }
+}
+
+// ---- serving grid ----------------------------------------------------------------------------
+// Claims the next item of the ring for this block (thread 0): the item's
+// sequence number, or -1 once no item has come for idle_ns nanoseconds or
+// the host has set stop.  Every wait is bounded: a block that finds no work
+// sleeps in short steps and leaves after idle_ns.
+__device__ long long feed_claim(FeedCtrl32* c, long long idle_ns) {
+    volatile unsigned* vc = reinterpret_cast<volatile unsigned*>(c);
+    long long t0 = 0;
+    bool waiting = false;
+    long long got = -1;
+    for (;;) {
+        const unsigned h = vc[0], t = vc[1];  // head, tail
+        if ((int)(t - h) > 0) {
+            if (atomicCAS(&c->head, h, h + 1u) == h) { got = (long long)h; break; }
+            continue;
+        }
+        if (vc[5]) break;  // stop
+        const long long now = (long long)global_ns();
+        if (!waiting) {
+            waiting = true;
+            t0 = now;
+            atomicAdd(&c->waiting, 1u);
+        } else if (now - t0 > idle_ns) {
+            break;
+        }
+        __nanosleep(8000);
+    }
+    if (waiting) atomicSub(&c->waiting, 1u);
+    return got;
+}
+
+__shared__ __align__(16) MCParams32 s_params;  // the running item's search parameters (serving grid)
+static_assert(sizeof(FeedItem32) % 16 == 0 && sizeof(DMaps32) % 16 == 0 && sizeof(MCParams32) % 16 == 0 &&
+                  sizeof(Chain32) % 16 == 0,
+              "serving-grid records are copied in 16-byte pieces");
+
+// The serving grid: persistent blocks that take items from a ring the host
+// keeps filling while the grid runs, so that a ligand's chains start as
+// soon as a block is free, whatever launch it came with.  An item's block
+// stages its ligand's model and runs one chain per warp; its chains signal
+// completion as in k_mc32.  Everything an item points to is read through
+// L2 only (the host reuses device memory while the grid runs).  A block
+// leaves after idle_ns without work; the host starts more blocks when
+// items wait and none is free.
+__global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32_feed(DTables32 T, const FeedItem32* ring,
+                                                                 unsigned cap, FeedCtrl32* ctrl, long long idle_ns) {
+    __shared__ long long s_seq;
+    __shared__ FeedItem32 s_fi;
+    const int tid = threadIdx.x, nthr = blockDim.x, warp = tid >> 5;
+    if (tid == 0) {
+        sT32 = T;
+        atomicAdd(&ctrl->started, 1u);
+    }
+    for (;;) {
+        if (tid == 0) {
+            s_seq = feed_claim(ctrl, idle_ns);
+            if (s_seq >= 0) {
+                const int4* src = reinterpret_cast<const int4*>(ring + (size_t)(s_seq % cap));
+                int4* dst = reinterpret_cast<int4*>(&s_fi);
+                for (int k = 0; k < (int)(sizeof(FeedItem32) / 16); k++) dst[k] = __ldcg(src + k);
+                const int4* gs = reinterpret_cast<const int4*>(s_fi.maps);
+                int4* gd = reinterpret_cast<int4*>(&sG32);
+                for (int k = 0; k < (int)(sizeof(DMaps32) / 16); k++) gd[k] = __ldcg(gs + k);
+                const int4* ps = reinterpret_cast<const int4*>(s_fi.params);
+                int4* pd = reinterpret_cast<int4*>(&s_params);
+                for (int k = 0; k < (int)(sizeof(MCParams32) / 16); k++) pd[k] = __ldcg(ps + k);
+                sWs0 = s_fi.stage_stride;
+                sWsStride = s_fi.ws_stride;
+            }
+        }
+        __syncthreads();
+        if (s_seq < 0) break;
+        stage_model(s_fi.model, tid, nthr);
+        if (warp < s_fi.count) {
+            Chain32 ch;
+            const int4* cs = reinterpret_cast<const int4*>(s_fi.chains + warp);
+            int4* cd = reinterpret_cast<int4*>(&ch);
+            for (int k = 0; k < (int)(sizeof(Chain32) / 16); k++) cd[k] = __ldcg(cs + k);
+            run_chain32(ch, s_params);
+        }
+        __syncthreads();  // the staged model is in use until every warp is done
+    }
+    if (tid == 0) atomicAdd(&ctrl->exited, 1u);
 }
 
 // model::eval_deriv in FP32 for a batch of confs of one model (one warp per
@@ -763,6 +858,32 @@ cudaError_t launch_bfgs32(const DModel* dm, size_t stage, size_t ws, const DTabl
     k_bfgs32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, maxiters,
                                  accurate, early, e, (int)stage);
     return cudaGetLastError();
+}
+
+// A serving grid of `blocks` blocks of 32 * wpb threads with `smem` bytes
+// of dynamic shared memory (raised beforehand with mc32_reserve_smem).
+cudaError_t launch_mc32_feed(const DTables32& T, const FeedItem32* ring, unsigned cap, FeedCtrl32* ctrl,
+                             long long idle_ns, int blocks, int wpb, size_t smem, cudaStream_t s) {
+    k_mc32_feed<<<blocks, 32 * wpb, smem, s>>>(T, ring, cap, ctrl, idle_ns);
+    return cudaGetLastError();
+}
+
+// raises k_mc32_feed's dynamic shared-memory limit ahead of its launches
+cudaError_t mc32_feed_reserve_smem(size_t smem) { return prep32((const void*)k_mc32_feed, smem); }
+
+// the largest dynamic shared memory a k_mc32_feed block can take within
+// `optin` bytes: less the kernel's static shared memory
+cudaError_t mc32_feed_max_dynamic_smem(size_t optin, size_t* out) {
+    cudaFuncAttributes fa{};
+    cudaError_t rc = cudaFuncGetAttributes(&fa, (const void*)k_mc32_feed);
+    if (rc != cudaSuccess) return rc;
+    *out = optin > fa.sharedSizeBytes ? optin - fa.sharedSizeBytes : 0;
+    return cudaSuccess;
+}
+
+// resident k_mc32_feed blocks per SM with `wpb` warps and `smem` bytes
+cudaError_t mc32_feed_occupancy(int wpb, size_t smem, int* blocks) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_mc32_feed, 32 * wpb, smem);
 }
 
 #ifdef SG_PROFILE

@@ -1,14 +1,16 @@
 // Serving: a request loop with continuous batching over resident receptors.
 //
 // Requests (one ligand against one resident receptor each) are queued by
-// sg_serve_submit.  A worker thread launches them in small batches: a batch
-// goes out as soon as enough requests wait or the oldest has waited
-// max_wait_ms, if the device memory the server holds for requests in flight
-// stays under its budget.  Batches run on their own streams with one block
-// per work item (a group of chains of one ligand), so a new batch's blocks
-// start as soon as earlier batches' blocks retire: the device keeps a mix of
-// requests in flight rather than a queue of whole batches.  Ligands of
-// different receptors share a batch (the kernel takes a table of map sets).
+// sg_serve_submit.  A worker thread uploads them in small batches (a batch
+// goes out as soon as the device can take it, or, under light load, once
+// the oldest request has waited max_wait_ms for others to share it) if the
+// device memory the server holds for requests in flight stays under its
+// budget.  A batch's work items (a group of chains of one ligand each) go
+// into a ring in device memory that a resident serving grid takes items
+// from while it runs: a ligand's chains start as soon as a block is free,
+// whatever batch it came with, so the device keeps a mix of requests in
+// flight rather than a queue of whole launches.  Ligands of different
+// receptors share a batch (every item names its receptor's map set).
 // The last chain of a ligand to finish raises a flag in host-mapped memory;
 // the worker then copies that ligand's chain results back, merges them
 // (min_rmsd 2) and refines the merged poses in FP64 on a separate stream,
@@ -129,7 +131,8 @@ struct SvBatch {
     size_t e_at = 0, conf_at = 0, xyz_at = 0, order_at = 0, count_at = 0, evals_at = 0, span_at = 0;
     int S = 20;
     uint64_t seq = 0;  // launch number (1, 2, ... per server)
-    cudaEvent_t kdone = nullptr;  // recorded once every ligand's chains are done (see worker)
+    char* pin = nullptr;           // pinned staging of its ring items and tail word
+    size_t pin_cap = 0;
     int flagged = 0;               // ligands whose completion flag has been seen
     int published = 0;
 };
@@ -150,7 +153,23 @@ struct Server {
     bool stopping = false;
     int error = SG_OK;
     std::string error_text;
-    std::vector<cudaStream_t> streams, free_streams;  // one launch in flight per stream
+    // serving grids: items wait in a ring in device memory that resident
+    // blocks take from; the worker starts blocks when items wait and no block
+    // is free (blocks leave after an idle time)
+    static constexpr unsigned kRing = 1u << 16;
+    FeedItem32* d_ring = nullptr;
+    FeedCtrl32* d_ctrl = nullptr;
+    FeedCtrl32* h_ctrl = nullptr;        // pinned snapshot of the control words
+    FeedCtrl32 seen{};                    // the last snapshot that landed
+    cudaEvent_t ctrl_ev = nullptr;
+    bool ctrl_pending = false;
+    uint64_t snap_req = 0, snap_seen = 0, launch_req = 0;  // snapshot requests, and the one a launch waits past
+    unsigned tail = 0;                    // items published
+    unsigned blocks_launched = 0;         // blocks of every grid started so far
+    int target_blocks = 0;                // serving blocks the device holds at once
+    long long idle_ns = 500000000;        // a block leaves after this long without work
+    cudaStream_t feed_stream = nullptr, ctrl_stream = nullptr;
+    std::vector<cudaStream_t> grid_streams;  // a grid per stream; grids end on their own
     int inflight_ligs = 0;
     cudaStream_t refine_stream = nullptr, copy_stream = nullptr;
     // completion flags in host-mapped memory
@@ -167,7 +186,6 @@ struct Server {
     std::vector<char*> pin_all;
     size_t smem_block = 0;  // dynamic shared memory of every search launch (same for all, set at start)
     static constexpr int kFlags = 1 << 16;
-    static constexpr int kMaxStreams = 112;  // concurrent kernels: 128 per device, some kept for refines and copies
 };
 
 static size_t req_bytes(const sg_model_desc& m, const sg_ligand_job& j, int S) {
@@ -195,21 +213,16 @@ static int serve_shape(const Server& s, size_t stage, size_t ws, int max_chains)
     return 0;
 }
 
-// Launches one batch; called by the worker with mu held.
+static char* pin_get(Server& s, size_t bytes, size_t& cap);
+
+// Uploads one batch and publishes its items to the serving grid's ring;
+// called by the worker with mu held.
 static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     sg_engine* e = s.e;
     auto b = std::make_unique<SvBatch>();
     const sg_mc_params& p = reqs[0].p;
     const int S = p.num_saved_mins;
     b->S = S;
-    if (s.free_streams.empty()) {
-        cudaStream_t st;
-        cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "serve: stream");
-        s.streams.push_back(st);
-        s.free_streams.push_back(st);
-    }
-    b->stream = s.free_streams.back();
-    s.free_streams.pop_back();
     std::vector<sg_model_desc> descs;
     for (auto& r : reqs) descs.push_back(r.m->d);
     size_t need = 0;
@@ -231,8 +244,6 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     const size_t maps_at = at; at = r16(at + SG_MAX_RECEPTORS * sizeof(DMaps32));
     const size_t boxes_at = at; at = r16(at + SG_MAX_RECEPTORS * 6 * sizeof(double));
     const size_t chains_at = at; at = r16(at + nchains * sizeof(Chain32));
-    const size_t items_at = at; at = r16(at + nchains * sizeof(Item32));
-    const size_t queue_at = at; at = r16(at + 256);
     const size_t cnt_at = at; at = r16(at + reqs.size() * sizeof(unsigned));
     b->e_at = at; at = r16(at + nchains * S * sizeof(double));
     b->conf_at = at; at = r16(at + nconf * sizeof(double));
@@ -242,9 +253,10 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     b->evals_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
     const size_t hits_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
     b->span_at = at; at = r16(at + nchains * 2 * sizeof(unsigned long long));
+    const size_t params_at = at; at = r16(at + sizeof(MCParams32));
     b->bytes = std::max(at, need);
     b->seq = ++s.launches;
-    cuda_check(cudaMallocAsync((void**)&b->dmem, b->bytes, b->stream), "serve: batch memory");
+    cuda_check(cudaMallocAsync((void**)&b->dmem, b->bytes, s.feed_stream), "serve: batch memory");
     pack_models_image(descs.data(), (int)descs.size(), b->dmem, b->img);
     // map sets and search boxes of every receptor
     std::vector<DMaps32> tab(SG_MAX_RECEPTORS);
@@ -335,7 +347,7 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
     std::vector<Item32> q(items.size());
     for (size_t k = 0; k < items.size(); k++) q[k] = items[order[k]];
-    cudaStream_t st = b->stream;
+    cudaStream_t st = s.feed_stream;
     cuda_check(cudaMemcpyAsync(b->dmem, b->img.bytes.data(), b->img.bytes.size(), cudaMemcpyHostToDevice, st), "serve");
     cuda_check(cudaMemcpyAsync(b->dmem + maps_at, tab.data(), tab.size() * sizeof(DMaps32), cudaMemcpyHostToDevice, st),
                "serve");
@@ -345,9 +357,6 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     cuda_check(cudaMemcpyAsync(b->dmem + chains_at, b->hc.data(), b->hc.size() * sizeof(Chain32),
                                cudaMemcpyHostToDevice, st),
                "serve");
-    cuda_check(cudaMemcpyAsync(b->dmem + items_at, q.data(), q.size() * sizeof(Item32), cudaMemcpyHostToDevice, st),
-               "serve");
-    cuda_check(cudaMemsetAsync(b->dmem + queue_at, 0, 256, st), "serve");
     cuda_check(cudaMemsetAsync(b->dmem + cnt_at, 0, reqs.size() * sizeof(unsigned) + 16, st), "serve");
     MCParams32 P{};
     for (int i = 0; i < 3; i++) {
@@ -364,18 +373,34 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     P.maxiters = p.maxiters;
     P.accurate_line = p.accurate_line;
     P.early_term = p.early_term;
-    // one block per work item, so blocks of later batches fill in as these retire
-    cuda_check(launch_mc32_fixed(reinterpret_cast<const DModel*>(b->dmem + b->img.dmodel_off), tables32(e), tab[0],
-                                 reinterpret_cast<const DMaps32*>(b->dmem + maps_at),
-                                 reinterpret_cast<const Chain32*>(b->dmem + chains_at),
-                                 reinterpret_cast<const Item32*>(b->dmem + items_at), (int)q.size(), P,
-                                 reinterpret_cast<unsigned*>(b->dmem + queue_at), (int)q.size(), wpb, stage_stride,
-                                 ws_stride, s.smem_block, st),
-               "serve: search launch");
-    // The kernel-end event is recorded only when every ligand of the batch has
-    // flagged completion: a command queued behind a kernel that runs for
-    // seconds would hold up the hardware queue it shares with other streams.
-    cuda_check(cudaEventCreateWithFlags(&b->kdone, cudaEventDisableTiming), "serve");
+    // the batch's items, in cost order, into the ring; then the tail word.
+    // Everything goes through the one feed stream, so the grid sees a tail
+    // only after the data it covers has landed.
+    const unsigned n = (unsigned)q.size();
+    require(s.tail + n - s.seen.head <= Server::kRing, "serve: work ring full");
+    const size_t pin_bytes = r16(sizeof(MCParams32)) + n * sizeof(FeedItem32) + 16;
+    b->pin = pin_get(s, pin_bytes, b->pin_cap);
+    std::memcpy(b->pin, &P, sizeof(MCParams32));
+    FeedItem32* fi = reinterpret_cast<FeedItem32*>(b->pin + r16(sizeof(MCParams32)));
+    const DModel* dms = reinterpret_cast<const DModel*>(b->dmem + b->img.dmodel_off);
+    const Chain32* dch = reinterpret_cast<const Chain32*>(b->dmem + chains_at);
+    const DMaps32* dmaps = reinterpret_cast<const DMaps32*>(b->dmem + maps_at);
+    for (unsigned k = 0; k < n; k++) {
+        fi[k] = FeedItem32{dms + q[k].model, dch + q[k].first, dmaps + q[k].rec,
+                           reinterpret_cast<const MCParams32*>(b->dmem + params_at), q[k].count, (int)stage_stride,
+                           (int)ws_stride, 0};
+    }
+    unsigned* tail_word = reinterpret_cast<unsigned*>(b->pin + r16(sizeof(MCParams32)) + n * sizeof(FeedItem32));
+    *tail_word = s.tail + n;
+    cuda_check(cudaMemcpyAsync(b->dmem + params_at, b->pin, sizeof(MCParams32), cudaMemcpyHostToDevice, st), "serve");
+    const unsigned at0 = s.tail % Server::kRing, first_part = std::min(n, Server::kRing - at0);
+    cuda_check(cudaMemcpyAsync(s.d_ring + at0, fi, first_part * sizeof(FeedItem32), cudaMemcpyHostToDevice, st), "serve");
+    if (first_part < n)
+        cuda_check(cudaMemcpyAsync(s.d_ring, fi + first_part, (n - first_part) * sizeof(FeedItem32),
+                                   cudaMemcpyHostToDevice, st),
+                   "serve");
+    cuda_check(cudaMemcpyAsync(&s.d_ctrl->tail, tail_word, sizeof(unsigned), cudaMemcpyHostToDevice, st), "serve");
+    s.tail += n;
     s.inflight_bytes += b->bytes;
     s.inflight_ligs += (int)b->ligs.size();
     s.inflight.push_back(std::move(b));
@@ -633,31 +658,59 @@ static void worker(Server* sp) {
     for (;;) {
         bool busy = false;
         try {
-            // 1. launch.  At most max_inflight_ligands ligands are on the device;
-            // the rest wait here, so a launch never queues on the GPU behind
-            // resident work.  A launch holds one of at most kMaxStreams
-            // concurrent kernels until its last ligand is done, so launches
-            // must carry several ligands each for the device to fill: while
-            // more requests wait than the device can take, a launch waits
-            // until a batch of `full` ligands fits (twice the ligands in
-            // flight per launch slot).  When everything queued fits, it goes
-            // at once if a full batch has queued, else after the oldest
-            // request has waited max_wait_ms (scaled up as launch slots run
-            // out) for others to share it.  Same search parameters per
-            // launch; device memory held for requests in flight stays under
-            // the budget.
-            const int in_use = (int)(s.streams.size() - s.free_streams.size());
-            if (!s.queue.empty() && in_use < Server::kMaxStreams) {
+            // 0. serving grids: a snapshot of the ring's control words (an
+            // async copy, read once it has landed); blocks are started when
+            // items wait and no block is free, counting blocks launched but
+            // not yet seen to start, and only on a snapshot taken after the
+            // last start
+            if (!s.ctrl_pending) {
+                cuda_check(cudaMemcpyAsync(s.h_ctrl, s.d_ctrl, sizeof(FeedCtrl32), cudaMemcpyDeviceToHost,
+                                           s.ctrl_stream),
+                           "serve: control words");
+                cuda_check(cudaEventRecord(s.ctrl_ev, s.ctrl_stream), "serve: control words");
+                s.ctrl_pending = true;
+                s.snap_req++;
+            } else if (event_done(s.ctrl_ev)) {
+                s.ctrl_pending = false;
+                s.seen = *s.h_ctrl;
+                s.snap_seen = s.snap_req;
+            }
+            if (s.tail != s.seen.head && s.seen.waiting == 0 && s.snap_seen > s.launch_req) {
+                const int live = (int)(s.blocks_launched - s.seen.exited);
+                const int more = s.target_blocks - live;
+                if (more > 0) {
+                    cudaStream_t gs = nullptr;
+                    for (cudaStream_t c : s.grid_streams)
+                        if (cudaStreamQuery(c) == cudaSuccess) { gs = c; break; }
+                    if (!gs && s.grid_streams.size() < 32) {
+                        cuda_check(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking), "serve: stream");
+                        s.grid_streams.push_back(gs);
+                    }
+                    if (gs) {
+                        cuda_check(launch_mc32_feed(tables32(s.e), s.d_ring, Server::kRing, s.d_ctrl, s.idle_ns, more, 8,
+                                                    s.smem_block, gs),
+                                   "serve: search grid");
+                        s.blocks_launched += (unsigned)more;
+                        s.launch_req = s.snap_req;
+                        busy = true;
+                    }
+                }
+            }
+            // 1. upload.  At most max_inflight_ligands ligands are on the device;
+            // the rest wait here.  While more requests wait than the device can
+            // take, a batch goes out as soon as any fits; when everything
+            // queued fits, it goes once a full batch has queued or the oldest
+            // request has waited max_wait_ms for others to share it.  Same
+            // search parameters per batch; device memory held for requests in
+            // flight stays under the budget.
+            if (!s.queue.empty()) {
                 const double waited =
                     std::chrono::duration<double, std::milli>(Clock::now() - s.queue.front().t_submit).count();
-                const int slots = Server::kMaxStreams - in_use;
                 const int open = std::max(0, s.o.max_inflight_ligands - s.inflight_ligs);
                 const int q = (int)s.queue.size();
                 const int want = std::min({q, open, s.o.max_batch_ligands, (int)s.free_flags.size()});
-                const int full = std::min(s.o.max_batch_ligands,
-                                          2 * ((s.o.max_inflight_ligands + Server::kMaxStreams - 1) / Server::kMaxStreams));
-                const double gather_ms = s.o.max_wait_ms * (double)Server::kMaxStreams / slots;
-                const bool go = want > 0 && (want >= full || s.stopping || (q <= open && waited >= gather_ms));
+                const bool go = want > 0 && (q > open || want >= s.o.max_batch_ligands || s.stopping ||
+                                             waited >= s.o.max_wait_ms);
                 if (go) {
                     std::vector<ServeReq> take;
                     size_t bytes = 0;
@@ -697,8 +750,7 @@ static void worker(Server* sp) {
                     if (L.state == 0 && s.flags[L.flag]) {
                         fetch_merge(s, *b, L);
                         fin.emplace_back(b.get(), &L);
-                        if (++b->flagged == (int)b->ligs.size())  // its blocks are retiring now
-                            cuda_check(cudaEventRecord(b->kdone, b->stream), "serve: kernel end");
+                        ++b->flagged;
                     }
             if (!fin.empty()) {
                 launch_refines(s, fin);
@@ -721,14 +773,13 @@ static void worker(Server* sp) {
                     i++;
                 }
             }
-            // 3. retire batches whose kernel ended and whose ligands are all published
+            // 3. retire batches whose ligands are all published (their chains
+            // have signalled completion, their last access to the batch)
             for (size_t i = 0; i < s.inflight.size();) {
                 SvBatch& b = *s.inflight[i];
-                if (b.flagged == (int)b.ligs.size() && b.published == (int)b.ligs.size() &&
-                    event_done(b.kdone)) {
-                    cuda_check(cudaFreeAsync(b.dmem, b.stream), "serve: free batch");
-                    cudaEventDestroy(b.kdone);
-                    s.free_streams.push_back(b.stream);
+                if (b.flagged == (int)b.ligs.size() && b.published == (int)b.ligs.size()) {
+                    cuda_check(cudaFreeAsync(b.dmem, s.feed_stream), "serve: free batch");
+                    pin_put(s, b.pin, b.pin_cap);
                     s.inflight_bytes -= b.bytes;
                     s.inflight.erase(s.inflight.begin() + i);
                     busy = true;
@@ -744,11 +795,11 @@ static void worker(Server* sp) {
                 if (herr != kDevOk)
                     throw EngineError(herr == kDevOverlap ? SG_ERR_OVERLAP : SG_ERR_ARG,
                                       "serve: device reported error " + std::to_string(herr));
-                // a launch that failed on the device never raises its flags: the
-                // first batch's stream reports the error instead
-                if (!s.inflight.empty()) {
-                    const cudaError_t q = cudaStreamQuery(s.inflight.front()->stream);
-                    if (q != cudaSuccess && q != cudaErrorNotReady) cuda_check(q, "serve: search kernel");
+                // a grid that failed on the device never raises its flags: its
+                // stream reports the error instead
+                for (cudaStream_t c : s.grid_streams) {
+                    const cudaError_t q = cudaStreamQuery(c);
+                    if (q != cudaSuccess && q != cudaErrorNotReady) cuda_check(q, "serve: search grid");
                 }
             }
         } catch (EngineError& x) {
@@ -763,6 +814,33 @@ static void worker(Server* sp) {
         else std::this_thread::sleep_for(std::chrono::microseconds(100));
         lk.lock();
     }
+}
+
+// Ends the serving grids (their blocks see stop within one sleep step, or
+// leave after their idle time) and frees the ring.
+static void stop_grids(Server& s) {
+    if (s.d_ctrl) {
+        const unsigned one = 1;
+        cudaMemcpy(&s.d_ctrl->stop, &one, sizeof(unsigned), cudaMemcpyHostToDevice);
+    }
+    for (cudaStream_t c : s.grid_streams) {
+        cudaStreamSynchronize(c);
+        cudaStreamDestroy(c);
+    }
+    s.grid_streams.clear();
+    if (s.feed_stream) cudaStreamSynchronize(s.feed_stream);
+    if (s.ctrl_stream) cudaStreamSynchronize(s.ctrl_stream);
+    if (s.feed_stream) cudaStreamDestroy(s.feed_stream);
+    if (s.ctrl_stream) cudaStreamDestroy(s.ctrl_stream);
+    if (s.ctrl_ev) cudaEventDestroy(s.ctrl_ev);
+    if (s.d_ring) cudaFree(s.d_ring);
+    if (s.d_ctrl) cudaFree(s.d_ctrl);
+    if (s.h_ctrl) cudaFreeHost(s.h_ctrl);
+    s.feed_stream = s.ctrl_stream = nullptr;
+    s.ctrl_ev = nullptr;
+    s.d_ring = nullptr;
+    s.d_ctrl = nullptr;
+    s.h_ctrl = nullptr;
 }
 
 }  // namespace sg
@@ -787,6 +865,7 @@ void sg::serve_shutdown(sg_engine* e) {
         s->stopping = true;
     }
     if (s->th.joinable()) s->th.join();
+    stop_grids(*s);
     std::lock_guard<std::mutex> lk(g_srv_mu);
     g_servers.erase(e);
 }
@@ -817,11 +896,11 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
         // the driver's reserve), so that the largest ligands also run eight
         // chains per block; block_smem_bytes overrides it.
         size_t dyn_max = 0, two_per_sm = 0;
-        cuda_check(mc32_max_dynamic_smem((size_t)e->max_smem, &dyn_max), "serve: kernel attributes");
+        cuda_check(mc32_feed_max_dynamic_smem((size_t)e->max_smem, &dyn_max), "serve: kernel attributes");
         int per_sm = 0, reserved = 0;
         cuda_check(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, e->device), "serve");
         cuda_check(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, e->device), "serve");
-        cuda_check(mc32_max_dynamic_smem((size_t)std::max(0, per_sm / 2 - reserved), &two_per_sm), "serve");
+        cuda_check(mc32_feed_max_dynamic_smem((size_t)std::max(0, per_sm / 2 - reserved), &two_per_sm), "serve");
         if (s->o.block_smem_bytes > 0) {
             require((size_t)s->o.block_smem_bytes <= dyn_max, "serve: block_smem_bytes above the device's limit");
             s->smem_block = (size_t)s->o.block_smem_bytes;
@@ -829,7 +908,22 @@ int sg_serve_start(sg_engine* e, const sg_serve_opts* o) {
             s->smem_block = std::min(dyn_max, two_per_sm & ~(size_t)1023);
         }
         require(s->smem_block >= 4096, "serve: too little shared memory per block");
-        cuda_check(mc32_reserve_smem(s->smem_block), "serve: kernel attributes");
+        cuda_check(mc32_feed_reserve_smem(s->smem_block), "serve: kernel attributes");
+        {   // serving blocks the device holds at once (8-warp blocks at the fixed
+            // shared memory), less 16, so that the FP64 refinements find room
+            int per = 0;
+            cuda_check(mc32_feed_occupancy(8, s->smem_block, &per), "serve: occupancy");
+            require(per > 0, "serve: the serving block does not fit an SM");
+            s->target_blocks = std::max(1, per * e->num_sms - 16);
+        }
+        cuda_check(cudaMalloc((void**)&s->d_ring, (size_t)Server::kRing * sizeof(FeedItem32)), "serve: work ring");
+        cuda_check(cudaMalloc((void**)&s->d_ctrl, sizeof(FeedCtrl32)), "serve: work ring");
+        cuda_check(cudaMemset(s->d_ctrl, 0, sizeof(FeedCtrl32)), "serve: work ring");
+        cuda_check(cudaHostAlloc((void**)&s->h_ctrl, sizeof(FeedCtrl32), cudaHostAllocDefault), "serve: work ring");
+        std::memset(s->h_ctrl, 0, sizeof(FeedCtrl32));
+        cuda_check(cudaEventCreateWithFlags(&s->ctrl_ev, cudaEventDisableTiming), "serve: event");
+        cuda_check(cudaStreamCreateWithFlags(&s->feed_stream, cudaStreamNonBlocking), "serve: stream");
+        cuda_check(cudaStreamCreateWithFlags(&s->ctrl_stream, cudaStreamNonBlocking), "serve: stream");
         cuda_check(cudaStreamCreateWithFlags(&s->refine_stream, cudaStreamNonBlocking), "serve: stream");
         cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "serve: stream");
         unsigned* hf = nullptr;
@@ -968,10 +1062,9 @@ int sg_serve_stop(sg_engine* e) {
             s->stopping = true;
         }
         if (s->th.joinable()) s->th.join();
-        for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+        stop_grids(*s);
         cudaStreamSynchronize(s->refine_stream);
         cudaStreamSynchronize(s->copy_stream);
-        for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
         cudaStreamDestroy(s->refine_stream);
         cudaStreamDestroy(s->copy_stream);
         cudaFreeHost((void*)s->flags);

@@ -128,7 +128,7 @@ struct DTables32 {
 
 // packed-corner grid maps: each cell's 8 corner values contiguous
 // FP32: 2 x float4 = (f000 f100 f010 f110)(f001 f101 f011 f111); FP16: 1 x uint4
-struct DMaps32 {
+struct __align__(16) DMaps32 {
     int cdim[3];  // cells per axis (dim - 1)
     float init[3], factor[3], factor_inv[3], dim_fl_minus_1[3];
     const float4* m32[kNumTypes];
@@ -138,7 +138,7 @@ struct DMaps32 {
 };
 
 // Chain bookkeeping of the batched mixed-precision path
-struct Chain32 {
+struct __align__(16) Chain32 {
     int model;
     unsigned steps;
     int maxiters;            // BFGS iterations of this ligand's search
@@ -158,6 +158,30 @@ struct Chain32 {
     int lig_chains;
     const double* box;  // search box (lo xyz, hi xyz) of this chain's receptor; null: the launch's
     unsigned long long* span;  // [2] device clock (ns) at the chain's start and end; null: not recorded
+};
+
+struct __align__(16) MCParams32;
+
+// A serving grid's unit of work, published by the host in a ring while the
+// grid runs: up to a block's worth of chains of one ligand, with everything
+// the block needs to run them (all in the memory of the ligand's batch)
+struct __align__(16) FeedItem32 {
+    const DModel* model;
+    const Chain32* chains;     // [count]
+    const DMaps32* maps;       // the ligand's receptor's map set
+    const MCParams32* params;
+    int count;                 // chains (warps) of this item
+    int stage_stride;          // shared-memory layout of the item's block
+    int ws_stride;
+    int pad_;
+};
+// The ring's control words (device memory): the host advances tail after
+// copying items in; blocks claim items by advancing head
+struct FeedCtrl32 {
+    unsigned head, tail;
+    unsigned started, exited, waiting;  // blocks of serving grids
+    unsigned stop;                      // set by the host to end the grids
+    unsigned pad_[2];
 };
 
 // A block's unit of work: chains [first, first + count) of one model
@@ -224,7 +248,7 @@ SG_HD int stage32_bytes(int natoms, int nframes, int nheavy, int npchunks, int n
            r(4 * nheavy) + r(128 * npchunks) + 3 * r(4 * nlig) + 3 * r(4 * nblocks) + 2 * r(4 * ntors);
 }
 
-struct MCParams32 {
+struct __align__(16) MCParams32 {
     float hunt[3], auth[3];
     float slope;
     double temperature, amplitude, min_rmsd;

@@ -399,25 +399,24 @@ int sg_autotune32(sg_engine* e, int receptor_id, const sg_model_desc* models, in
 /* ---- serving: a request loop with continuous batching ------------------
  * No counterpart in the reference (its screens are offline batches).
  * Requests (one ligand against one resident receptor) are queued by
- * sg_serve_submit; a worker thread launches them as they arrive (in bigger
- * launches once the device is full), ligands of different receptors in the
- * same launch, each launch on its own stream with one block per group of
- * chains, so new launches fill the GPU as older work retires.
+ * sg_serve_submit; a worker thread uploads them in small batches as they
+ * arrive and publishes their work items (a group of chains of one ligand
+ * each) to a ring in device memory.  A resident serving grid takes items
+ * from the ring while it runs, so a ligand's chains start as soon as a
+ * block is free, whatever batch it came with; ligands of different
+ * receptors mix freely.  Blocks that find no work for a while leave, and
+ * the worker starts blocks again when items wait and none is free.
  * Admission keeps the device memory held for requests in flight under
  * hbm_budget_bytes.  Each ligand is merged and refined (FP64) as soon as its
  * own chains finish.  A result equals sg_dock_batch32's (refine = 1) for the
  * same (seed, ligand_key), alone or in any mix.  While a server runs, the
- * engine's other entry points must not be called except sg_serve_*.
- * Launches go to up to 112 streams; with the driver's default of 8 hardware
- * queues, streams share queues, so set CUDA_DEVICE_MAX_CONNECTIONS=32 in the
- * environment before the process creates its CUDA context. */
+ * engine's other entry points must not be called except sg_serve_*. */
 typedef struct sg_serve_opts {
     uint64_t hbm_budget_bytes;  /* 0: a quarter of the free device memory   */
-    int max_batch_ligands;      /* ligands per launch (0: 64)                */
-    double max_wait_ms;         /* how long the oldest request may wait for
-                                   others to share its launch, scaled up as
-                                   the concurrent launches (at most 112) run
-                                   out (0: 20 ms)                            */
+    int max_batch_ligands;      /* ligands per upload batch (0: 64)          */
+    double max_wait_ms;         /* under light load, how long the oldest
+                                   request may wait for others to share its
+                                   batch (0: 20 ms)                          */
     int max_inflight_ligands;   /* at most this many ligands on the device;
                                    later requests wait in the server's queue
                                    (0: two per SM, what the device holds at
@@ -435,13 +434,13 @@ typedef struct sg_serve_done {
     int conf_size, num_heavy;  /* sizes for sg_serve_fetch's arrays         */
     uint64_t evals;            /* eval_deriv calls of the search            */
     double latency_ms;         /* submit to result                          */
-    uint64_t launch;           /* the search launch it ran in (1, 2, ...)   */
+    uint64_t launch;           /* the upload batch it came with (1, 2, ...) */
     uint64_t device_start_ns;  /* device clock (%globaltimer, ns) when its
                                   first chain started ...                   */
     uint64_t device_end_ns;    /* ... and when its last chain ended; two
                                   requests of different launches whose
                                   spans overlap were on the device at once  */
-    double queue_ms;           /* submit to launch (waiting in the server's
+    double queue_ms;           /* submit to upload (waiting in the server's
                                   queue)                                    */
     double searched_ms;        /* submit to the worker seeing its chains
                                   done (then merge and FP64 refinement)     */
