@@ -84,6 +84,8 @@ struct sg_engine {
     bool has_tables = false;
     sg::DevBuf tab_smooth, tab_fast, tab32;
     int force_wpb = 0, last_wpb = 0, last_blocks = 0;
+    bool es_on = false;   // early stop of the batched search (--fast; sg_set_early_stop)
+    sg_early_stop es{};
     double last_mc_ms = 0, last_refine_ms = 0;
     uint64_t last_evals = 0, last_grid_hits = 0, last_pair_hits = 0, last_h2d = 0, last_d2h = 0;
     sg::DTables tables{};

@@ -173,7 +173,6 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         d_evals.alloc((size_t)nchains * sizeof(unsigned long long));
         d_hits.alloc((size_t)nchains * 2 * sizeof(unsigned long long));
         d_queue.alloc(sizeof(unsigned));
-        cuda_check(cudaMemsetAsync(d_queue.p, 0, sizeof(unsigned), e->stream), "queue reset");
         for (int k = 0; k < nchains; k++) {
             Chain32& ch = hc[k];
             ch.out_e = d_e.as<double>() + (size_t)k * S;
@@ -190,27 +189,6 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         for (int j = 0; j < njobs; j++) max_chains = std::max(max_chains, jobs[j].num_chains);
         int wpb = 1, occ = 1;
         choose_launch(e, stage_stride, ws_stride, max_chains, wpb, occ);
-        std::vector<Item32> items;
-        std::vector<double> item_cost;
-        for (int k = 0; k < nchains;) {
-            const int j = chain_job[k];
-            int n = 0;
-            while (k + n < nchains && chain_job[k + n] == j && n < wpb) n++;
-            items.push_back(Item32{hc[k].model, k, n, 0});
-            item_cost.push_back((double)hc[k].steps * pm.host[hc[k].model].cost * std::max(1, hc[k].maxiters));
-            k += n;
-        }
-        std::vector<int> order(items.size());
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_cost[a] > item_cost[b]; });
-        std::vector<Item32> queue(items.size());
-        for (size_t k = 0; k < items.size(); k++) queue[k] = items[order[k]];
-        const int nitems = (int)queue.size();
-        const int blocks = (int)std::min<long long>((long long)occ * e->num_sms, nitems);
-        DevBuf d_chains, d_items;
-        d_chains.upload(hc.data(), hc.size() * sizeof(Chain32), e->stream);
-        d_items.upload(queue.data(), queue.size() * sizeof(Item32), e->stream);
-        h2d += d_chains.bytes + d_items.bytes;
         MCParams32 P{};
         for (int i = 0; i < 3; i++) {
             P.hunt[i] = (float)p->hunt_cap[i];
@@ -226,18 +204,123 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         P.maxiters = p->maxiters;
         P.accurate_line = p->accurate_line;
         P.early_term = p->early_term;
+        // Early stop (--fast): phases ending at (first + k) / checkpoints of
+        // every chain's steps, each resuming from the state the previous one
+        // saved; the stopping rule between phases.  Without it, one phase.
+        const bool phased = e->es_on;
+        int es_n = 1, es_first = 1;
+        if (phased) {
+            es_n = std::max(1, e->es.checkpoints);
+            es_first = std::min(es_n, std::max(1, e->es.first));
+        }
+        const int nphases = es_n - es_first + 1;
+        std::vector<size_t> res_off(nchains, 0);
+        DevBuf d_resume;
+        if (phased) {
+            size_t nres = 0;
+            for (int k = 0; k < nchains; k++) {
+                const DModel& h = pm.host[hc[k].model];
+                res_off[k] = nres;
+                nres += (resume32_doubles(h.conf_size, h.natoms, h.nframes) + 1) & ~(size_t)1;  // 16-byte pieces
+            }
+            d_resume.alloc(std::max<size_t>(1, nres) * sizeof(double));
+            for (int k = 0; k < nchains; k++) hc[k].resume = d_resume.as<double>() + res_off[k];
+        }
+        std::vector<unsigned> done(nchains, 0);
+        std::vector<char> stopped(njobs, 0);
+        std::vector<double> hres;
+        DevBuf d_chains, d_items;
+        float mc_ms = 0;
+        int first_blocks = 0;
         cudaEvent_t ev[4];
         for (auto& x : ev) cuda_check(cudaEventCreate(&x), "event");
         struct EvGuard {
             cudaEvent_t* v;
             ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(v[i]); }
         } evg{ev};
-        cuda_check(cudaEventRecord(ev[0], e->stream), "event");
-        cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), nullptr, d_chains.as<Chain32>(),
-                               d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb, stage_stride,
-                               ws_stride, e->stream),
-                   "search launch");
-        cuda_check(cudaEventRecord(ev[1], e->stream), "event");
+        for (int ph = 0; ph < nphases; ph++) {
+            std::vector<int> active;
+            for (int k = 0; k < nchains; k++) {
+                if (stopped[chain_job[k]]) continue;
+                const unsigned steps = hc[k].steps;
+                const unsigned end = ph + 1 < nphases
+                                         ? (unsigned)(((unsigned long long)steps * (es_first + ph) + es_n - 1) / es_n)
+                                         : steps;
+                if (end <= done[k]) continue;
+                hc[k].begin = done[k];
+                hc[k].end = end;
+                done[k] = end;
+                active.push_back(k);
+            }
+            if (active.empty()) continue;
+            std::vector<Item32> items;
+            std::vector<double> item_cost;
+            for (size_t a = 0; a < active.size();) {
+                const int k = active[a], j = chain_job[k];
+                int n = 0;
+                while (a + n < active.size() && chain_job[active[a + n]] == j && n < wpb &&
+                       active[a + n] == k + n)
+                    n++;
+                items.push_back(Item32{hc[k].model, k, n, 0});
+                item_cost.push_back((double)(hc[k].end - hc[k].begin) * pm.host[hc[k].model].cost *
+                                    std::max(1, hc[k].maxiters));
+                a += n;
+            }
+            std::vector<int> order(items.size());
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return item_cost[x] > item_cost[y]; });
+            std::vector<Item32> queue(items.size());
+            for (size_t k = 0; k < items.size(); k++) queue[k] = items[order[k]];
+            const int nitems = (int)queue.size();
+            const int blocks = (int)std::min<long long>((long long)occ * e->num_sms, nitems);
+            if (ph == 0) first_blocks = blocks;
+            d_chains.upload(hc.data(), hc.size() * sizeof(Chain32), e->stream);
+            d_items.upload(queue.data(), queue.size() * sizeof(Item32), e->stream);
+            h2d += d_chains.bytes + d_items.bytes;
+            cuda_check(cudaMemsetAsync(d_queue.p, 0, sizeof(unsigned), e->stream), "queue reset");
+            cuda_check(cudaEventRecord(ev[0], e->stream), "event");
+            cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), nullptr, d_chains.as<Chain32>(),
+                                   d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb, stage_stride,
+                                   ws_stride, e->stream),
+                       "search launch");
+            cuda_check(cudaEventRecord(ev[1], e->stream), "event");
+            if (phased && ph + 1 < nphases) {  // the stopping rule on the best energies the chains saved
+                hres.resize(d_resume.bytes / sizeof(double));
+                cuda_check(cudaMemcpyAsync(hres.data(), d_resume.p, d_resume.bytes, cudaMemcpyDeviceToHost, e->stream),
+                           "best energies");
+                d2h += d_resume.bytes;
+            }
+            cuda_check(cudaStreamSynchronize(e->stream), "search");
+            float ms = 0;
+            cuda_check(cudaEventElapsedTime(&ms, ev[0], ev[1]), "event time");
+            mc_ms += ms;
+            if (phased && ph + 1 < nphases) {
+                const int cpu = e->es.chains_per_unit;
+                for (int k0 = 0; k0 < nchains;) {  // per job: its units' best energies
+                    const int j = chain_job[k0];
+                    int k1 = k0;
+                    while (k1 < nchains && chain_job[k1] == j) k1++;
+                    if (!stopped[j]) {
+                        std::vector<double> ub;
+                        for (int k = k0; k < k1; k++) {
+                            const size_t u = (size_t)((k - k0) / cpu);
+                            if (ub.size() <= u) ub.resize(u + 1, DBL_MAX);
+                            const int cs = pm.host[hc[k].model].conf_size;
+                            ub[u] = std::min(ub[u], hres[res_off[k] + cs + 1]);
+                        }
+                        if (ub.size() >= 2) {
+                            const double best = *std::min_element(ub.begin(), ub.end());
+                            int agree = 0;
+                            for (double v : ub) agree += (v - best <= e->es.eps);
+                            const int need = std::max(2, (int)std::ceil(e->es.fraction * ub.size() - 1e-9));
+                            if (agree >= need) stopped[j] = 1;
+                        }
+                    }
+                    k0 = k1;
+                }
+            }
+        }
+        const int blocks = first_blocks;
         std::vector<double> he((size_t)nchains * S), hconf(nconf_res);
         std::vector<float> hxyz(nxyz_res);
         std::vector<int> horder((size_t)nchains * S), hcount(nchains);
@@ -255,8 +338,6 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         fetch(hev.data(), d_evals, hev.size() * sizeof(unsigned long long));
         fetch(hhits.data(), d_hits, hhits.size() * sizeof(unsigned long long));
         cuda_check(cudaStreamSynchronize(e->stream), "search");
-        float mc_ms = 0;
-        cuda_check(cudaEventElapsedTime(&mc_ms, ev[0], ev[1]), "event time");
         // merge_output_containers per ligand (chains in job order)
         std::vector<std::vector<HostPose>> merged(njobs);
         std::vector<uint64_t> job_evals(njobs, 0);
@@ -381,6 +462,20 @@ int sg_profile_read(unsigned long long* out16, int clear) {
     return profile_read32(out16, clear != 0) == cudaSuccess ? SG_OK : SG_ERR_CUDA;
 }
 #endif
+
+int sg_set_early_stop(sg_engine* e, const sg_early_stop* es) {
+    if (!e) return SG_ERR_ARG;
+    if (!es) {
+        e->es_on = false;
+        return SG_OK;
+    }
+    if (e->precision == SG_PREC_FP64 || es->checkpoints < 1 || es->checkpoints > 1000 || es->first < 1 ||
+        !(es->fraction >= 0 && es->fraction <= 1) || !(es->eps == es->eps) || es->chains_per_unit < 1)
+        return SG_ERR_ARG;
+    e->es = *es;
+    e->es_on = true;
+    return SG_OK;
+}
 
 int sg_set_chains_per_block(sg_engine* e, int n) {
     if (!e || !(n == 0 || n == 1 || n == 2 || n == 4 || n == 8)) return SG_ERR_ARG;

@@ -481,22 +481,36 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
     for (int i = w.lane; i < 65; i += 32) C[i] = 0;
     const int cs = m.conf_size;
     // model state as read (mutation may read it before the first set)
-    // (L2-only loads: a serving grid may read a ligand placed where an earlier
-    // one was, and this SM's L1 may still hold the earlier one's lines)
-    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldcg(m.lab32 + i);
-    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldcg(m.finit32 + f);
-    __syncwarp();
-    Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
+    const unsigned first = ch.begin, last = ch.end ? ch.end : ch.steps;
+    const bool resumed = ch.resume && first > 0;
     const int tmp_at = w.at(L.x_tmp), cand_at = w.at(L.x_cand);
     double* tmp = sp<double>(tmp_at);
     double* cand = sp<double>(cand_at);
-    randomize32(w, rng, tmp, ch.box ? ch.box : P.box);
-    const Mode32 hunt{make_float3(P.hunt[0], P.hunt[1], P.hunt[2]), P.slope};
-    const Mode32 auth{make_float3(P.auth[0], P.auth[1], P.auth[2]), P.slope};
+    Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
     double tmp_e = 0, best_e = kMaxFl;
     int count = 0;
-    if (w.lane == 0) *ch.out_count = 0;
-    for (unsigned step = 0; step < ch.steps; step++) {
+    const float4* saved_xyz = ch.resume ? reinterpret_cast<const float4*>(ch.resume + resume32_coords_at(cs)) : nullptr;
+    if (resumed) {  // a later phase: the state the previous one saved
+        for (int i = w.lane; i < cs; i += 32) tmp[i] = ch.resume[i];
+        for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = saved_xyz[i];
+        for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = saved_xyz[m.natoms + f];
+        tmp_e = ch.resume[cs];
+        best_e = ch.resume[cs + 1];
+        rng.n = (uint32_t)ch.resume[cs + 2];
+        count = *ch.out_count;
+        __syncwarp();
+    } else {
+        // (L2-only loads: a serving grid may read a ligand placed where an
+        // earlier one was, and this SM's L1 may still hold the earlier one's lines)
+        for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldcg(m.lab32 + i);
+        for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldcg(m.finit32 + f);
+        __syncwarp();
+        randomize32(w, rng, tmp, ch.box ? ch.box : P.box);
+        if (w.lane == 0) *ch.out_count = 0;
+    }
+    const Mode32 hunt{make_float3(P.hunt[0], P.hunt[1], P.hunt[2]), P.slope};
+    const Mode32 auth{make_float3(P.auth[0], P.auth[1], P.auth[2]), P.slope};
+    for (unsigned step = first; step < last; step++) {
         SG_T0(t_mut);
         copyd(w, cand, tmp, cs);
         mutate32(w, rng, cand, P.amplitude);
@@ -517,15 +531,26 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
         }
     }
     __syncwarp();
+    if (ch.resume) {  // the state a later phase resumes from (and the best energy, for the stopping rule)
+        float4* sx = reinterpret_cast<float4*>(ch.resume + resume32_coords_at(cs));
+        for (int i = w.lane; i < cs; i += 32) ch.resume[i] = tmp[i];
+        for (int i = w.lane; i < m.natoms; i += 32) sx[i] = w.coords()[i];
+        for (int f = w.lane; f < m.nframes; f += 32) sx[m.natoms + f] = w.origin()[f];
+        if (w.lane == 0) {
+            ch.resume[cs] = tmp_e;
+            ch.resume[cs + 1] = best_e;
+            ch.resume[cs + 2] = (double)rng.n;
+        }
+    }
     unsigned long long gh = C[w.lane], ph = C[32 + w.lane];
     for (int o = 16; o > 0; o >>= 1) {
         gh += __shfl_xor_sync(kFull32, gh, o);
         ph += __shfl_xor_sync(kFull32, ph, o);
     }
     if (w.lane == 0) {
-        *ch.evals = C[64];
-        ch.hits[0] = gh;
-        ch.hits[1] = ph;
+        *ch.evals = (resumed ? *ch.evals : 0ull) + C[64];
+        ch.hits[0] = (resumed ? ch.hits[0] : 0ull) + gh;
+        ch.hits[1] = (resumed ? ch.hits[1] : 0ull) + ph;
         if (ch.span) ch.span[1] = global_ns();
         if (ch.done_count) {
             __threadfence();  // this chain's results, before its count

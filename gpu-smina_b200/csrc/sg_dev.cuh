@@ -158,7 +158,18 @@ struct __align__(16) Chain32 {
     int lig_chains;
     const double* box;  // search box (lo xyz, hi xyz) of this chain's receptor; null: the launch's
     unsigned long long* span;  // [2] device clock (ns) at the chain's start and end; null: not recorded
+    // phased runs (early stop): this launch runs steps [begin, end) (end 0:
+    // all steps), resuming from and saving to resume (resume32_doubles);
+    // null resume: one run of all steps
+    unsigned begin, end;
+    double* resume;
 };
+// a phased chain's saved state: conf, current and best energy, the Philox
+// draw index, then (16-byte aligned) its atoms' and frames' positions
+SG_HD int resume32_coords_at(int conf_size) { return (conf_size + 4) & ~1; }
+SG_HD size_t resume32_doubles(int conf_size, int natoms, int nframes) {
+    return (size_t)resume32_coords_at(conf_size) + 2 * (size_t)(natoms + nframes);
+}
 
 struct __align__(16) MCParams32;
 

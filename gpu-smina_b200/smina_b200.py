@@ -81,6 +81,11 @@ class LigandResult(C.Structure):
     _fields_ = [("count", C.c_int), ("e", _dp), ("conf", _dp), ("coords", _dp), ("evals", C.c_uint64)]
 
 
+class EarlyStop(C.Structure):
+    _fields_ = [("checkpoints", C.c_int), ("first", C.c_int), ("fraction", C.c_double), ("eps", C.c_double),
+                ("chains_per_unit", C.c_int)]
+
+
 class ServeOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_ligands", C.c_int), ("max_wait_ms", C.c_double),
                 ("max_inflight_ligands", C.c_int), ("block_smem_bytes", C.c_int)]
@@ -163,6 +168,7 @@ def _declare(L):
         "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
         "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
         "sg_set_chains_per_block": [vp, C.c_int],
+        "sg_set_early_stop": [vp, C.c_void_p],
         "sg_autotune32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
                           C.POINTER(MCParams), C.c_double, _dp, _ip],
         "sg_serve_start": [vp, C.POINTER(ServeOpts)],
@@ -655,6 +661,14 @@ class Engine:
 
     def set_chains_per_block(self, n: int):
         self._check(load().sg_set_chains_per_block(self._h, n))
+
+    def set_early_stop(self, checkpoints=10, first=2, fraction=0.5, eps=0.05, chains_per_unit=1, off=False):
+        """--fast's early stop for later dock_batch calls (sg_set_early_stop); off=True turns it off."""
+        if off:
+            self._check(load().sg_set_early_stop(self._h, None))
+        else:
+            es = EarlyStop(checkpoints, first, fraction, eps, chains_per_unit)
+            self._check(load().sg_set_early_stop(self._h, C.cast(C.byref(es), C.c_void_p)))
 
     def autotune(self, rid, models, jobs, params: MCParams, step_fraction=0.01):
         """Times the search at 8, 4, 2 and 1 chains per block on ``jobs`` with

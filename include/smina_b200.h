@@ -368,6 +368,27 @@ int sg_dock_batch32_noalloc(sg_engine* e, int receptor_id, const sg_model_desc* 
  * (1e9 bytes per second).  Allocates and frees the buffer itself. */
 int sg_probe_gather(sg_engine* e, uint64_t working_set_bytes, int bytes_per_lookup, double* out_gbs);
 
+/* --fast's early stop for sg_dock_batch32 (not smina's search; EarlyStop,
+ * src/gpu/gpu_kernels.h:45-56, applied as run_monte_carlo does,
+ * src/gpu/gpu_kernels_impl.cuh:607-657,740-810): the chains run in phases
+ * ending at first / checkpoints, (first + 1) / checkpoints, ... of their
+ * steps, each phase resuming exactly where the previous one stopped; after
+ * every phase but the last, a ligand whose chains form u >= 2 units of
+ * chains_per_unit consecutive chains stops when at least
+ * max(2, ceil(fraction * u)) of its units' best energies are within eps of
+ * its best.  A ligand that never stops gets the results it gets without
+ * early stop, bit for bit.  es == NULL turns it off; the setting stays on
+ * the engine for later sg_dock_batch32 calls.  FP32 engines only. */
+typedef struct sg_early_stop {
+    int checkpoints;      /* phases end at (first + k) / checkpoints (10)     */
+    int first;            /* the first check (2)                              */
+    double fraction;      /* share of a ligand's units that must agree (0.5)  */
+    double eps;           /* kcal/mol within the ligand's best (0.05)         */
+    int chains_per_unit;  /* consecutive chains of a job that form a unit
+                             (the --fast chain split; 1: every chain)         */
+} sg_early_stop;
+int sg_set_early_stop(sg_engine* e, const sg_early_stop* es);
+
 /* Timing and launch shape of the last sg_dock_batch32 call. */
 int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
                    int* chains_per_block, int* blocks);

@@ -17,13 +17,14 @@
  *     For FP64 engines these are the states the plain kernels start from, as
  *     the reference's --gpu_fp64 chains start from the host's.  FP32 engines
  *     key their counter-based streams by (seed, ligand index).
- *   - The reference's --fast search (not smina's) is built in part:
- *     chain_split and step_fraction (0: automatic) and dock_batch's first-pass
- *     budget, planned by sgh_fast_chains; skip_visited on FP64 engines.
- *     Refused at construction with a message: early_stop (it needs chains
- *     that stop and resume between phases), threads_per_chain above 32, and
- *     skip_visited with FP32 engines (QuickVina 2's history runs on the FP64
- *     path only).
+ *   - The reference's --fast search (not smina's): chain_split and
+ *     step_fraction (0: automatic) and dock_batch's first-pass budget,
+ *     planned by sgh_fast_chains; early_stop on FP32 engines (the batched
+ *     search in phases, sg_set_early_stop, with the reference's rule and
+ *     checkpoints); skip_visited on FP64 engines.  Refused at construction
+ *     with a message: threads_per_chain above 32, skip_visited with FP32
+ *     engines (QuickVina 2's history runs on the FP64 path only) and
+ *     early_stop with FP64 engines (the plain path does not run in phases).
  *
  * Precision follows the reference: the search runs in FP32 (mixed
  * precision, batched) unless settings.fp64; refinement and local
@@ -37,7 +38,9 @@
 #define SMINA_B200_HPP
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
+#include <limits>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -179,8 +182,10 @@ public:
         if (s.chain_split < 0) throw std::runtime_error("chain_split must be 0 (automatic) or positive");
         if (!(s.step_fraction >= 0 && s.step_fraction <= 1))
             throw std::runtime_error("step_fraction must lie in [0, 1] (0: automatic)");
-        if (s.early_stop != GpuSettings::EARLY_STOP_OFF)
-            throw std::runtime_error("early_stop is not built in this engine");
+        if (s.early_stop < GpuSettings::EARLY_STOP_OFF || s.early_stop > GpuSettings::EARLY_STOP_ALWAYS)
+            throw std::runtime_error("early_stop: unknown mode");
+        if (s.early_stop != GpuSettings::EARLY_STOP_OFF && s.fp64)
+            throw std::runtime_error("early_stop needs the FP32 search (the FP64 path does not run in phases)");
         if (s.threads_per_chain != 0 && s.threads_per_chain != 32)
             throw std::runtime_error("threads_per_chain: this engine runs 32 threads per chain");
         if (s.skip_visited && !s.fp64)
@@ -263,6 +268,72 @@ public:
         for (std::thread& t : th) t.join();
         for (const std::string& s : errors)
             if (!s.empty()) throw std::runtime_error(s);
+    }
+
+    /* top_score (main.cpp:355-373): the best final score finish_docking
+     * would report for a job's refined poses -- the conf-independent terms
+     * applied to each pose's energy on the direct receptor sum less the
+     * intramolecular energy of the best pose (FP64, sg_score on the first
+     * device); max double for a job without poses. */
+    double top_score(const DockJob& job, const sgh_tables* p, sgh_receptor* rec, const sg_grid_dims& gd,
+                     const double cap[3], double slope = 1e6) {
+        const int n = int(job.out.size());
+        if (n == 0) return std::numeric_limits<double>::max();
+        sg_engine* e = prepare(0, true, p, rec, gd);
+        const sg_model_desc d = detail::desc_of(job.m);
+        const int heavy = sgh_model_heavy(job.m);
+        std::vector<const Pose*> sorted;
+        for (const Pose& q : job.out) sorted.push_back(&q);
+        std::stable_sort(sorted.begin(), sorted.end(), [](const Pose* a, const Pose* b) { return a->e < b->e; });
+        std::vector<double> c(size_t(n) * d.conf_size), tot(n), intra(n);
+        std::vector<int> pm(n, 0);
+        for (int i = 0; i < n; i++) std::copy(sorted[i]->conf.begin(), sorted[i]->conf.end(), c.begin() + size_t(i) * d.conf_size);
+        check(e, sg_score(e, 0, &d, 1, pm.data(), n, c.data(), d.conf_size, cap, slope, tot.data(), intra.data(), nullptr,
+                          heavy),
+              "top score");
+        double inputs[7];
+        detail::check_host(sgh_model_conf_independent_inputs(job.m, inputs), "conf-independent inputs");
+        double best = std::numeric_limits<double>::max();
+        for (int i = 0; i < n; i++) {
+            if (!(sorted[i]->e < std::numeric_limits<double>::max())) continue;
+            double v = 0;
+            detail::check_host(sgh_tables_conf_independent(p, inputs, tot[i] - intra[0], &v), "conf-independent terms");
+            best = std::min(best, v);
+        }
+        return best;
+    }
+
+    /* Two-pass screening (--fast_top, main.cpp:1563-1597; not smina's search):
+     * once top_history and the batch hold at least 20 ligands and 0 <
+     * fast_top < 1, every job is docked briefly (fast_first of smina's
+     * steps), scored with top_score and its score added to top_history; the
+     * jobs scoring within fast_top_margin of the best fast_top fraction of
+     * top_history get the full search (their poses replaced).  Otherwise one
+     * full pass.  Returns how many jobs got the full search. */
+    size_t dock_batch_two_pass(std::vector<DockJob*>& jobs, const sgh_tables* p, sgh_receptor* rec,
+                               const sg_grid_dims& gd, int seed, const double cap[3], double fast_top,
+                               double fast_top_margin, double fast_first, std::vector<double>& top_history) {
+        if (!(fast_top > 0 && fast_top < 1) || top_history.size() + jobs.size() < 20) {
+            dock_batch(jobs, p, rec, gd, seed, cap);
+            return jobs.size();
+        }
+        if (!(fast_first > 0 && fast_first <= 1)) throw std::runtime_error("two-pass: fast_first must lie in (0, 1]");
+        dock_batch(jobs, p, rec, gd, seed, cap, fast_first);
+        std::vector<double> score(jobs.size());
+        for (size_t k = 0; k < jobs.size(); k++) score[k] = top_score(*jobs[k], p, rec, gd, cap);
+        top_history.insert(top_history.end(), score.begin(), score.end());
+        std::vector<double> sorted(top_history);
+        const size_t q = std::max<size_t>(1, size_t(std::ceil(fast_top * sorted.size()))) - 1;
+        std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
+        const double cutoff = sorted[q] + fast_top_margin;
+        std::vector<DockJob*> again;
+        for (size_t k = 0; k < jobs.size(); k++)
+            if (score[k] <= cutoff) {
+                jobs[k]->out.clear();
+                again.push_back(jobs[k]);
+            }
+        if (!again.empty()) dock_batch(again, p, rec, gd, seed, cap);
+        return again.size();
     }
 
     /* MinimizeJob (gpu_docking.h:96-103): a pose refined in its own box
@@ -406,6 +477,7 @@ private:
         for (int i = 0; i < 3; i++)  /* the batched search refines at authentic_v */
             if (mc.authentic_v[i] != cap[i])
                 throw std::runtime_error("dock_batch: with the FP32 search the refinement cap must be authentic_v");
+        apply_early_stop(e, plan(k, tasks, budget, mc.num_steps), budget);
         check(e, sg_dock_batch32(e, 0, models.data(), int(n), lj.data(), int(n), &mc, 1, res.data()), "dock_batch");
         for (size_t j = 0; j < n; j++)
             append(jobs[lo + j]->out, res[j].count, e_[j], c_[j], x_[j], models[j].conf_size, heavy[j]);
@@ -415,6 +487,7 @@ private:
     struct Plan {
         int split = 1;
         unsigned steps = 1;
+        double fraction = 1;
     };
     Plan plan(size_t k, long long tasks, double budget, unsigned steps) const {
         Plan f;
@@ -422,9 +495,29 @@ private:
         sg_device_info(dev_[k].search, nullptr, &sms, nullptr);
         const long long capacity = (long long)sms * (settings_.fp64 ? 32 : 16);
         detail::check_host(sgh_fast_chains(tasks, capacity, settings_.chain_split, settings_.step_fraction, budget,
-                                           steps, &f.split, &f.steps, nullptr),
+                                           steps, &f.split, &f.steps, &f.fraction),
                            "chain split");
         return f;
+    }
+
+    /* the early stop of device k's FP32 search for a plan (GpuDocking's
+     * stops / stop_for, gpu_docking.cpp:170-188): never on a first pass;
+     * EARLY_STOP_FULL only for splits below 32 (the GPU full); checks after
+     * every tenth of smina's steps the chains run, from the second on */
+    void apply_early_stop(sg_engine* e, const Plan& f, double budget) const {
+        const bool on = !(budget > 0) && (settings_.early_stop == GpuSettings::EARLY_STOP_ALWAYS ||
+                                          (settings_.early_stop == GpuSettings::EARLY_STOP_FULL && f.split < 32));
+        if (!on) {
+            check(e, sg_set_early_stop(e, nullptr), "early stop");
+            return;
+        }
+        sg_early_stop es;
+        es.first = 2;
+        es.checkpoints = std::max(es.first + 1, int(std::lround(10 * f.fraction)));
+        es.fraction = 0.5;
+        es.eps = 0.05;
+        es.chains_per_unit = f.split;
+        check(e, sg_set_early_stop(e, &es), "early stop");
     }
 
     void search_on(size_t k, const ParallelMC& par, const sgh_model* m, OutputContainer& out, const sgh_tables* p,
@@ -458,6 +551,7 @@ private:
         } else {
             const sg_ligand_job job{0, n, mc.num_steps, mc.maxiters, uint64_t(seed), 0};
             sg_ligand_result r{0, e_.data(), conf.data(), xyz.data(), 0};
+            apply_early_stop(e, f, budget);
             check(e, sg_dock_batch32(e, 0, &d, 1, &job, 1, &mc, 0, &r), "parallel_mc");
             count = r.count;
         }

@@ -10,6 +10,8 @@
 //
 //   gpu_docking_api_test host          (no device present)
 //   gpu_docking_api_test device        (device 0 present)
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -210,6 +212,85 @@ static void device_checks() {
                    "C ABI minimize");
         expect_poses(mposes, n, en.data(), cf.data(), xyz.data(), d1.conf_size, h1, "minimize_batch");
     }
+    // early stop (--fast, ALWAYS, chain split 2): the class applies the reference's rule and checkpoints
+    {
+        GpuSettings se;
+        se.early_stop = GpuSettings::EARLY_STOP_ALWAYS;
+        se.chain_split = 2;
+        GpuDocking ges(se);
+        smina_b200::ParallelMC p2 = par;
+        p2.mc.num_steps = 40;
+        smina_b200::OutputContainer out_es;
+        ges.parallel_mc(p2, m1, out_es, T, R, gd, seed);
+        int sms = 0, split = 0;
+        unsigned chain_steps = 0;
+        double fraction = 0;
+        sg_device_info(e32, nullptr, &sms, nullptr);
+        require_ok(sgh_fast_chains(tasks, (long long)sms * 16, 2, 1.0, 0, p2.mc.num_steps, &split, &chain_steps, &fraction),
+                   "fast chains");
+        sg_early_stop es;
+        es.first = 2;
+        es.checkpoints = std::max(3, int(std::lround(10 * fraction)));
+        es.fraction = 0.5;
+        es.eps = 0.05;
+        es.chains_per_unit = split;
+        require_ok(sg_set_early_stop(e32, &es), "early stop");
+        std::vector<double> e(S), conf(size_t(S) * d1.conf_size), xyz(size_t(S) * h1 * 3);
+        const sg_ligand_job job{0, tasks * split, chain_steps, p2.mc.maxiters, uint64_t(seed), 0};
+        sg_ligand_result r{0, e.data(), conf.data(), xyz.data(), 0};
+        require_ok(sg_dock_batch32(e32, 0, &d1, 1, &job, 1, &p2.mc, 0, &r), "C ABI dock_batch32 with early stop");
+        require_ok(sg_set_early_stop(e32, nullptr), "early stop off");
+        expect_poses(out_es, r.count, e.data(), conf.data(), xyz.data(), d1.conf_size, h1, "parallel_mc with early stop");
+    }
+    // two-pass screening: 24 ligands, the full search for those within the
+    // margin of the best quarter; the others keep their first pass
+    {
+        GpuDocking g2(GpuSettings{});
+        const int nl = 24;
+        std::vector<sgh_model*> lm;
+        std::vector<GpuDocking::DockJob> tj(nl), first(nl), full(nl);
+        for (int k = 0; k < nl; k++) {
+            lm.push_back(ligand(12 + (k % 5) * 4, k % 4, 300 + k, c));
+            for (auto* v : {&tj, &first, &full}) {
+                (*v)[k].m = lm.back();
+                (*v)[k].par = par;
+                (*v)[k].par.mc.num_steps = 60;
+                sg_mc_params mk;
+                require_ok(sgh_search_params(lm.back(), 9, &mk), "search params");
+                (*v)[k].par.mc.maxiters = mk.maxiters;
+            }
+        }
+        auto ptrs = [](std::vector<GpuDocking::DockJob>& v) {
+            std::vector<GpuDocking::DockJob*> r;
+            for (auto& j : v) r.push_back(&j);
+            return r;
+        };
+        std::vector<double> hist;
+        std::vector<GpuDocking::DockJob*> tp = ptrs(tj);
+        const size_t nfull = g2.dock_batch_two_pass(tp, T, R, gd, seed, mc.authentic_v, 0.25, 0.3, 0.1, hist);
+        expect(hist.size() == size_t(nl), "two-pass keeps every first-pass score");
+        expect(nfull >= 6 && nfull <= size_t(nl), "two-pass: at least the best quarter gets the full search");
+        std::vector<GpuDocking::DockJob*> fp = ptrs(first);
+        g2.dock_batch(fp, T, R, gd, seed, mc.authentic_v, 0.1);
+        std::vector<double> sorted(hist);
+        std::sort(sorted.begin(), sorted.end());
+        const double cutoff = sorted[5] + 0.3;
+        std::vector<GpuDocking::DockJob*> sel;
+        for (int k = 0; k < nl; k++) {
+            expect(hist[k] == g2.top_score(first[k], T, R, gd, mc.authentic_v), "first-pass score");
+            if (hist[k] <= cutoff) sel.push_back(&full[k]);
+        }
+        expect(sel.size() == nfull, "two-pass selects by the cutoff");
+        g2.dock_batch(sel, T, R, gd, seed, mc.authentic_v);
+        for (int k = 0; k < nl; k++) {
+            const GpuDocking::DockJob& want = hist[k] <= cutoff ? full[k] : first[k];
+            bool same = want.out.size() == tj[k].out.size();
+            for (size_t i = 0; same && i < want.out.size(); i++)
+                same = want.out[i].e == tj[k].out[i].e && want.out[i].conf == tj[k].out[i].conf;
+            expect(same, "two-pass poses: the full search for selected ligands, the first pass for the others");
+        }
+        for (sgh_model* x : lm) sgh_model_free(x);
+    }
     // FP64 engine: parallel_mc = host-seeded mt19937 chains, merged with min_rmsd 2
     {
         GpuSettings s64;
@@ -257,8 +338,9 @@ int main(int argc, char** argv) {
                  "negative chain_split");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.step_fraction = 1.5; })); }, "step_fraction",
                  "step_fraction above 1");
-    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_FULL; })); },
-                 "early_stop", "early_stop");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_FULL; s.fp64 = true; })); },
+                 "early_stop", "early_stop with fp64");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = 7; })); }, "early_stop", "unknown early_stop");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 128; })); }, "threads_per_chain",
                  "threads_per_chain");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.skip_visited = true; })); }, "fp64",
@@ -276,6 +358,8 @@ int main(int argc, char** argv) {
                      "not usable", "--fast settings pass validation");
         expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.fp64 = true; })); }, "not usable",
                      "no device present, fp64");
+        expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_ALWAYS; })); },
+                     "not usable", "early_stop passes validation on FP32");
     }
     if (mode == "device") device_checks();
     std::printf("%s: %d failure(s)\n", mode.c_str(), failures);
