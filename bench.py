@@ -358,6 +358,7 @@ def run_flex(args):
         wall = time.perf_counter() - t0
     clocks = clk.summary()
     lps = len(models) / wall
+    print(f"flex: {len(models)} ligands searched in {wall:.1f} s", file=sys.stderr, flush=True)
     # accuracy on a subsample: FP16 batched (two seeds) against plain FP64 (two seeds)
     na = min(args.flex_acc, len(models))
     sub = models[:na]
@@ -391,7 +392,9 @@ def run_flex(args):
         return np.array(out)
 
     t1 = time.perf_counter()
-    a64, b64 = best64(args.seed), best64(args.seed + 7919)
+    a64 = best64(args.seed)
+    print(f"flex: FP64 run 1 of {na} ligands in {time.perf_counter() - t1:.1f} s", file=sys.stderr, flush=True)
+    b64 = best64(args.seed + 7919)
     t64 = (time.perf_counter() - t1) / 2
     a16 = np.array([float(r["e"][0]) for r in r16[:na]])
     r16b = e16.dock_batch(0, sub, jobs_for(sub, list(range(na)), exh, args.seed + 7919, 0, args.step_scale), p,
@@ -681,8 +684,9 @@ def run_serve(args):
         arrivals = np.array(arrivals)
     else:
         arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    eng.set_threads_per_chain(args.threads_per_chain)
     eng.serve_start(block_smem_bytes=args.serve_block_smem)
-    lat, evals, dev, queue, searched, done_at = {}, 0, {}, {}, {}, {}
+    lat, evals, dev, queue, searched, done_at, tpcs = {}, 0, {}, {}, {}, {}, {}
     k = 0
     occupancy = []  # (queued, ligands in flight) sampled every 100 ms
     next_sample = 0.0
@@ -698,7 +702,8 @@ def run_serve(args):
                 occupancy.append((st["queued"], st["inflight"]))
                 next_sample = now + 0.1
             wait = 1 if k < n else 20
-            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1, qms, sms) in eng.serve_poll(256, wait_ms=wait, spans=True):
+            for (t, st, cnt, ms, ev, cs, nh, launch, d0, d1, qms, sms, tpc) in eng.serve_poll(256, wait_ms=wait,
+                                                                                                spans=True):
                 if st != 0:
                     raise RuntimeError(f"request {t} failed with status {st}")
                 eng.serve_fetch(t, cnt, cs, nh)
@@ -707,6 +712,7 @@ def run_serve(args):
                 dev[t] = (launch, d0, d1)
                 queue[t] = qms
                 searched[t] = sms
+                tpcs[t] = tpc
                 evals += ev
         wall = time.perf_counter() - t0
     eng.serve_stop()
@@ -741,6 +747,7 @@ def run_serve(args):
         "ligands_searching_at_once": concurrency,
         "completions_per_s_middle_80pct": mid_rate,
         "launches": launches,
+        "threads_per_chain": {str(c): int(sum(1 for x in tpcs.values() if x == c)) for c in sorted(set(tpcs.values()))},
         "requests": n, "offered_rate_per_s": args.rates or args.rate, "wall_s": wall, "evals_per_s": evals / wall,
         "inflight_ligands": {"mean": float(np.mean([o[1] for o in occupancy])),
                              "max": int(max(o[1] for o in occupancy)),
@@ -755,7 +762,8 @@ def run_serve(args):
                    "precision": args.precision,
                    "arrivals": (f"Poisson at rates {args.rates} per second, each for {args.rate_period} s in turn"
                                 if args.rates else f"Poisson at {args.rate} per second") + f", seed {args.seed}",
-                   "block_smem_bytes": args.serve_block_smem or "automatic"},
+                   "block_smem_bytes": args.serve_block_smem or "automatic",
+                   "threads_per_chain": args.threads_per_chain or "automatic (by the blocks in flight)"},
         "clocks": {k_: clocks[k_] for k_ in ("sm_mhz", "sm_max_mhz", "reasons")},
     }), flush=True)
 
@@ -840,6 +848,8 @@ def main():
     ap.add_argument("--cpu-ligands", type=int, default=4, help="ligands in the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--chains-per-block", type=int, default=0)
+    ap.add_argument("--threads-per-chain", type=int, default=32, choices=[0, 32, 64, 128],
+                    help="threads per chain of the batched search and the serving loop (0: automatic)")
     ap.add_argument("--autotune", type=float, default=0.0,
                     help="autotune the launch shape first on the step's ligands at this fraction of their steps "
                          "(0: the occupancy rule; short samples overweight the wait for each block's slowest chain)")
@@ -916,6 +926,7 @@ def main():
     p = make_params(models)
     B = args.batch or args.ligands
     tuned = None
+    eng.set_threads_per_chain(args.threads_per_chain)
     if args.chains_per_block:
         eng.set_chains_per_block(args.chains_per_block)
     elif args.autotune > 0:  # launch shape timed on a short sample of the screen, before any timed step

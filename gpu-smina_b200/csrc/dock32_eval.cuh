@@ -371,24 +371,73 @@ __device__ __noinline__ float2 table32_nc(int p, bool swap, float qa, float qb, 
     return make_float2(e1 + rem * (e2 - e1), d1 + rem * (d2 - d1));
 }
 
-// model::eval_deriv in FP32; returns the energy (same on every lane), writes g (FP64)
-__device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, int g_at) {
-    const W32 w = here();
+// ---- chain teams ------------------------------------------------------------------------------
+// A chain may run on a team of G warps (G = 1, 2, 4; the reference's
+// threads_per_chain 32, 64, 128), for latency when the device has warps to
+// spare.  The team's first warp, the leader, runs the chain: mutation,
+// BFGS, line searches, model::set and the derivative.  At every evaluation
+// it hands the grid and pair terms out: warp k of the team takes atoms
+// k, k + G, ... and a contiguous share of the pair chunks, adding forces
+// into its own workspace's force array.  The leader then sums the G
+// energies and force arrays in team order, so a team's results do not
+// depend on scheduling (they differ from one warp's only by the order of
+// FP32 additions).  The hand-out is two named-barrier phases per
+// evaluation (barrier id: team index + 1, 32 G threads); helpers take their
+// command (the caps, slope and an opcode) from their own workspace's
+// scratch words, which the leader writes before the first phase.
+constexpr unsigned kTeamEval = 1u, kTeamExit = 2u;
+// scratch words of a helper warp's workspace: [0, 4) caps v and slope,
+// [4] opcode; [8] energy share, [9] grid lookups, [10] pair lookups
+constexpr int kTeamOp = 4, kTeamE = 8, kTeamGrid = 9, kTeamPairs = 10;
+
+template <int G>
+__device__ __forceinline__ void team_bar() {
+    static_assert(G == 2 || G == 4, "teams of 2 or 4 warps");
+    // immediate barrier ids, so that a kernel reserves only the ones it uses
+    const int t = (int)(threadIdx.x >> 5) / G;  // the team's index in its block (at most 8 warps)
+    if (G == 4) {
+        if (t == 0) asm volatile("bar.sync 1, 128;" ::: "memory");
+        else asm volatile("bar.sync 2, 128;" ::: "memory");
+    } else {
+        if (t == 0) asm volatile("bar.sync 1, 64;" ::: "memory");
+        else if (t == 1) asm volatile("bar.sync 2, 64;" ::: "memory");
+        else if (t == 2) asm volatile("bar.sync 3, 64;" ::: "memory");
+        else asm volatile("bar.sync 4, 64;" ::: "memory");
+    }
+}
+// leader: the command for every helper of its team, then the first phase
+template <int G>
+__device__ __forceinline__ void team_publish(const W32& w, float3 v, float slope, unsigned op) {
+    if (w.lane > 0 && w.lane < G) {
+        unsigned* S = sp<unsigned>(w.ws + w.lane * sWsStride + smodel().L.scratch);
+        S[0] = __float_as_uint(v.x);
+        S[1] = __float_as_uint(v.y);
+        S[2] = __float_as_uint(v.z);
+        S[3] = __float_as_uint(slope);
+        S[kTeamOp] = op;
+    }
+    team_bar<G>();
+}
+
+// The grid and pair terms of model::eval_deriv for warp k of a team of G
+// (G = 1: the whole of them).  X: the chain's coordinates; F: this warp's
+// force array (every movable atom's entry is written).  Returns the warp's
+// energy share (same on every lane); adds its lookups to ghits and hits.
+template <int G>
+__device__ __forceinline__ float eval_terms32(const W32& w, int k, const float4* X, float4* F, float3 v, float slope,
+                                              unsigned& ghits, unsigned& hits) {
     const SModel& m = smodel();
-    double* g = sp<double>(g_at);
-    SG_T0(t_set);
-    set_conf32(conf_at);
-    SG_T1(t_set, 0);
     SG_T0(t_grid);
-    float4* X = w.coords();
-    float4* Fz = w.force();
     float e = 0;
-    unsigned ghits = 0;
     // grid part; every movable atom gets its force reset (hydrogens: zero)
     const int nmov = m.nmov;
     const int* TYPE = sp<const int>(m.type);
     const float4* LQ = sp<const float4>(m.local32);
-    for (int i = w.lane; i < nmov; i += 32) {
+    if (G > 1) {  // the atoms of other warps start at zero in this warp's array
+        for (int i = w.lane; i < nmov; i += 32) F[i] = make_float4(0, 0, 0, 0);
+        __syncwarp();
+    }
+    for (int i = w.lane * G + k; i < nmov; i += 32 * G) {
         const int t = TYPE[i];
         float3 d = make_float3(0, 0, 0);
         if (t < kNumTypes && !is_h(t)) {
@@ -403,7 +452,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
                 ghits++;
             }
         }
-        Fz[i] = make_float4(d.x, d.y, d.z, 0);
+        F[i] = make_float4(d.x, d.y, d.z, 0);
     }
     __syncwarp();
     SG_T1(t_grid, 1);
@@ -411,17 +460,17 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
     // Pairs: intramolecular (v[0]) and other (v[2]), SG_PAIR_CHUNKS chunks
     // of 32 in flight.  Within a chunk no atom is twice a first atom or twice a
     // second atom, so the force updates are plain read-add-writes: first
-    // atoms, sync, second atoms, sync.
+    // atoms, sync, second atoms, sync.  This warp's chunks: [c0, c1).
     const int nch = m.npchunks;
+    const int c0 = k * nch / G, c1 = (k + 1) * nch / G;
     const uint32_t* PS = sp<const uint32_t>(m.pslot);
     const DTables32 T = sT32;
     const int lane = w.lane;
-    unsigned hits = 0;
     uint32_t nsl[SG_PAIR_CHUNKS];  // next round's slots, loaded a round ahead
 #pragma unroll
-    for (int u = 0; u < SG_PAIR_CHUNKS; u++) nsl[u] = u < nch ? PS[u * 32 + lane] : kSlotEmpty;
-    for (int c = 0; c < nch; c += SG_PAIR_CHUNKS) {
-        const int live = min(SG_PAIR_CHUNKS, nch - c);  // chunks this round (warp-uniform)
+    for (int u = 0; u < SG_PAIR_CHUNKS; u++) nsl[u] = c0 + u < c1 ? PS[(c0 + u) * 32 + lane] : kSlotEmpty;
+    for (int c = c0; c < c1; c += SG_PAIR_CHUNKS) {
+        const int live = min(SG_PAIR_CHUNKS, c1 - c);  // chunks this round (warp-uniform)
         uint32_t sl[SG_PAIR_CHUNKS];
         int ia[SG_PAIR_CHUNKS], ib[SG_PAIR_CHUNKS];
         float3 r[SG_PAIR_CHUNKS];
@@ -430,7 +479,7 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
 #pragma unroll
         for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
             sl[u] = nsl[u];
-            nsl[u] = c + SG_PAIR_CHUNKS + u < nch ? PS[(c + SG_PAIR_CHUNKS + u) * 32 + lane] : kSlotEmpty;
+            nsl[u] = c + SG_PAIR_CHUNKS + u < c1 ? PS[(c + SG_PAIR_CHUNKS + u) * 32 + lane] : kSlotEmpty;
             ia[u] = sl[u] & 0xff;
             ib[u] = (sl[u] >> 8) & 0xff;
             r[u] = f3(X[ib[u]]) - f3(X[ia[u]]);
@@ -476,15 +525,15 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
         for (int u = 0; u < SG_PAIR_CHUNKS; u++) {
             if (u >= live) break;
             if (ok[u]) {
-                float4 t = Fz[ia[u]];
+                float4 t = F[ia[u]];
                 t.x -= f[u].x; t.y -= f[u].y; t.z -= f[u].z;
-                Fz[ia[u]] = t;
+                F[ia[u]] = t;
             }
             __syncwarp();
             if (ok[u]) {
-                float4 t = Fz[ib[u]];
+                float4 t = F[ib[u]];
                 t.x += f[u].x; t.y += f[u].y; t.z += f[u].z;
-                Fz[ib[u]] = t;
+                F[ib[u]] = t;
             }
             __syncwarp();
         }
@@ -492,6 +541,67 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
     e = warp_sum(e);
     __syncwarp();
     SG_T1(t_pairs, 2);
+    return e;
+}
+
+// a helper warp of a chain team: serves the leader's evaluations until it
+// sends kTeamExit
+template <int G>
+__device__ __noinline__ void team_help32() {
+    const W32 w = here();
+    const SModel& m = smodel();
+    const int k = (int)(threadIdx.x >> 5) % G;
+    const float4* X = sp<const float4>(w.ws - k * sWsStride + m.L.coords);  // the leader's coordinates
+    unsigned* S = w.counters();
+    for (;;) {
+        team_bar<G>();  // the leader's command and coordinates are in
+        if (S[kTeamOp] != kTeamEval) break;
+        const float3 v = make_float3(__uint_as_float(S[0]), __uint_as_float(S[1]), __uint_as_float(S[2]));
+        const float slope = __uint_as_float(S[3]);
+        unsigned gh = 0, ph = 0;
+        const float e = eval_terms32<G>(w, k, X, w.force(), v, slope, gh, ph);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            gh += __shfl_xor_sync(kFull32, gh, o);
+            ph += __shfl_xor_sync(kFull32, ph, o);
+        }
+        if (w.lane == 0) {
+            S[kTeamE] = __float_as_uint(e);
+            S[kTeamGrid] = gh;
+            S[kTeamPairs] = ph;
+        }
+        team_bar<G>();  // this warp's forces and energy share are in
+    }
+}
+
+// model::eval_deriv in FP32 on a team of G warps (called by the leader);
+// returns the energy (same on every lane), writes g (FP64)
+template <int G>
+__device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, int g_at) {
+    const W32 w = here();
+    const SModel& m = smodel();
+    double* g = sp<double>(g_at);
+    SG_T0(t_set);
+    set_conf32(conf_at);
+    SG_T1(t_set, 0);
+    if constexpr (G > 1) team_publish<G>(w, v, slope, kTeamEval);
+    float4* X = w.coords();
+    float4* Fz = w.force();
+    const int nmov = m.nmov;
+    unsigned ghits = 0, hits = 0;
+    float e = eval_terms32<G>(w, 0, X, Fz, v, slope, ghits, hits);
+    if constexpr (G > 1) {
+        team_bar<G>();  // the helpers' shares are in
+#pragma unroll
+        for (int k = 1; k < G; k++) {
+            const unsigned* S = sp<const unsigned>(w.ws + k * sWsStride + m.L.scratch);
+            e += __uint_as_float(S[kTeamE]);
+            if (w.lane == 0) {
+                ghits += S[kTeamGrid];
+                hits += S[kTeamPairs];
+            }
+        }
+    }
     SG_T0(t_der);
     // Derivative.  A frame's subtree owns the contiguous atom range
     // [fbegin, fsub_end), so its force and torque are differences of two
@@ -508,6 +618,8 @@ __device__ __noinline__ float eval_deriv32(int conf_at, float3 v, float slope, i
         float3 F = make_float3(0, 0, 0), Cq = make_float3(0, 0, 0);
         if (i < nmov) {
             F = f3(Fz[i]);
+#pragma unroll
+            for (int k = 1; k < G; k++) F = F + f3(sp<const float4>(w.ws + k * sWsStride + m.L.force)[i]);
             Cq = cross3(f3(X[i]) - oref, F);
         }
         float3 iF = F, iC = Cq;

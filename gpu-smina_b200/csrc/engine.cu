@@ -812,9 +812,10 @@ static int eval_common(sg_engine* e, int rid, const sg_model_desc* m, int nconfs
             const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
             const size_t stage =
                 (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
-            require(stage + ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
+            require(stage + (size_t)std::max(1, e->tpc / 32) * ws <= (size_t)e->max_smem,
+                    "model too large for the mixed-precision path's shared memory");
             cuda_check(launch_eval32(pm.dmodels.as<DModel>(), stage, ws, tables32(e), maps32(e, r), nconfs, dc.p(), v, slope,
-                                     de.p(), dg.p(), out_coords ? dx.p() : nullptr, e->stream),
+                                     de.p(), dg.p(), out_coords ? dx.p() : nullptr, std::max(1, e->tpc / 32), e->stream),
                        "eval launch");
             de.fetch(out_e, e->stream);
             dg.fetch(out_g, e->stream);
@@ -868,9 +869,11 @@ int sg_bfgs(sg_engine* e, int rid, const sg_model_desc* m, int nconfs, double* c
             const size_t ws = (ws32_bytes(h) + 15) & ~(size_t)15;
             const size_t stage =
                 (size_t)stage32_bytes(h.natoms, h.nframes, h.nheavy, h.npchunks, h.nlig, h.nblocks, h.ntors);
-            require(stage + ws <= (size_t)e->max_smem, "model too large for the mixed-precision path's shared memory");
+            require(stage + (size_t)std::max(1, e->tpc / 32) * ws <= (size_t)e->max_smem,
+                    "model too large for the mixed-precision path's shared memory");
             cuda_check(launch_bfgs32(pm.dmodels.as<DModel>(), stage, ws, tables32(e), maps32(e, r), nconfs, dc.p(), v,
-                                     slope, maxiters, accurate_line, early_term, de.p(), e->stream),
+                                     slope, maxiters, accurate_line, early_term, de.p(), std::max(1, e->tpc / 32),
+                                     e->stream),
                        "bfgs launch");
             dc.fetch(confs, e->stream);
             de.fetch(out_e, e->stream);

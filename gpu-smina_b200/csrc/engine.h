@@ -84,6 +84,8 @@ struct sg_engine {
     bool has_tables = false;
     sg::DevBuf tab_smooth, tab_fast, tab32;
     int force_wpb = 0, last_wpb = 0, last_blocks = 0;
+    int tpc = 32;        // threads per chain of the batched search: 32, 64, 128, or 0 (by the batch's size)
+    int last_team = 1;   // warps per chain of the last batched search
     bool es_on = false;   // early stop of the batched search (--fast; sg_set_early_stop)
     sg_early_stop es{};
     double last_mc_ms = 0, last_refine_ms = 0;
@@ -139,7 +141,7 @@ cudaError_t launch_refine64(const DModel*, size_t, const DTables&, const DRecept
                             const double[3], int, const int* pose_maxiters, const double* pose_box, int, int, double*,
                             double*, int, int*, cudaStream_t);
 size_t ws32_bytes(const DModel& hm);
-int mc32_occupancy(int wpb, size_t smem);
+int mc32_occupancy(int team, int wpb, size_t smem);
 cudaError_t launch_mc32_feed(const DTables32& T, const FeedItem32* ring, unsigned cap, FeedCtrl32* ctrl,
                              long long idle_ns, int blocks, int wpb, size_t smem, cudaStream_t s);
 cudaError_t mc32_feed_reserve_smem(size_t smem);
@@ -152,13 +154,13 @@ cudaError_t launch_mc32_fixed(const DModel*, const DTables32&, const DMaps32&, c
                               size_t stage_stride, size_t ws_stride, size_t smem_fixed, cudaStream_t s);
 cudaError_t launch_mc32(const DModel*, const DTables32&, const DMaps32&, const DMaps32* maps_tab, const Chain32*,
                         const Item32*, int nitems, const MCParams32&, unsigned*, int blocks, int wpb,
-                        size_t stage_stride, size_t ws_stride, cudaStream_t);
+                        size_t stage_stride, size_t ws_stride, int team, cudaStream_t);
 cudaError_t launch_eval32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, const double*,
-                          const double[3], double, double*, double*, double*, cudaStream_t);
+                          const double[3], double, double*, double*, double*, int team, cudaStream_t);
 cudaError_t gather_probe(size_t working_set, int bytes_per_lookup, int num_sms, double* gbs, cudaStream_t s);
 cudaError_t launch_bfgs32(const DModel*, size_t stage, size_t ws, const DTables32&, const DMaps32&, int, double*,
                           const double v[3], double slope, int maxiters, int accurate, int early, double* e,
-                          cudaStream_t);
+                          int team, cudaStream_t);
 
 // FP32 views of the engine's tables and of a receptor's packed maps
 DTables32 tables32(const sg_engine* e);

@@ -82,22 +82,34 @@ static void add_pose(std::vector<HostPose>& out, HostPose&& t, double min_rmsd, 
     std::stable_sort(out.begin(), out.end(), [](const HostPose& a, const HostPose& b) { return a.e < b.e; });
 }
 
-// launch shape: chains (warps) per block with the most resident chains per
-// SM (ties: more chains per block, so fewer model copies)
-void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ) {
+// Launch shape for chains on teams of `team` warps: chains per block (wpb)
+// with the most resident chains per SM (ties: more chains per block, so
+// fewer model copies).  A batch of at most one chain per SM (nchains) runs
+// one chain per block, so that every chain has an SM to itself.  False
+// when no shape fits the shared memory.
+bool try_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int team, long long nchains,
+                int& wpb, int& occ) {
     const int cands[4] = {8, 4, 2, 1};
     int best_w = 0, best_occ = 0, best_res = 0;
+    const bool spread = !e->force_wpb && nchains <= e->num_sms;
     for (int c : cands) {
+        if (c * team > 8) continue;
         if (e->force_wpb && c != e->force_wpb) continue;
-        if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;  // half the warps would idle
-        const size_t smem = stage_stride + (size_t)c * ws_stride;
+        if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;  // half the chains' warps would idle
+        if (spread && c > 1) continue;
+        const size_t smem = stage_stride + (size_t)c * team * ws_stride;
         if (smem > (size_t)e->max_smem) continue;
-        const int o = mc32_occupancy(c, smem);
+        const int o = mc32_occupancy(team, c * team, smem);
         if (o * c > best_res) { best_res = o * c; best_w = c; best_occ = o; }
     }
-    require(best_res > 0, "model too large for the mixed-precision path's shared memory");
     wpb = best_w;
     occ = best_occ;
+    return best_res > 0;
+}
+
+void choose_launch(sg_engine* e, size_t stage_stride, size_t ws_stride, int max_chains, int& wpb, int& occ) {
+    require(try_launch(e, stage_stride, ws_stride, max_chains, 1, 1ll << 40, wpb, occ),
+            "model too large for the mixed-precision path's shared memory");
 }
 
 #ifdef SG_PROFILE
@@ -187,8 +199,23 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
         // persistent kernel's queue ends evenly
         int max_chains = 1;
         for (int j = 0; j < njobs; j++) max_chains = std::max(max_chains, jobs[j].num_chains);
-        int wpb = 1, occ = 1;
-        choose_launch(e, stage_stride, ws_stride, max_chains, wpb, occ);
+        // Threads per chain: as set, or (0) the most warps per chain whose
+        // resident chains still hold the whole batch (the reference's
+        // threads_per_chain, gpu_kernels_impl.cuh:572-605).
+        int wpb = 1, occ = 1, team = std::max(1, e->tpc / 32);
+        if (e->tpc == 0) {
+            team = 1;
+            for (int g : {4, 2}) {
+                int w = 0, o = 0;
+                if (try_launch(e, stage_stride, ws_stride, max_chains, g, nchains, w, o) &&
+                    (long long)nchains <= (long long)o * w * e->num_sms) {
+                    team = g;
+                    break;
+                }
+            }
+        }
+        require(try_launch(e, stage_stride, ws_stride, max_chains, team, nchains, wpb, occ),
+                "model too large for the mixed-precision path's shared memory at this many threads per chain");
         MCParams32 P{};
         for (int i = 0; i < 3; i++) {
             P.hunt[i] = (float)p->hunt_cap[i];
@@ -280,8 +307,8 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             cuda_check(cudaMemsetAsync(d_queue.p, 0, sizeof(unsigned), e->stream), "queue reset");
             cuda_check(cudaEventRecord(ev[0], e->stream), "event");
             cuda_check(launch_mc32(pm.dmodels.as<DModel>(), tables32(e), maps32(e, r), nullptr, d_chains.as<Chain32>(),
-                                   d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb, stage_stride,
-                                   ws_stride, e->stream),
+                                   d_items.as<Item32>(), nitems, P, d_queue.as<unsigned>(), blocks, wpb * team,
+                                   stage_stride, ws_stride, team, e->stream),
                        "search launch");
             cuda_check(cudaEventRecord(ev[1], e->stream), "event");
             if (phased && ph + 1 < nphases) {  // the stopping rule on the best energies the chains saved
@@ -425,6 +452,7 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
             }
         }
         e->last_wpb = wpb;
+        e->last_team = team;
         e->last_blocks = blocks;
         e->last_mc_ms = mc_ms;
         e->last_refine_ms = ref_ms;
@@ -474,6 +502,19 @@ int sg_set_early_stop(sg_engine* e, const sg_early_stop* es) {
         return SG_ERR_ARG;
     e->es = *es;
     e->es_on = true;
+    return SG_OK;
+}
+
+int sg_set_threads_per_chain(sg_engine* e, int threads) {
+    if (!e || !(threads == 0 || threads == 32 || threads == 64 || threads == 128)) return SG_ERR_ARG;
+    e->tpc = threads;
+    return SG_OK;
+}
+
+int sg_threads_per_chain(const sg_engine* e, int* configured, int* last_batch) {
+    if (!e) return SG_ERR_ARG;
+    if (configured) *configured = e->tpc;
+    if (last_batch) *last_batch = 32 * e->last_team;
     return SG_OK;
 }
 

@@ -122,14 +122,17 @@ struct Mode32 {
     float slope;
 };
 
-// energy and gradient of the conf at smem32 offset x_at (gradient to g_at)
+// energy and gradient of the conf at smem32 offset x_at (gradient to g_at),
+// on the chain's team of G warps
+template <int G>
 __device__ __forceinline__ double feval32(int x_at, int g_at, const Mode32& em) {
-    return (double)eval_deriv32(x_at, em.v, em.slope, g_at);
+    return (double)eval_deriv32<G>(x_at, em.v, em.slope, g_at);
 }
 
 // ---- line searches (bfgs.h:30-200) ------------------------------------------------------
 // x, g, p, x_new, g_new: offsets of this warp's workspace arrays in smem32
 // pg: p . g, computed by the caller with p
+template <int G>
 __device__ __forceinline__ double line_fast32(const W32& w, int x_at, double pg, double f0, int p_at, int xn_at,
                                               int gn_at, double& f1, const Mode32& em) {
     const SModel& m = smodel();
@@ -142,7 +145,7 @@ __device__ __forceinline__ double line_fast32(const W32& w, int x_at, double pg,
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
         SG_T1(t_ls, 4);
-        f1 = feval32(xn_at, gn_at, em);
+        f1 = feval32<G>(xn_at, gn_at, em);
         if (f1 - f0 < 0.0001 * alpha * pg) break;
         alpha *= 0.5;
     }
@@ -151,6 +154,7 @@ __device__ __forceinline__ double line_fast32(const W32& w, int x_at, double pg,
 
 // Out of line; arguments by value and (alpha, f1) returned by value, so that
 // no variable of the caller has its address taken.
+template <int G>
 __device__ __noinline__ double2 line_accurate32(W32 w, int x_at, double pg, double f0, int p_at, int xn_at, int gn_at,
                                                  Mode32 em) {
     const SModel& m = smodel();
@@ -178,7 +182,7 @@ __device__ __noinline__ double2 line_accurate32(W32 w, int x_at, double pg, doub
     for (int it = 0; it < 128; it++) {
         copyd(w, x_new, x, m.conf_size);
         increment32(w, x_new, p, alpha);
-        f1 = feval32(xn_at, gn_at, em);
+        f1 = feval32<G>(xn_at, gn_at, em);
         if (alpha < alamin) return give_up();
         if (f1 <= f0 + ALF * alpha * slope) return make_double2(alpha, f1);
         if (alpha == FIRST) {
@@ -210,6 +214,7 @@ __device__ __noinline__ double2 line_accurate32(W32 w, int x_at, double pg, doub
 // a row sweep read consecutive words.  Every entry (i, j) is computed from
 // (min(i, j), max(i, j)) operands in one fixed order, so h stays exactly
 // symmetric.  x_at: smem32 offset of the conf, optimised in place.
+template <int G>
 __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int early, Mode32 em) {
     const W32 w = here();
     const SModel& m = smodel();
@@ -223,7 +228,7 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
     for (int i = w.lane; i < n; i += 32)
         for (int j = 0; j < n; j++) h[j * n + i] = (i == j) ? 1.0 : 0.0;
     __syncwarp();
-    double f0 = feval32(x_at, g_at, em);
+    double f0 = feval32<G>(x_at, g_at, em);
     const double f_orig = f0;
     copyd(w, g_orig, g, n);
     copyd(w, x_orig, x, cs);
@@ -242,11 +247,11 @@ __device__ __noinline__ double bfgs32(int x_at, int maxiters, int accurate, int 
         SG_T1(t_alg, 5);
         double f1 = 0, alpha;
         if (accurate) {
-            const double2 r = line_accurate32(w, x_at, pg, f0, p_at, xn_at, gn_at, em);
+            const double2 r = line_accurate32<G>(w, x_at, pg, f0, p_at, xn_at, gn_at, em);
             alpha = r.x;
             f1 = r.y;
         } else {
-            alpha = line_fast32(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em);
+            alpha = line_fast32<G>(w, x_at, pg, f0, p_at, xn_at, gn_at, f1, em);
         }
         if (alpha == 0) break;
         SG_T0(t_alg2);
@@ -470,7 +475,9 @@ __device__ __forceinline__ int add_output32(const W32& w, const Chain32& ch, con
     return count;
 }
 
-// monte_carlo::operator() for one chain
+// monte_carlo::operator() for one chain, run by the leader of its team of G
+// warps
+template <int G>
 __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P) {
     SG_T0(t_chain);
     const W32 w = here();
@@ -515,7 +522,7 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
         copyd(w, cand, tmp, cs);
         mutate32(w, rng, cand, P.amplitude);
         SG_T1(t_mut, 6);
-        const double cand_e = bfgs32(cand_at, ch.maxiters, P.accurate_line, P.early_term, hunt);
+        const double cand_e = bfgs32<G>(cand_at, ch.maxiters, P.accurate_line, P.early_term, hunt);
         bool accept = step == 0 || cand_e < tmp_e;
         if (!accept) accept = ph_u01(rng) < exp((tmp_e - cand_e) / P.temperature);
         if (accept) {
@@ -523,7 +530,7 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
             tmp_e = cand_e;
             set_conf32(tmp_at);
             if (tmp_e < best_e || count < P.num_saved) {
-                tmp_e = bfgs32(tmp_at, ch.maxiters, P.accurate_line, P.early_term, auth);
+                tmp_e = bfgs32<G>(tmp_at, ch.maxiters, P.accurate_line, P.early_term, auth);
                 set_conf32(tmp_at);
                 count = add_output32(w, ch, tmp, tmp_e, P.min_rmsd, P.num_saved, count);
                 if (tmp_e < best_e) best_e = tmp_e;
@@ -622,9 +629,26 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
     __syncthreads();
 }
 
+// A chain on its team of G warps: the leader runs it and then releases the
+// helpers, which serve its evaluations until then.
+template <int G>
+__device__ __forceinline__ void run_team32(const Chain32& ch, const MCParams32& P) {
+    if constexpr (G == 1) {
+        run_chain32<1>(ch, P);
+    } else {
+        if ((threadIdx.x >> 5) % G == 0) {
+            run_chain32<G>(ch, P);
+            team_publish<G>(here(), make_float3(0, 0, 0), 0.f, kTeamExit);
+        } else {
+            team_help32<G>();
+        }
+    }
+}
+
 // Persistent search kernel.  A block takes work items (a group of chains
 // of one ligand, longest first) from *queue, stages the ligand's model in
-// shared memory once for all its warps, and runs one chain per warp.
+// shared memory once for all its warps, and runs one chain per team of G
+// warps (every warp has a workspace; a helper's holds its force share).
 // SG_MC32_MINB resident 256-thread blocks per SM bound the registers
 // (2: 128 per thread).
 #ifndef SG_MC32_MINB
@@ -635,6 +659,7 @@ __device__ void stage_model(const DModel* gm, int tid, int nthr) {
 #endif
 // maps_tab: one DMaps32 per receptor (items name theirs), or null when the
 // whole launch uses G.
+template <int TEAM>
 __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DModel* models, DTables32 T, DMaps32 G,
                                                             const DMaps32* maps_tab, const Chain32* chains,
                                                             const Item32* items, int nitems,
@@ -651,9 +676,7 @@ __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32(const DM
         const Item32 item = items[it];
         if (maps_tab && tid == 0) sG32 = maps_tab[item.rec];  // read after stage_model's barrier
         stage_model(models + item.model, tid, nthr);
-        if (warp < item.count) {
-            run_chain32(chains[item.first + warp], P);
-        }
+        if (warp / TEAM < item.count) run_team32<TEAM>(chains[item.first + warp / TEAM], P);
         SG_T0(t_bar);
         __syncthreads();  // the staged model is in use until every warp is done
         SG_T1(t_bar, 8);
@@ -699,8 +722,8 @@ static_assert(sizeof(FeedItem32) % 16 == 0 && sizeof(DMaps32) % 16 == 0 && sizeo
 // The serving grid: persistent blocks that take items from a ring the host
 // keeps filling while the grid runs, so that a ligand's chains start as
 // soon as a block is free, whatever launch it came with.  An item's block
-// stages its ligand's model and runs one chain per warp; its chains signal
-// completion as in k_mc32.  Everything an item points to is read through
+// stages its ligand's model and runs one chain per team of warps (the
+// item's team size); its chains signal completion as in k_mc32.  Everything an item points to is read through
 // L2 only (the host reuses device memory while the grid runs).  A block
 // leaves after idle_ns without work; the host starts more blocks when
 // items wait and none is free.
@@ -733,28 +756,39 @@ __global__ void __launch_bounds__(SG_MC32_THREADS, SG_MC32_MINB) k_mc32_feed(DTa
         __syncthreads();
         if (s_seq < 0) break;
         stage_model(s_fi.model, tid, nthr);
-        if (warp < s_fi.count) {
+        const int team = s_fi.team == 4 ? 4 : s_fi.team == 2 ? 2 : 1;
+        if (warp / team < s_fi.count) {
             Chain32 ch;
-            const int4* cs = reinterpret_cast<const int4*>(s_fi.chains + warp);
+            const int4* cs = reinterpret_cast<const int4*>(s_fi.chains + warp / team);
             int4* cd = reinterpret_cast<int4*>(&ch);
             for (int k = 0; k < (int)(sizeof(Chain32) / 16); k++) cd[k] = __ldcg(cs + k);
-            run_chain32(ch, s_params);
+            if (team == 4) run_team32<4>(ch, s_params);
+            else if (team == 2) run_team32<2>(ch, s_params);
+            else run_team32<1>(ch, s_params);
         }
         __syncthreads();  // the staged model is in use until every warp is done
     }
     if (tid == 0) atomicAdd(&ctrl->exited, 1u);
 }
 
-// model::eval_deriv in FP32 for a batch of confs of one model (one warp per
-// conf); the model is staged like the search kernel's, the workspace
-// follows it at ws_at
-__global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T, DMaps32 G, int n, const double* confs,
-                                               float v0, float v1, float v2, float slope, double* out_e, double* out_g,
-                                               double* out_coords, int ws_at) {
+// model::eval_deriv in FP32 for a batch of confs of one model (one team of
+// TEAM warps per conf); the model is staged like the search kernel's, the
+// warps' workspaces follow it at ws_at, ws_stride apart
+template <int TEAM>
+__global__ void __launch_bounds__(32 * TEAM) k_eval32(const DModel* model, DTables32 T, DMaps32 G, int n,
+                                                      const double* confs, float v0, float v1, float v2, float slope,
+                                                      double* out_e, double* out_g, double* out_coords, int ws_at,
+                                                      int ws_stride) {
     const int k = blockIdx.x;
     if (k >= n) return;
-    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = 0; }
-    stage_model(model, threadIdx.x, 32);
+    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = ws_stride; }
+    stage_model(model, threadIdx.x, 32 * TEAM);
+    if constexpr (TEAM > 1) {
+        if (threadIdx.x >= 32) {
+            team_help32<TEAM>();
+            return;
+        }
+    }
     const W32 w = here();
     const SModel& m = smodel();
     const Ws32& L = m.L;
@@ -762,7 +796,8 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
     for (int i = w.lane; i < 65; i += 32) C[i] = 0;
     for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = __ldg(m.lab32 + i);  // inflex atoms stay here
     copyd(w, w.d(L.x_tmp), confs + (size_t)k * m.conf_size, m.conf_size);
-    const float e = eval_deriv32(w.at(L.x_tmp), make_float3(v0, v1, v2), slope, w.at(L.g));
+    const float e = eval_deriv32<TEAM>(w.at(L.x_tmp), make_float3(v0, v1, v2), slope, w.at(L.g));
+    if constexpr (TEAM > 1) team_publish<TEAM>(w, make_float3(0, 0, 0), 0.f, kTeamExit);
     const double* g = w.d(L.g);
     if (w.lane == 0) out_e[k] = e;
     for (int i = w.lane; i < m.dof; i += 32) out_g[(size_t)k * m.dof + i] = g[i];
@@ -775,14 +810,23 @@ __global__ void __launch_bounds__(32) k_eval32(const DModel* model, DTables32 T,
 }
 
 // quasi_newton for a batch of confs of one model with the search's own
-// mixed-precision BFGS (one warp per conf); confs are optimised in place
-__global__ void __launch_bounds__(32) k_bfgs32(const DModel* model, DTables32 T, DMaps32 G, int n, double* confs,
-                                               float v0, float v1, float v2, float slope, int maxiters, int accurate,
-                                               int early, double* out_e, int ws_at) {
+// mixed-precision BFGS (one team of TEAM warps per conf); confs are
+// optimised in place
+template <int TEAM>
+__global__ void __launch_bounds__(32 * TEAM) k_bfgs32(const DModel* model, DTables32 T, DMaps32 G, int n,
+                                                      double* confs, float v0, float v1, float v2, float slope,
+                                                      int maxiters, int accurate, int early, double* out_e, int ws_at,
+                                                      int ws_stride) {
     const int k = blockIdx.x;
     if (k >= n) return;
-    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = 0; }
-    stage_model(model, threadIdx.x, 32);
+    if (threadIdx.x == 0) { sT32 = T; sG32 = G; sWs0 = ws_at; sWsStride = ws_stride; }
+    stage_model(model, threadIdx.x, 32 * TEAM);
+    if constexpr (TEAM > 1) {
+        if (threadIdx.x >= 32) {
+            team_help32<TEAM>();
+            return;
+        }
+    }
     const W32 w = here();
     const SModel& m = smodel();
     const Ws32& L = m.L;
@@ -792,7 +836,8 @@ __global__ void __launch_bounds__(32) k_bfgs32(const DModel* model, DTables32 T,
     for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = __ldg(m.finit32 + f);
     double* c = confs + (size_t)k * m.conf_size;
     copyd(w, w.d(L.x_tmp), c, m.conf_size);
-    const double e = bfgs32(w.at(L.x_tmp), maxiters, accurate, early, Mode32{make_float3(v0, v1, v2), slope});
+    const double e = bfgs32<TEAM>(w.at(L.x_tmp), maxiters, accurate, early, Mode32{make_float3(v0, v1, v2), slope});
+    if constexpr (TEAM > 1) team_publish<TEAM>(w, make_float3(0, 0, 0), 0.f, kTeamExit);
     const double* x = w.d(L.x_tmp);
     for (int i = w.lane; i < m.conf_size; i += 32) c[i] = x[i];
     if (w.lane == 0) out_e[k] = e;
@@ -813,13 +858,18 @@ static cudaError_t prep32(const void* fn, size_t smem) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-// resident blocks per SM of k_mc32 with `wpb` chains (warps) per block; 0
-// when the shape does not fit (the failed call's error is cleared, so the
-// next launch's check does not see it)
-int mc32_occupancy(int wpb, size_t smem) {
+static const void* k_mc32_for(int team) {
+    return team == 4 ? (const void*)k_mc32<4> : team == 2 ? (const void*)k_mc32<2> : (const void*)k_mc32<1>;
+}
+
+// resident blocks per SM of k_mc32 with `wpb` warps per block in teams of
+// `team`; 0 when the shape does not fit (the failed call's error is
+// cleared, so the next launch's check does not see it)
+int mc32_occupancy(int team, int wpb, size_t smem) {
     int blocks = 0;
-    if (prep32((const void*)k_mc32, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_mc32, 32 * wpb, smem) != cudaSuccess) {
+    const void* fn = k_mc32_for(team);
+    if (prep32(fn, smem) != cudaSuccess || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, 32 * wpb, smem) !=
+                                               cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -828,12 +878,20 @@ int mc32_occupancy(int wpb, size_t smem) {
 
 cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G, const DMaps32* maps_tab,
                         const Chain32* chains, const Item32* items, int nitems, const MCParams32& P, unsigned* queue,
-                        int blocks, int wpb, size_t stage_stride, size_t ws_stride, cudaStream_t s) {
+                        int blocks, int wpb, size_t stage_stride, size_t ws_stride, int team, cudaStream_t s) {
+    if (!(team == 1 || team == 2 || team == 4) || wpb % team) return cudaErrorInvalidValue;
     const size_t smem = stage_stride + (size_t)wpb * ws_stride;
-    cudaError_t rc = prep32((const void*)k_mc32, smem);
+    cudaError_t rc = prep32(k_mc32_for(team), smem);
     if (rc != cudaSuccess) return rc;
-    k_mc32<<<blocks, 32 * wpb, smem, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue, (int)stage_stride,
-                                          (int)ws_stride);
+    if (team == 4)
+        k_mc32<4><<<blocks, 32 * wpb, smem, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
+                                                 (int)stage_stride, (int)ws_stride);
+    else if (team == 2)
+        k_mc32<2><<<blocks, 32 * wpb, smem, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
+                                                 (int)stage_stride, (int)ws_stride);
+    else
+        k_mc32<1><<<blocks, 32 * wpb, smem, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
+                                                 (int)stage_stride, (int)ws_stride);
     return cudaGetLastError();
 }
 
@@ -841,13 +899,13 @@ cudaError_t launch_mc32(const DModel* dms, const DTables32& T, const DMaps32& G,
 // launches (serving's many concurrent ones, the no-allocation entry point's)
 // set no function attribute while other launches of the kernel run.  The
 // first use also loads the kernel's module.
-cudaError_t mc32_reserve_smem(size_t smem) { return prep32((const void*)k_mc32, smem); }
+cudaError_t mc32_reserve_smem(size_t smem) { return prep32((const void*)k_mc32<1>, smem); }
 
 // the largest dynamic shared memory a k_mc32 block can take: the device's
 // opt-in limit less the kernel's static shared memory
 cudaError_t mc32_max_dynamic_smem(size_t optin, size_t* out) {
     cudaFuncAttributes fa{};
-    cudaError_t rc = cudaFuncGetAttributes(&fa, (const void*)k_mc32);
+    cudaError_t rc = cudaFuncGetAttributes(&fa, (const void*)k_mc32<1>);
     if (rc != cudaSuccess) return rc;
     *out = optin > fa.sharedSizeBytes ? optin - fa.sharedSizeBytes : 0;
     return cudaSuccess;
@@ -858,30 +916,43 @@ cudaError_t launch_mc32_fixed(const DModel* dms, const DTables32& T, const DMaps
                               unsigned* queue, int blocks, int wpb, size_t stage_stride, size_t ws_stride,
                               size_t smem_fixed, cudaStream_t s) {
     if (stage_stride + (size_t)wpb * ws_stride > smem_fixed) return cudaErrorInvalidValue;
-    k_mc32<<<blocks, 32 * wpb, smem_fixed, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
-                                                (int)stage_stride, (int)ws_stride);
+    k_mc32<1><<<blocks, 32 * wpb, smem_fixed, s>>>(dms, T, G, maps_tab, chains, items, nitems, P, queue,
+                                                   (int)stage_stride, (int)ws_stride);
     return cudaGetLastError();
 }
 
+// ws: one warp's workspace bytes (a multiple of 16); a team's block holds
+// `team` of them
 cudaError_t launch_eval32(const DModel* dm, size_t stage, size_t ws, const DTables32& T, const DMaps32& G, int n,
                           const double* confs, const double v[3], double slope, double* e, double* g, double* coords,
-                          cudaStream_t s) {
-    const size_t smem = stage + ws;
-    cudaError_t rc = prep32((const void*)k_eval32, smem);
+                          int team, cudaStream_t s) {
+    if (!(team == 1 || team == 2 || team == 4)) return cudaErrorInvalidValue;
+    const size_t smem = stage + (size_t)team * ws;
+    const void* fn = team == 4 ? (const void*)k_eval32<4> : team == 2 ? (const void*)k_eval32<2> : (const void*)k_eval32<1>;
+    cudaError_t rc = prep32(fn, smem);
     if (rc != cudaSuccess) return rc;
-    k_eval32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, e, g, coords,
-                                 (int)stage);
+    const float v0 = (float)v[0], v1 = (float)v[1], v2 = (float)v[2], sl = (float)slope;
+    if (team == 4) k_eval32<4><<<n, 128, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, e, g, coords, (int)stage, (int)ws);
+    else if (team == 2) k_eval32<2><<<n, 64, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, e, g, coords, (int)stage, (int)ws);
+    else k_eval32<1><<<n, 32, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, e, g, coords, (int)stage, (int)ws);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bfgs32(const DModel* dm, size_t stage, size_t ws, const DTables32& T, const DMaps32& G, int n,
                           double* confs, const double v[3], double slope, int maxiters, int accurate, int early,
-                          double* e, cudaStream_t s) {
-    const size_t smem = stage + ws;
-    cudaError_t rc = prep32((const void*)k_bfgs32, smem);
+                          double* e, int team, cudaStream_t s) {
+    if (!(team == 1 || team == 2 || team == 4)) return cudaErrorInvalidValue;
+    const size_t smem = stage + (size_t)team * ws;
+    const void* fn = team == 4 ? (const void*)k_bfgs32<4> : team == 2 ? (const void*)k_bfgs32<2> : (const void*)k_bfgs32<1>;
+    cudaError_t rc = prep32(fn, smem);
     if (rc != cudaSuccess) return rc;
-    k_bfgs32<<<n, 32, smem, s>>>(dm, T, G, n, confs, (float)v[0], (float)v[1], (float)v[2], (float)slope, maxiters,
-                                 accurate, early, e, (int)stage);
+    const float v0 = (float)v[0], v1 = (float)v[1], v2 = (float)v[2], sl = (float)slope;
+    if (team == 4)
+        k_bfgs32<4><<<n, 128, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, maxiters, accurate, early, e, (int)stage, (int)ws);
+    else if (team == 2)
+        k_bfgs32<2><<<n, 64, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, maxiters, accurate, early, e, (int)stage, (int)ws);
+    else
+        k_bfgs32<1><<<n, 32, smem, s>>>(dm, T, G, n, confs, v0, v1, v2, sl, maxiters, accurate, early, e, (int)stage, (int)ws);
     return cudaGetLastError();
 }
 

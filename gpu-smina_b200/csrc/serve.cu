@@ -110,6 +110,8 @@ static void sv_add_pose(std::vector<SvPose>& out, SvPose&& t, double min_rmsd, i
 struct SvLig {
     ServeReq req;
     int model = 0, first = 0, nchains = 0, flag = -1;
+    int blocks = 0;  // its work items (a block's worth of its chains each)
+    int team = 1;    // warps per chain of its search
     int state = 0;  // 0 searching, 1 refining, 2 published
     uint64_t evals = 0;
     uint64_t dev_start = 0, dev_end = 0;  // device clock (ns): first chain's start, last chain's end
@@ -171,6 +173,7 @@ struct Server {
     cudaStream_t feed_stream = nullptr, ctrl_stream = nullptr;
     std::vector<cudaStream_t> grid_streams;  // a grid per stream; grids end on their own
     int inflight_ligs = 0;
+    long long inflight_blocks = 0;  // work items of ligands whose chains are not yet seen done
     cudaStream_t refine_stream = nullptr, copy_stream = nullptr;
     // completion flags in host-mapped memory
     volatile unsigned* flags = nullptr;
@@ -282,14 +285,36 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     }
     ws_stride = (ws_stride + 15) & ~(size_t)15;
     for (auto& r : reqs) max_chains = std::max(max_chains, r.job.num_chains);
-    // the most chains per block that fit the server's fixed shared memory per block
-    int wpb = 0;
-    for (int c : {8, 4, 2, 1}) {
-        if (e->force_wpb && c != e->force_wpb) continue;
-        if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;
-        if (stage_stride + (size_t)c * ws_stride <= s.smem_block) { wpb = c; break; }
+    // the most chains per block (8-warp blocks, chains on teams of g warps)
+    // that fit the server's fixed shared memory per block
+    auto chains_per_block = [&](int g) {
+        for (int c : {8, 4, 2, 1}) {
+            if (c * g > 8) continue;
+            if (e->force_wpb && c != e->force_wpb) continue;
+            if (!e->force_wpb && c > 1 && c / 2 >= max_chains) continue;
+            if (stage_stride + (size_t)c * g * ws_stride <= s.smem_block) return c;
+        }
+        return 0;
+    };
+    // Threads per chain: the engine's setting, or (0) the most warps per
+    // chain (128, 64) at which the items in flight and this batch's all
+    // have a block at once, so that a lone ligand's chains run shorter.
+    int team = std::max(1, e->tpc / 32);
+    if (e->tpc == 0) {
+        team = 1;
+        for (int g : {4, 2}) {
+            const int c = chains_per_block(g);
+            if (!c) continue;
+            long long nb = 0;
+            for (auto& r : reqs) nb += (r.job.num_chains + c - 1) / c;
+            if (s.inflight_blocks + nb <= s.target_blocks) {
+                team = g;
+                break;
+            }
+        }
     }
-    require(wpb > 0, "serve: model too large for the mixed-precision path's shared memory");
+    const int wpb = chains_per_block(team);
+    require(wpb > 0, "serve: model too large for the mixed-precision path's shared memory at this many threads per chain");
     std::vector<Item32> items;
     std::vector<double> cost;
     size_t conf_off = 0, xyz_off = 0;
@@ -308,6 +333,7 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
         L.xyz_off = xyz_off;
         L.batch = b.get();
         L.launch = b->seq;
+        L.team = team;
         L.t_launch = Clock::now();
         const sg_ligand_job& J = L.req.job;
         for (int c = 0; c < J.num_chains; c++) {
@@ -339,7 +365,9 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
         for (int c0 = 0; c0 < J.num_chains; c0 += wpb) {
             items.push_back(Item32{(int)k, L.first + c0, std::min(wpb, J.num_chains - c0), L.req.rid});
             cost.push_back((double)J.num_steps * h.cost * std::max(1, b->hc[L.first].maxiters));
+            L.blocks++;
         }
+        s.inflight_blocks += L.blocks;
         b->ligs.push_back(std::move(L));
     }
     std::vector<int> order(items.size());
@@ -388,7 +416,7 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
     for (unsigned k = 0; k < n; k++) {
         fi[k] = FeedItem32{dms + q[k].model, dch + q[k].first, dmaps + q[k].rec,
                            reinterpret_cast<const MCParams32*>(b->dmem + params_at), q[k].count, (int)stage_stride,
-                           (int)ws_stride, 0};
+                           (int)ws_stride, team};
     }
     unsigned* tail_word = reinterpret_cast<unsigned*>(b->pin + r16(sizeof(MCParams32)) + n * sizeof(FeedItem32));
     *tail_word = s.tail + n;
@@ -427,6 +455,7 @@ static void pin_put(Server& s, char* p, size_t cap) {
 // A ligand's chains are done: copy their containers back and merge them.
 static void fetch_merge(Server& s, SvBatch& b, SvLig& L) {
     L.t_flag = Clock::now();
+    s.inflight_blocks -= L.blocks;
     const DModel& h = b.img.host[L.model];
     const int S = b.S, cs = h.conf_size, H = h.nheavy;
     const size_t nc = L.nchains;
@@ -598,6 +627,7 @@ static void publish(Server& s, const RefineGroup& g, size_t k) {
     d.info.launch = L.launch;
     d.info.queue_ms = std::chrono::duration<double, std::milli>(L.t_launch - L.req.t_submit).count();
     d.info.searched_ms = std::chrono::duration<double, std::milli>(L.t_flag - L.req.t_submit).count();
+    d.info.threads_per_chain = 32 * L.team;
     d.info.device_start_ns = L.dev_start;
     d.info.device_end_ns = L.dev_end;
     for (int i = 0; i < np; i++) {
@@ -640,6 +670,7 @@ static void fail_all(Server& s, int code, const std::string& why) {
     s.inflight.clear();
     s.refining.clear();
     s.inflight_bytes = 0;
+    s.inflight_blocks = 0;
     s.cv_done.notify_all();
 }
 

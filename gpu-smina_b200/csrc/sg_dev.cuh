@@ -181,10 +181,10 @@ struct __align__(16) FeedItem32 {
     const Chain32* chains;     // [count]
     const DMaps32* maps;       // the ligand's receptor's map set
     const MCParams32* params;
-    int count;                 // chains (warps) of this item
+    int count;                 // chains of this item
     int stage_stride;          // shared-memory layout of the item's block
     int ws_stride;
-    int pad_;
+    int team;                  // warps per chain: 1, 2 or 4
 };
 // The ring's control words (device memory): the host advances tail after
 // copying items in; blocks claim items by advancing head

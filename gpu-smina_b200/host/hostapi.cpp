@@ -97,6 +97,38 @@ int sgh_receptor_pdbqt(const sgh_receptor* r, char* buf, int buflen) {
     return 0;
 }
 
+int sgh_sdf_count(const char* text) {
+    int n = -1;
+    if (guarded([&] {
+            if (!text) throw std::runtime_error("sdf_count: null text");
+            n = sgh::sdf_count(text);
+        }))
+        return -1;
+    return n;
+}
+
+int sgh_pdbqt_from_sdf(const char* text, int index, int add_hydrogens, char* buf, int buflen) {
+    std::string s;
+    if (guarded([&] {
+            if (!text || index < 0) throw std::runtime_error("pdbqt_from_sdf: bad arguments");
+            s = sgh::pdbqt_from_sdf(text, index, add_hydrogens != 0);
+        }))
+        return -1;
+    if ((int)s.size() + 1 > buflen) return (int)s.size() + 1;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return 0;
+}
+
+int sgh_model_from_sdf(const char* text, int index, int add_hydrogens, sgh_model** out) {
+    *out = nullptr;
+    return guarded([&] {
+        if (!text || index < 0) throw std::runtime_error("model_from_sdf: bad arguments");
+        sgh_model* m = new sgh_model();
+        try { m->m = sgh::read_pdbqt_ligand(sgh::pdbqt_from_sdf(text, index, add_hydrogens != 0)); } catch (...) { delete m; throw; }
+        *out = m;
+    });
+}
+
 int sgh_make_ligand_pdbqt(int heavy, int rotors, uint64_t seed, const double center[3], char* buf, int buflen) {
     std::string s;
     int rc = guarded([&] { s = sgh::make_ligand_pdbqt(heavy, rotors, seed, center); });

@@ -95,7 +95,7 @@ class ServeDone(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("status", C.c_int), ("count", C.c_int), ("conf_size", C.c_int),
                 ("num_heavy", C.c_int), ("evals", C.c_uint64), ("latency_ms", C.c_double), ("launch", C.c_uint64),
                 ("device_start_ns", C.c_uint64), ("device_end_ns", C.c_uint64), ("queue_ms", C.c_double),
-                ("searched_ms", C.c_double)]
+                ("searched_ms", C.c_double), ("threads_per_chain", C.c_int), ("pad_", C.c_int)]
 
 
 _lib = None
@@ -119,6 +119,9 @@ def _declare(L):
     L.sg_last_error.argtypes = [vp]
     for name, args in {
         "sgh_model_from_pdbqt": [C.c_char_p, C.POINTER(vp)],
+        "sgh_sdf_count": [C.c_char_p],
+        "sgh_pdbqt_from_sdf": [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int],
+        "sgh_model_from_sdf": [C.c_char_p, C.c_int, C.c_int, C.POINTER(vp)],
         "sgh_model_desc": [vp, C.POINTER(ModelDesc)],
         "sgh_model_heavy": [vp], "sgh_model_torsdof": [vp],
         "sgh_make_receptor": [C.c_int, C.c_uint64, C.c_double * 3, C.c_double, C.POINTER(vp)],
@@ -168,6 +171,8 @@ def _declare(L):
         "sg_batch_stats": [vp, _dp, _dp, _ip, _ip],
         "sg_batch_counters": [vp] + [C.POINTER(C.c_uint64)] * 5,
         "sg_set_chains_per_block": [vp, C.c_int],
+        "sg_set_threads_per_chain": [vp, C.c_int],
+        "sg_threads_per_chain": [vp, _ip, _ip],
         "sg_set_early_stop": [vp, C.c_void_p],
         "sg_autotune32": [vp, C.c_int, C.POINTER(ModelDesc), C.c_int, C.POINTER(LigandJob), C.c_int,
                           C.POINTER(MCParams), C.c_double, _dp, _ip],
@@ -307,6 +312,27 @@ class Receptor:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.sgh_receptor_free(self._h)
             self._h = None
+
+
+def sdf_count(text: str) -> int:
+    """Records in SDF text (sgh_sdf_count)."""
+    L = load()
+    n = L.sgh_sdf_count(text.encode())
+    if n < 0:
+        raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
+    return n
+
+
+def pdbqt_from_sdf(text: str, index: int = 0, add_hydrogens: bool = True) -> str:
+    """SDF record ``index`` as the PDBQT the reference's converter writes
+    (sgh_pdbqt_from_sdf); ``Model(pdbqt_from_sdf(...))`` docks it."""
+    L = load()
+    need = L.sgh_pdbqt_from_sdf(text.encode(), index, int(add_hydrogens), None, 0)
+    if need < 0:
+        raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
+    buf = C.create_string_buffer(need)
+    L.sgh_pdbqt_from_sdf(text.encode(), index, int(add_hydrogens), buf, need)
+    return buf.value.decode()
 
 
 def make_ligand_pdbqt(heavy: int, rotors: int, seed: int, center=(0.0, 0.0, 0.0)) -> str:
@@ -634,7 +660,8 @@ class Engine:
 
     def serve_poll(self, max_n=256, wait_ms=0, spans=False):
         """Finished requests as (ticket, status, count, latency_ms, evals, conf_size, num_heavy) tuples;
-        with spans, each tuple also carries (launch, device_start_ns, device_end_ns, queue_ms, searched_ms)."""
+        with spans, each tuple also carries (launch, device_start_ns, device_end_ns, queue_ms, searched_ms,
+        threads_per_chain)."""
         buf = (ServeDone * max_n)()
         n = C.c_int()
         self._check(load().sg_serve_poll(self._h, buf, max_n, wait_ms, C.byref(n)))
@@ -642,7 +669,8 @@ class Engine:
         for i in range(n.value):
             d = buf[i]
             t = (d.ticket, d.status, d.count, d.latency_ms, d.evals, d.conf_size, d.num_heavy)
-            out.append(t + (d.launch, d.device_start_ns, d.device_end_ns, d.queue_ms, d.searched_ms) if spans else t)
+            out.append(t + (d.launch, d.device_start_ns, d.device_end_ns, d.queue_ms, d.searched_ms,
+                            d.threads_per_chain) if spans else t)
         return out
 
     def serve_fetch(self, ticket, count, conf_size, num_heavy):
@@ -661,6 +689,16 @@ class Engine:
 
     def set_chains_per_block(self, n: int):
         self._check(load().sg_set_chains_per_block(self._h, n))
+
+    def set_threads_per_chain(self, threads: int):
+        """Threads per chain of the batched search and the serving loop: 32, 64, 128, or 0 (by load)."""
+        self._check(load().sg_set_threads_per_chain(self._h, threads))
+
+    def threads_per_chain(self):
+        """(setting, the last batch's threads per chain)."""
+        a, b = C.c_int(), C.c_int()
+        self._check(load().sg_threads_per_chain(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def set_early_stop(self, checkpoints=10, first=2, fraction=0.5, eps=0.05, chains_per_unit=1, off=False):
         """--fast's early stop for later dock_batch calls (sg_set_early_stop); off=True turns it off."""

@@ -399,10 +399,26 @@ int sg_batch_stats(const sg_engine* e, double* mc_ms, double* refine_ms,
 int sg_batch_counters(const sg_engine* e, uint64_t* evals, uint64_t* grid_lookups,
                       uint64_t* pair_lookups, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
-/* Chains (warps) per block of the search kernel: 1, 2, 4 or 8, or 0 to
- * pick the shape with the most resident chains per SM (the default).  The
- * chains of one block share one copy of their ligand's model. */
+/* Chains per block of the search kernel: 1, 2, 4 or 8 (at most 8 warps
+ * per block, so 2 with 128 threads per chain), or 0 to pick the shape with
+ * the most resident chains per SM (the default; a batch of at most one
+ * chain per SM then runs one chain per block).  The chains of one block
+ * share one copy of their ligand's model. */
 int sg_set_chains_per_block(sg_engine* e, int n);
+
+/* Threads per chain of the batched search (sg_dock_batch32, and the FP32
+ * sg_eval / sg_bfgs): 32 (the default), 64 or 128 -- the reference's
+ * threads_per_chain (gpu_kernels_impl.cuh:572-605) -- or 0 to pick, per
+ * call, the most (128, 64, 32) at which the batch's chains all stay
+ * resident at once.  More threads per chain shorten each chain (its grid
+ * and pair terms are shared out among the warps) when the device has warps
+ * to spare, such as for a lone ligand; they do not raise a full device's
+ * throughput.  Results depend on the setting (the order of FP32 additions
+ * changes with the team size) but, for a given value, not on the batch or
+ * the launch shape; with 0 the value follows the batch's size.
+ * sg_threads_per_chain reports the setting and the last batch's value. */
+int sg_set_threads_per_chain(sg_engine* e, int threads);
+int sg_threads_per_chain(const sg_engine* e, int* configured, int* last_batch);
 
 /* Launch-shape autotuner for the search kernel: runs the given jobs with
  * their step counts scaled by step_fraction (0 < f <= 1, at least one step
@@ -465,6 +481,12 @@ typedef struct sg_serve_done {
                                   queue)                                    */
     double searched_ms;        /* submit to the worker seeing its chains
                                   done (then merge and FP64 refinement)     */
+    int threads_per_chain;     /* its search's threads per chain (32, 64,
+                                  128): the engine's sg_set_threads_per_chain
+                                  setting at its upload, or with 0 there the
+                                  most at which everything on the device
+                                  then had a block at once                  */
+    int pad_;
 } sg_serve_done;
 
 int sg_serve_start(sg_engine* e, const sg_serve_opts* opts);

@@ -22,7 +22,7 @@
  *     planned by sgh_fast_chains; early_stop on FP32 engines (the batched
  *     search in phases, sg_set_early_stop, with the reference's rule and
  *     checkpoints); skip_visited on FP64 engines.  Refused at construction
- *     with a message: threads_per_chain above 32, skip_visited with FP32
+ *     with a message: threads_per_chain above 32 with FP64, skip_visited with FP32
  *     engines (QuickVina 2's history runs on the FP64 path only) and
  *     early_stop with FP64 engines (the plain path does not run in phases).
  *
@@ -56,7 +56,7 @@ namespace smina_b200 {
 struct GpuSettings {
     std::vector<int> devices{0};
     bool fp64 = false;
-    int threads_per_chain = 0;  /* 0: automatic; only 32 threads per chain are built */
+    int threads_per_chain = 0;  /* 0: automatic (by the batch's size), or 32, 64, 128 */
     int chain_split = 1;        /* chains per search task (0: automatic, --fast) */
     double step_fraction = 1;   /* fraction of smina's steps (0: automatic, --fast) */
     bool skip_visited = false;
@@ -186,8 +186,12 @@ public:
             throw std::runtime_error("early_stop: unknown mode");
         if (s.early_stop != GpuSettings::EARLY_STOP_OFF && s.fp64)
             throw std::runtime_error("early_stop needs the FP32 search (the FP64 path does not run in phases)");
-        if (s.threads_per_chain != 0 && s.threads_per_chain != 32)
-            throw std::runtime_error("threads_per_chain: this engine runs 32 threads per chain");
+        if (!(s.threads_per_chain == 0 || s.threads_per_chain == 32 || s.threads_per_chain == 64 ||
+              s.threads_per_chain == 128))
+            throw std::runtime_error("threads_per_chain: 0 (automatic), 32, 64 or 128");
+        if (s.fp64 && s.threads_per_chain > 32)
+            throw std::runtime_error("threads_per_chain above 32 needs the FP32 search (the FP64 path runs one warp "
+                                     "per chain, bit for bit as the CPU search)");
         if (s.skip_visited && !s.fp64)
             throw std::runtime_error("skip_visited needs the double precision search (fp64)");
         for (size_t i = 0; i < s.devices.size(); i++) {
@@ -205,6 +209,7 @@ public:
                 dev_.clear();
                 throw std::runtime_error("CUDA device " + std::to_string(d) + " is not usable");
             }
+            if (!s.fp64) sg_set_threads_per_chain(x.search, s.threads_per_chain);
             dev_.push_back(x);
         }
     }

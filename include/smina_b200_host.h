@@ -35,6 +35,18 @@ typedef struct sgh_tables sgh_tables;
 const char* sgh_last_error(void);
 
 int  sgh_model_from_pdbqt(const char* text, sgh_model** out);
+/* SDF / MOL (V2000) ligands, the reference's OpenBabel route
+ * (molgetter.cpp:103-125 with SminaConverter.cpp:87-130 and
+ * PDBQTUtilities.cpp:50-627) without OpenBabel: record `index` (0-based;
+ * records end at "$$$$") typed, charged (Gasteiger) and cut into a
+ * torsion tree, written as PDBQT, and read by the PDBQT reader.
+ * add_hydrogens: add the hydrogens N, O and S lack (the reference's
+ * default adds them).  sgh_sdf_count returns the records in the text (or
+ * -1); sgh_pdbqt_from_sdf returns 0, -1 on error, or the buffer size
+ * needed. */
+int  sgh_sdf_count(const char* text);
+int  sgh_pdbqt_from_sdf(const char* text, int index, int add_hydrogens, char* buf, int buflen);
+int  sgh_model_from_sdf(const char* text, int index, int add_hydrogens, sgh_model** out);
 /* A ligand plus the receptor's flexible residues (smina --flex; flex PDBQT
  * with BEGIN_RES/END_RES blocks, parse_pdbqt.cpp:412-437), combined as
  * model::append does (model.cpp:302-347). */

@@ -124,6 +124,9 @@ static void device_checks() {
     const int S = mc.num_saved_mins, tasks = 4, seed = 7;
     sg_engine* e32 = engine(SG_PREC_FP32, T, R, gd);
     sg_engine* e64 = engine(SG_PREC_FP64, T, R, gd);
+    // the class's default threads_per_chain (0: automatic), so that its
+    // results and the C ABI's are the same searches
+    require_ok(sg_set_threads_per_chain(e32, 0), "automatic threads per chain");
 
     // FP32 engine: parallel_mc = one batched job, not refined
     GpuDocking g32(GpuSettings{});
@@ -341,8 +344,12 @@ int main(int argc, char** argv) {
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_FULL; s.fp64 = true; })); },
                  "early_stop", "early_stop with fp64");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = 7; })); }, "early_stop", "unknown early_stop");
-    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 128; })); }, "threads_per_chain",
-                 "threads_per_chain");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 256; })); }, "threads_per_chain",
+                 "threads_per_chain 256");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 48; })); }, "threads_per_chain",
+                 "threads_per_chain 48");
+    expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 64; s.fp64 = true; })); },
+                 "FP32 search", "threads_per_chain 64 with fp64");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.skip_visited = true; })); }, "fp64",
                  "skip_visited without fp64");
     expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.devices.clear(); })); }, "no CUDA device",
@@ -358,6 +365,8 @@ int main(int argc, char** argv) {
                      "not usable", "--fast settings pass validation");
         expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.fp64 = true; })); }, "not usable",
                      "no device present, fp64");
+        expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.threads_per_chain = 128; })); }, "not usable",
+                     "threads_per_chain 128 passes validation");
         expect_throw([] { GpuDocking g(with([](GpuSettings& s) { s.early_stop = GpuSettings::EARLY_STOP_ALWAYS; })); },
                      "not usable", "early_stop passes validation on FP32");
     }

@@ -21,7 +21,8 @@ def _job(seed, key, chains=4, steps=25):
 def _collect(eng, tickets, timeout_s=120):
     got, t0 = {}, time.time()
     while len(got) < len(tickets) and time.time() - t0 < timeout_s:
-        for (t, status, count, lat, evals, cs, nh, launch, d0, d1, qms, sms) in eng.serve_poll(64, wait_ms=50, spans=True):
+        for (t, status, count, lat, evals, cs, nh, launch, d0, d1, qms, sms, tpc) in eng.serve_poll(64, wait_ms=50,
+                                                                                                 spans=True):
             assert status == sb.SG_OK
             got[t] = eng.serve_fetch(t, count, cs, nh)
             got[t].update(latency_ms=lat, launch=launch, span=(d0, d1), queue_ms=qms)
