@@ -475,37 +475,6 @@ __device__ __forceinline__ int add_output32(const W32& w, const Chain32& ch, con
     return count;
 }
 
-// A later phase of a chain (early stop): the state the previous phase saved
-// -- conf, current and best energy, draw index, atom and frame positions --
-// and the chain's output count.  Out of line, as is the save, so that the
-// chain loop's registers are those of a chain without phases.
-__device__ __noinline__ double3 resume_restore32(const Chain32& ch, double* tmp) {
-    const W32 w = here();
-    const SModel& m = smodel();
-    const int cs = m.conf_size;
-    const float4* sx = reinterpret_cast<const float4*>(ch.resume + resume32_coords_at(cs));
-    for (int i = w.lane; i < cs; i += 32) tmp[i] = ch.resume[i];
-    for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = sx[i];
-    for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = sx[m.natoms + f];
-    __syncwarp();
-    return make_double3(ch.resume[cs], ch.resume[cs + 1], ch.resume[cs + 2]);  // tmp_e, best_e, draw index
-}
-__device__ __noinline__ void resume_save32(const Chain32& ch, const double* tmp, double tmp_e, double best_e,
-                                           uint32_t draws) {
-    const W32 w = here();
-    const SModel& m = smodel();
-    const int cs = m.conf_size;
-    float4* sx = reinterpret_cast<float4*>(ch.resume + resume32_coords_at(cs));
-    for (int i = w.lane; i < cs; i += 32) ch.resume[i] = tmp[i];
-    for (int i = w.lane; i < m.natoms; i += 32) sx[i] = w.coords()[i];
-    for (int f = w.lane; f < m.nframes; f += 32) sx[m.natoms + f] = w.origin()[f];
-    if (w.lane == 0) {
-        ch.resume[cs] = tmp_e;
-        ch.resume[cs + 1] = best_e;
-        ch.resume[cs + 2] = (double)draws;
-    }
-}
-
 // monte_carlo::operator() for one chain, run by the leader of its team of G
 // warps
 template <int G>
@@ -520,18 +489,23 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
     const int cs = m.conf_size;
     // model state as read (mutation may read it before the first set)
     const unsigned first = ch.begin, last = ch.end ? ch.end : ch.steps;
+    const bool resumed = ch.resume && first > 0;
     const int tmp_at = w.at(L.x_tmp), cand_at = w.at(L.x_cand);
     double* tmp = sp<double>(tmp_at);
     double* cand = sp<double>(cand_at);
     Philox rng{ch.key0, ch.key1, ch.lig, ch.chain, 0u};
     double tmp_e = 0, best_e = kMaxFl;
     int count = 0;
-    if (ch.resume && first > 0) {  // a later phase: the state the previous one saved
-        const double3 r = resume_restore32(ch, tmp);
-        tmp_e = r.x;
-        best_e = r.y;
-        rng.n = (uint32_t)r.z;
+    const float4* saved_xyz = ch.resume ? reinterpret_cast<const float4*>(ch.resume + resume32_coords_at(cs)) : nullptr;
+    if (resumed) {  // a later phase: the state the previous one saved
+        for (int i = w.lane; i < cs; i += 32) tmp[i] = ch.resume[i];
+        for (int i = w.lane; i < m.natoms; i += 32) w.coords()[i] = saved_xyz[i];
+        for (int f = w.lane; f < m.nframes; f += 32) w.origin()[f] = saved_xyz[m.natoms + f];
+        tmp_e = ch.resume[cs];
+        best_e = ch.resume[cs + 1];
+        rng.n = (uint32_t)ch.resume[cs + 2];
         count = *ch.out_count;
+        __syncwarp();
     } else {
         // (L2-only loads: a serving grid may read a ligand placed where an
         // earlier one was, and this SM's L1 may still hold the earlier one's lines)
@@ -564,9 +538,17 @@ __device__ __noinline__ void run_chain32(const Chain32& ch, const MCParams32& P)
         }
     }
     __syncwarp();
-    // the state a later phase resumes from (and the best energy, for the stopping rule)
-    if (ch.resume) resume_save32(ch, tmp, tmp_e, best_e, rng.n);
-    const bool resumed = ch.resume && ch.begin > 0;
+    if (ch.resume) {  // the state a later phase resumes from (and the best energy, for the stopping rule)
+        float4* sx = reinterpret_cast<float4*>(ch.resume + resume32_coords_at(cs));
+        for (int i = w.lane; i < cs; i += 32) ch.resume[i] = tmp[i];
+        for (int i = w.lane; i < m.natoms; i += 32) sx[i] = w.coords()[i];
+        for (int f = w.lane; f < m.nframes; f += 32) sx[m.natoms + f] = w.origin()[f];
+        if (w.lane == 0) {
+            ch.resume[cs] = tmp_e;
+            ch.resume[cs + 1] = best_e;
+            ch.resume[cs + 2] = (double)rng.n;
+        }
+    }
     unsigned long long gh = C[w.lane], ph = C[32 + w.lane];
     for (int o = 16; o > 0; o >>= 1) {
         gh += __shfl_xor_sync(kFull32, gh, o);

@@ -415,7 +415,11 @@ int sg_set_chains_per_block(sg_engine* e, int n);
  * to spare, such as for a lone ligand; they do not raise a full device's
  * throughput.  Results depend on the setting (the order of FP32 additions
  * changes with the team size) but, for a given value, not on the batch or
- * the launch shape; with 0 the value follows the batch's size.
+ * the launch shape; with 0 the value follows the batch's size.  A serving
+ * loop (sg_serve_*) reads the setting at each upload; with 0 it picks, per
+ * upload, the most at which the work items already on the device and the
+ * new batch's all have a block (each result reports its value).  FP64
+ * engines ignore it: the plain path runs one warp per chain.
  * sg_threads_per_chain reports the setting and the last batch's value. */
 int sg_set_threads_per_chain(sg_engine* e, int threads);
 int sg_threads_per_chain(const sg_engine* e, int* configured, int* last_batch);
