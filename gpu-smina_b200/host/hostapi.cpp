@@ -107,6 +107,18 @@ int sgh_sdf_count(const char* text) {
     return n;
 }
 
+int sgh_sdf_offsets(const char* text, int64_t* offsets, int max) {
+    int n = -1;
+    if (guarded([&] {
+            if (!text || max < 0 || (max > 0 && !offsets)) throw std::runtime_error("sdf_offsets: bad arguments");
+            const std::vector<size_t> st = sgh::sdf_starts(text);
+            for (int k = 0; k < (int)st.size() && k < max; k++) offsets[k] = (int64_t)st[k];
+            n = (int)st.size();
+        }))
+        return -1;
+    return n;
+}
+
 int sgh_pdbqt_from_sdf(const char* text, int index, int add_hydrogens, char* buf, int buflen) {
     std::string s;
     if (guarded([&] {

@@ -399,42 +399,52 @@ void gasteiger(Mol& m, const Graph& g) {
 
 }  // namespace
 
-int sdf_count(const std::string& text) {
-    int n = 0;
-    std::istringstream in(text);
-    std::string s, cur;
+// byte offsets at which the records of an SDF text start (a record ends at
+// a "$$$$" line; lines that are all blank do not make a record)
+std::vector<size_t> sdf_starts(const std::string& text) {
+    std::vector<size_t> out;
+    size_t pos = 0, start = 0;
     bool any = false;
-    while (std::getline(in, s)) {
-        if (s.compare(0, 4, "$$$$") == 0) {
-            if (any) n++;
+    while (pos < text.size()) {
+        size_t end = text.find('\n', pos);
+        if (end == std::string::npos) end = text.size();
+        const std::string line = text.substr(pos, end - pos);
+        if (line.compare(0, 4, "$$$$") == 0) {
+            if (any) out.push_back(start);
             any = false;
-            continue;
+            start = end + 1;
+        } else if (!strip(line).empty()) {
+            any = true;
         }
-        if (!strip(s).empty()) any = true;
+        pos = end + 1;
     }
-    return n + (any ? 1 : 0);
+    if (any) out.push_back(start);
+    return out;
 }
 
+int sdf_count(const std::string& text) { return (int)sdf_starts(text).size(); }
+
+// record `index`; scans no further than its end
 static std::string sdf_record(const std::string& text, int index) {
-    std::istringstream in(text);
-    std::string s, cur;
-    int k = 0;
+    size_t pos = 0, start = 0;
     bool any = false;
-    while (std::getline(in, s)) {
-        if (s.compare(0, 4, "$$$$") == 0) {
+    int k = 0;
+    while (pos < text.size()) {
+        size_t end = text.find('\n', pos);
+        if (end == std::string::npos) end = text.size();
+        if (text.compare(pos, 4, "$$$$") == 0) {
             if (any) {
-                if (k == index) return cur;
+                if (k == index) return text.substr(start, pos - start);
                 k++;
             }
-            cur.clear();
             any = false;
-            continue;
+            start = end + 1;
+        } else if (!strip(text.substr(pos, end - pos)).empty()) {
+            any = true;
         }
-        if (!strip(s).empty()) any = true;
-        cur += s;
-        cur += '\n';
+        pos = end + 1;
     }
-    if (any && k == index) return cur;
+    if (any && k == index) return text.substr(start);
     throw std::runtime_error("SDF: no record " + std::to_string(index));
 }
 

@@ -120,6 +120,7 @@ Model read_pdbqt_ligand(const std::string& text);
 // SDF / MOL V2000 records: how many, and record `index` as the PDBQT the
 // reference's converter writes (sdf.cpp)
 int sdf_count(const std::string& text);
+std::vector<size_t> sdf_starts(const std::string& text);  // byte offset of each record
 std::string pdbqt_from_sdf(const std::string& text, int index, bool add_hydrogens);
 // A ligand with the receptor's flexible residues (smina --flex): residues in
 // PDBQT BEGIN_RES/END_RES blocks (parse_pdbqt.cpp:412-437), the ligand

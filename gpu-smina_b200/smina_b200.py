@@ -120,6 +120,7 @@ def _declare(L):
     for name, args in {
         "sgh_model_from_pdbqt": [C.c_char_p, C.POINTER(vp)],
         "sgh_sdf_count": [C.c_char_p],
+        "sgh_sdf_offsets": [C.c_char_p, C.POINTER(C.c_int64), C.c_int],
         "sgh_pdbqt_from_sdf": [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int],
         "sgh_model_from_sdf": [C.c_char_p, C.c_int, C.c_int, C.POINTER(vp)],
         "sgh_model_desc": [vp, C.POINTER(ModelDesc)],
@@ -321,6 +322,20 @@ def sdf_count(text: str) -> int:
     if n < 0:
         raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
     return n
+
+
+def sdf_records(text: str) -> list:
+    """The records of SDF text, each as its own text (sgh_sdf_offsets); pass
+    them one at a time to ``pdbqt_from_sdf`` for a large file."""
+    L = load()
+    raw = text.encode()
+    n = L.sgh_sdf_offsets(raw, None, 0)
+    if n < 0:
+        raise SminaError(SG_ERR_ARG, L.sgh_last_error().decode())
+    off = (C.c_int64 * max(n, 1))()
+    L.sgh_sdf_offsets(raw, off, n)
+    ends = list(off[1:n]) + [len(raw)]
+    return [raw[off[k]:ends[k]].decode() for k in range(n)]
 
 
 def pdbqt_from_sdf(text: str, index: int = 0, add_hydrogens: bool = True) -> str:

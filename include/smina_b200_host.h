@@ -45,6 +45,10 @@ int  sgh_model_from_pdbqt(const char* text, sgh_model** out);
  * -1); sgh_pdbqt_from_sdf returns 0, -1 on error, or the buffer size
  * needed. */
 int  sgh_sdf_count(const char* text);
+/* Byte offsets of the records (up to max written; returns the count, or
+ * -1).  For a large file, pass text + offsets[k] with index 0: a call then
+ * reads only that record, where index k scans the k records before it. */
+int  sgh_sdf_offsets(const char* text, int64_t* offsets, int max);
 int  sgh_pdbqt_from_sdf(const char* text, int index, int add_hydrogens, char* buf, int buflen);
 int  sgh_model_from_sdf(const char* text, int index, int add_hydrogens, sgh_model** out);
 /* A ligand plus the receptor's flexible residues (smina --flex; flex PDBQT

@@ -184,6 +184,9 @@ def test_records_of_a_file():
     text = sdf("one", a1, b1) + sdf("two", a2, b2)
     assert sb.sdf_count(text) == 2
     assert "Name = two" in sb.pdbqt_from_sdf(text, 1)
+    recs = sb.sdf_records(text + "\n\n")  # trailing blank lines are not a record
+    assert len(recs) == 2 and recs[1].startswith("two")
+    assert [sb.pdbqt_from_sdf(r) for r in recs] == [sb.pdbqt_from_sdf(text, 0), sb.pdbqt_from_sdf(text, 1)]
     with pytest.raises(sb.SminaError):
         sb.pdbqt_from_sdf(text, 2)
 
@@ -226,3 +229,32 @@ def test_synthetic_ligand_round_trip(heavy, rotors, seed):
     assert torsdof(out) == want >= rotors
     m = sb.Model(out)
     assert m.num_movable == len(rows) and m.torsdof == want
+
+
+NAPHTHALENE = [("C", 1.212, 0.7, 0), ("C", 0, 1.4, 0), ("C", -1.212, 0.7, 0), ("C", -1.212, -0.7, 0),
+               ("C", 0, -1.4, 0), ("C", 1.212, -0.7, 0), ("C", 2.425, 1.4, 0), ("C", 3.637, 0.7, 0),
+               ("C", 3.637, -0.7, 0), ("C", 2.425, -1.4, 0)]
+NAPH_EDGES = [(1, 2), (2, 3), (3, 4), (4, 5), (5, 6), (6, 1), (1, 7), (7, 8), (8, 9), (9, 10), (10, 6)]
+
+
+@pytest.mark.parametrize("doubles", [{(2, 3), (4, 5), (6, 1), (7, 8), (9, 10)},   # shared bond double
+                                     {(1, 2), (3, 4), (5, 6), (7, 8), (9, 10)}])  # shared bond single: fused pass
+def test_naphthalene_both_kekule_forms_aromatic(doubles):
+    bonds = [(i, j, 2 if (i, j) in doubles else 1) for i, j in NAPH_EDGES]
+    types = [r[1] for r in atoms_of(sb.pdbqt_from_sdf(sdf("naphthalene", NAPHTHALENE, bonds)))]
+    assert types == ["A"] * 10
+
+
+def test_biphenyl_one_torsion_phenol_and_chlorine():
+    ring_a = ring6()
+    ring_b = [(el, x + 4.29, y, z) for el, x, y, z in ring6()]
+    kek = [(1, 2, 2), (2, 3, 1), (3, 4, 2), (4, 5, 1), (5, 6, 2), (6, 1, 1)]
+    bonds = kek + [(i + 6, j + 6, o) for i, j, o in kek] + [(1, 10, 1)]  # ring A atom 1 to ring B atom 4
+    atoms = ring_a + ring_b + [("O", -2.76, 0.0, 0.0), ("Cl", 5.0, 2.6, 0.0)]
+    bonds += [(4, 13, 1), (8, 14, 1)]
+    p = sb.pdbqt_from_sdf(sdf("biphenyl", atoms, bonds))
+    t = [r[1] for r in atoms_of(p)]
+    assert t.count("A") == 12 and t.count("OA") == 1 and t.count("HD") == 1 and t.count("Cl") == 1
+    assert torsdof(p) == 1  # the ring-ring bond; C-O and C-Cl end at one-heavy-neighbour atoms
+    m = sb.Model(p)
+    assert m.torsdof == 1
