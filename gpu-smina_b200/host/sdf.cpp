@@ -33,6 +33,7 @@
  * Atom order: fragment by fragment in tree order, file order within one.
  */
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <functional>
