@@ -438,6 +438,43 @@ def heavy_rmsd(a, b):
     return float(np.sqrt(((a - b) ** 2).sum(1).mean())) if len(a) else 0.0
 
 
+def run_lone(args):
+    """A lone ligand's search latency at 32, 64 and 128 threads per chain:
+    each ligand of ``args.lone`` ("heavy:rotors,...", synthetic, seed 11)
+    docked alone through the batched entry point (exhaustiveness 8, smina's
+    step counts, seed 5) against the 3,000-atom receptor (22 A box at
+    0.375 A, default scoring), with the device otherwise idle.  For each it
+    runs the previous launch shape (32 threads, 8 chains per block), then 32,
+    64 and 128 threads with the automatic shape, and prints one JSON line per
+    run with the search time (CUDA events, ``sg_batch_stats``)."""
+    import workloads as W
+    eng = sb.Engine(0, sb.PREC_FP32)
+    eng.set_tables(W.tables())
+    eng.set_receptor(0, W.receptor(), W.box())
+    for spec in args.lone.split(","):
+        heavy, rot = (int(x) for x in spec.split(":"))
+        m = W.ligand(heavy, rot, 11)
+        p = m.search_params()
+        steps = max(1, int(p.num_steps * args.step_scale))
+        job = sb.LigandJob(model=0, num_chains=args.exhaustiveness, num_steps=steps, maxiters=0, seed=5, ligand_key=1)
+        eng.set_threads_per_chain(32)
+        eng.dock_batch(0, [m], [sb.LigandJob(model=0, num_chains=args.exhaustiveness, num_steps=2, maxiters=0, seed=5,
+                                             ligand_key=1)], p)  # warm-up
+        for tpc, cpb in [(32, 8), (32, 0), (64, 0), (128, 0)]:
+            eng.set_threads_per_chain(tpc)
+            eng.set_chains_per_block(cpb)
+            t0 = time.perf_counter()
+            r = eng.dock_batch(0, [m], [job], p, refine=True)[0]
+            wall = time.perf_counter() - t0
+            st = eng.batch_stats()
+            print(json.dumps({"mode": "lone", "heavy": heavy, "rotors": rot, "steps": steps, "threads_per_chain": tpc,
+                              "chains_per_block": st["chains_per_block"], "search_ms": round(st["mc_ms"], 1),
+                              "wall_s": round(wall, 2), "best_e": float(r["e"][0]), "evals": int(r["evals"])}),
+                  flush=True)
+        eng.set_chains_per_block(0)
+    eng.close()
+
+
 def run_redock(args):
     """The single-ligand redock: a 24-heavy-atom, 5-rotor ligand against the
     3,000-atom receptor (22 A box at 0.375 A, default scoring, smina's step
@@ -882,6 +919,8 @@ def main():
     ap.add_argument("--flex-screen", type=int, default=0,
                     help="instead of timing the screen: this many ligands of the 20,000-ligand screen with 4 flexible "
                          "residues, custom scoring and FP16 maps, plus an accuracy check against FP64")
+    ap.add_argument("--lone", default="",
+                    help="heavy:rotors,... -- a lone ligand's search time at 32, 64 and 128 threads per chain")
     ap.add_argument("--flex-acc", type=int, default=24, help="with --flex-screen: ligands in the FP64 comparison")
     ap.add_argument("--redock", type=int, default=0,
                     help="instead of timing: the single-ligand redock (FP64 exhaustiveness 8, FP32 exhaustiveness "
@@ -896,6 +935,9 @@ def main():
         return
     if args.flex_screen:
         run_flex(args)
+        return
+    if args.lone:
+        run_lone(args)
         return
     if args.ref_gpu:
         run_ref_gpu(args)
