@@ -214,6 +214,8 @@ int sg_dock_batch32(sg_engine* e, int rid, const sg_model_desc* models, int nmod
                 }
             }
         }
+        require(!e->force_wpb || e->force_wpb * team <= 8,
+                "chains per block (sg_set_chains_per_block) times warps per chain is above 8 warps per block");
         require(try_launch(e, stage_stride, ws_stride, max_chains, team, nchains, wpb, occ),
                 "model too large for the mixed-precision path's shared memory at this many threads per chain");
         MCParams32 P{};

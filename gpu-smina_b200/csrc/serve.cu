@@ -313,6 +313,8 @@ static void launch_batch(Server& s, std::vector<ServeReq>&& reqs) {
             }
         }
     }
+    require(!e->force_wpb || e->force_wpb * team <= 8,
+            "serve: chains per block (sg_set_chains_per_block) times warps per chain is above 8 warps per block");
     const int wpb = chains_per_block(team);
     require(wpb > 0, "serve: model too large for the mixed-precision path's shared memory at this many threads per chain");
     std::vector<Item32> items;
