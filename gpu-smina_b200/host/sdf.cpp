@@ -1,5 +1,5 @@
 /*
- * SDF / MOL (V2000) ligands.  The reference reads them through OpenBabel
+ * SDF / MOL (V2000 and V3000) ligands.  The reference reads them through OpenBabel
  * (molgetter.cpp:103-125) and turns the molecule into smina's parse tree
  * with its own converter (SminaConverter.cpp:87-130, PDBQTUtilities.cpp:
  * 50-627): hydrogens added, non-polar hydrogens deleted with their partial
@@ -95,7 +95,75 @@ double to_double(const std::string& s, const char* what) {
     }
 }
 
-// one MOL record (ctab V2000): header, counts, atom block, bond block, M CHG
+std::string element_symbol(std::string el) {
+    if (el.empty() || !std::isalpha((unsigned char)el[0])) throw std::runtime_error("SDF: atom without element");
+    el[0] = (char)std::toupper((unsigned char)el[0]);
+    for (size_t k = 1; k < el.size(); k++) el[k] = (char)std::tolower((unsigned char)el[k]);
+    if (el == "D" || el == "T") el = "H";
+    return el;
+}
+
+// the connection table of a V3000 record: "M  V30" lines (a trailing "-"
+// continues a line), COUNTS, the ATOM block (index, element, x, y, z,
+// map, then KEY=VALUE fields of which CHG is read) and the BOND block
+// (index, type, atom, atom)
+Mol parse_v3000(const std::vector<std::string>& L, const std::string& name) {
+    std::vector<std::string> v;
+    for (size_t k = 4; k < L.size(); k++) {
+        const std::string& l = L[k];
+        if (l.compare(0, 6, "M  END") == 0) break;
+        if (l.compare(0, 7, "M  V30 ") != 0) continue;
+        std::string body = strip(l.substr(7));
+        if (!v.empty() && !v.back().empty() && v.back().back() == '-') {
+            v.back().pop_back();
+            v.back() += body;
+        } else {
+            v.push_back(body);
+        }
+    }
+    Mol m;
+    m.name = name;
+    int na = -1, nb = -1;
+    enum { NONE, ATOMS, BONDS } block = NONE;
+    std::map<int, int> index_of;  // the file's atom index -> position
+    for (const std::string& line : v) {
+        std::istringstream ls(line);
+        std::string w;
+        ls >> w;
+        if (w == "COUNTS") {
+            ls >> na >> nb;
+            if (!ls || na <= 0 || nb < 0) throw std::runtime_error("SDF: bad V3000 COUNTS line");
+        } else if (w == "BEGIN" || w == "END") {
+            std::string what;
+            ls >> what;
+            block = w == "END" ? NONE : what == "ATOM" ? ATOMS : what == "BOND" ? BONDS : NONE;
+        } else if (block == ATOMS) {
+            MAtom t;
+            std::string el;
+            int map = 0;
+            ls >> el >> t.x[0] >> t.x[1] >> t.x[2] >> map;
+            if (!ls) throw std::runtime_error("SDF: bad V3000 atom line \"" + line + "\"");
+            t.el = element_symbol(el);
+            std::string kv;
+            while (ls >> kv)
+                if (kv.compare(0, 4, "CHG=") == 0) t.charge = to_int(kv.substr(4), "CHG");
+            index_of[to_int(w, "atom index")] = (int)m.atoms.size();
+            m.atoms.push_back(t);
+        } else if (block == BONDS) {
+            int type = 0, a = 0, b = 0;
+            ls >> type >> a >> b;
+            if (!ls || !index_of.count(a) || !index_of.count(b) || a == b)
+                throw std::runtime_error("SDF: bad V3000 bond line \"" + line + "\"");
+            m.bonds.push_back(MBond{index_of[a], index_of[b], (type < 1 || type > 4) ? 1 : type});
+        }
+    }
+    if (na <= 0 || (int)m.atoms.size() != na || (int)m.bonds.size() != nb)
+        throw std::runtime_error("SDF: V3000 counts do not match the atom and bond blocks");
+    return m;
+}
+
+// one MOL record (ctab V2000, or V3000): header, counts, atom block, bond
+// block, M CHG
 Mol parse_mol(const std::string& rec) {
     std::istringstream in(rec);
     std::vector<std::string> L;
@@ -105,7 +173,7 @@ Mol parse_mol(const std::string& rec) {
     Mol m;
     m.name = strip(L[0]);
     const std::string& c = L[3];
-    if (c.find("V3000") != std::string::npos) throw std::runtime_error("SDF: V3000 records are not read (V2000 only)");
+    if (c.find("V3000") != std::string::npos) return parse_v3000(L, m.name);
     const int na = to_int(field(c, 0, 3), "atom count"), nb = to_int(field(c, 3, 3), "bond count");
     if (na <= 0 || nb < 0 || (size_t)(4 + na + nb) > L.size())
         throw std::runtime_error("SDF: counts line does not match the record");
@@ -116,11 +184,7 @@ Mol parse_mol(const std::string& rec) {
         t.x[0] = to_double(field(a, 0, 10), "x");
         t.x[1] = to_double(field(a, 10, 10), "y");
         t.x[2] = to_double(field(a, 20, 10), "z");
-        t.el = strip(field(a, 31, 3));
-        if (t.el.empty() || !std::isalpha((unsigned char)t.el[0])) throw std::runtime_error("SDF: atom without element");
-        t.el[0] = (char)std::toupper((unsigned char)t.el[0]);
-        for (size_t k = 1; k < t.el.size(); k++) t.el[k] = (char)std::tolower((unsigned char)t.el[k]);
-        if (t.el == "D" || t.el == "T") t.el = "H";
+        t.el = element_symbol(strip(field(a, 31, 3)));
         const int cc = to_int(field(a, 36, 3), "charge");
         if (cc < 0 || cc > 7) throw std::runtime_error("SDF: bad charge code");
         t.charge = chg_code[cc];

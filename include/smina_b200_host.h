@@ -35,7 +35,7 @@ typedef struct sgh_tables sgh_tables;
 const char* sgh_last_error(void);
 
 int  sgh_model_from_pdbqt(const char* text, sgh_model** out);
-/* SDF / MOL (V2000) ligands, the reference's OpenBabel route
+/* SDF / MOL (V2000 or V3000) ligands, the reference's OpenBabel route
  * (molgetter.cpp:103-125 with SminaConverter.cpp:87-130 and
  * PDBQTUtilities.cpp:50-627) without OpenBabel: record `index` (0-based;
  * records end at "$$$$") typed, charged (Gasteiger) and cut into a

@@ -1,4 +1,4 @@
-"""SDF / MOL V2000 ligands (sgh_pdbqt_from_sdf, sgh_model_from_sdf): the
+"""SDF / MOL ligands (sgh_pdbqt_from_sdf, sgh_model_from_sdf): the
 reference's OpenBabel route (molgetter.cpp:103-125 through its converter,
 SminaConverter.cpp:87-130, PDBQTUtilities.cpp:50-627) restated without
 OpenBabel.  Checked here on molecules written by the test: typing (aromatic
@@ -6,9 +6,10 @@ carbon, acceptor nitrogen, polar hydrogens), rotatable bonds (single, not
 amide, not in a ring, both ends with another heavy neighbour), the root
 (the atom whose removal leaves the smallest largest piece), non-polar
 hydrogens deleted with their charge moved to their heavy atom, Gasteiger
-charges that sum to the formal charge, records of a multi-record file, and
-a round trip of the synthetic ligands (PDBQT -> SDF -> PDBQT) that keeps
-every heavy atom where it was and yields a model.
+charges that sum to the formal charge, records of a multi-record file,
+V3000 records read as their V2000 twins, and a round trip of the synthetic
+ligands (PDBQT -> SDF -> PDBQT) that keeps every heavy atom where it was and
+yields a model.
 """
 import numpy as np
 import pytest
@@ -258,3 +259,37 @@ def test_biphenyl_one_torsion_phenol_and_chlorine():
     assert torsdof(p) == 1  # the ring-ring bond; C-O and C-Cl end at one-heavy-neighbour atoms
     m = sb.Model(p)
     assert m.torsdof == 1
+
+
+def sdf3000(name, atoms, bonds, charges=(), split_at=None):
+    """The same molecule as a V3000 record; ``split_at``: an atom whose line is
+    continued onto a second one with a trailing "-"."""
+    chg = dict(charges)
+    out = [name, "  test", "", "  0  0  0     0  0            999 V3000", "M  V30 BEGIN CTAB",
+           f"M  V30 COUNTS {len(atoms)} {len(bonds)} 0 0 0", "M  V30 BEGIN ATOM"]
+    for k, (el, x, y, z) in enumerate(atoms, 1):
+        line = f"M  V30 {k} {el} {x:.4f} {y:.4f} {z:.4f} 0" + (f" CHG={chg[k]}" if k in chg else "")
+        if k == split_at:
+            cut = len(line) // 2
+            out += [line[:cut] + "-", "M  V30 " + line[cut:]]
+        else:
+            out.append(line)
+    out += ["M  V30 END ATOM", "M  V30 BEGIN BOND"]
+    out += [f"M  V30 {k} {o} {i} {j}" for k, (i, j, o) in enumerate(bonds, 1)]
+    out += ["M  V30 END BOND", "M  V30 END CTAB", "M  END", "$$$$"]
+    return "\n".join(out) + "\n"
+
+
+def test_v3000_records_read_as_their_v2000_twins():
+    atoms = [("C", 0, 0, 0), ("C", 1.5, 0, 0), ("O", 2.1, 1.05, 0), ("O", 2.1, -1.05, 0)]
+    bonds = [(1, 2, 1), (2, 3, 2), (2, 4, 1)]
+    for a, b, ch in [(atoms, bonds, [(4, -1)]), (NAPHTHALENE, [(i, j, 4) for i, j in NAPH_EDGES], [])]:
+        assert sb.pdbqt_from_sdf(sdf3000("m", a, b, ch, split_at=2)) == sb.pdbqt_from_sdf(sdf("m", a, b, ch))
+    src = sb.make_ligand_pdbqt(24, 5, 11)
+    el = {"C": "C", "A": "C", "N": "N", "NA": "N", "OA": "O", "SA": "S", "HD": "H", "Cl": "Cl", "F": "F",
+          "Br": "Br", "I": "I", "P": "P", "S": "S", "O": "O"}
+    syn = [(el[r[1]], r[2], r[3], r[4]) for r in atoms_of(src)]
+    sb_ = _bonds_by_distance(syn)
+    assert sb.pdbqt_from_sdf(sdf3000("s", syn, sb_)) == sb.pdbqt_from_sdf(sdf("s", syn, sb_))
+    with pytest.raises(sb.SminaError):  # counts that do not match the blocks
+        sb.pdbqt_from_sdf(sdf3000("m", atoms, bonds).replace("COUNTS 4 3", "COUNTS 5 3"))
