@@ -5,7 +5,8 @@
  * 50-627): hydrogens added, non-polar hydrogens deleted with their partial
  * charges moved to their heavy atom, rigid fragments cut at rotatable
  * bonds, the root fragment the one holding the atom whose removal leaves
- * the smallest largest piece, branches depth first, AutoDock types.  This
+ * the smallest largest piece, branches depth first, AutoDock types (after
+ * StripSalts, which keeps the largest connected piece).  This
  * file does the same steps without OpenBabel, writing the PDBQT text that
  * the PDBQT reader then builds the model from.  What OpenBabel perceived
  * is perceived here by these rules:
@@ -513,8 +514,48 @@ static std::string sdf_record(const std::string& text, int index) {
     throw std::runtime_error("SDF: no record " + std::to_string(index));
 }
 
+// The largest connected piece of the molecule (most atoms; the first of
+// equal ones), as the reference's StripSalts before conversion
+// (molgetter.cpp:107): counter-ions and solvent of a salt record go.
+Mol largest_piece(const Mol& m) {
+    const Graph g(m);
+    const int n = (int)m.atoms.size();
+    std::vector<int> comp(n, -1);
+    std::vector<int> size;
+    for (int s = 0; s < n; s++) {
+        if (comp[s] >= 0) continue;
+        const int c = (int)size.size();
+        size.push_back(0);
+        std::vector<int> st{s};
+        comp[s] = c;
+        while (!st.empty()) {
+            const int v = st.back();
+            st.pop_back();
+            size[c]++;
+            for (auto [w, k] : g.nb[v])
+                if (comp[w] < 0) {
+                    comp[w] = c;
+                    st.push_back(w);
+                }
+        }
+    }
+    if (size.size() <= 1) return m;
+    const int keep = (int)(std::max_element(size.begin(), size.end()) - size.begin());
+    Mol out;
+    out.name = m.name;
+    std::vector<int> at(n, -1);
+    for (int i = 0; i < n; i++)
+        if (comp[i] == keep) {
+            at[i] = (int)out.atoms.size();
+            out.atoms.push_back(m.atoms[i]);
+        }
+    for (const MBond& b : m.bonds)
+        if (at[b.a] >= 0 && at[b.b] >= 0) out.bonds.push_back(MBond{at[b.a], at[b.b], b.order});
+    return out;
+}
+
 std::string pdbqt_from_sdf(const std::string& text, int index, bool add_hydrogens) {
-    Mol m = parse_mol(sdf_record(text, index));
+    Mol m = largest_piece(parse_mol(sdf_record(text, index)));
     if (add_hydrogens) add_polar_hydrogens(m);
     {
         const Graph g(m);

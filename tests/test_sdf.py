@@ -6,7 +6,8 @@ carbon, acceptor nitrogen, polar hydrogens), rotatable bonds (single, not
 amide, not in a ring, both ends with another heavy neighbour), the root
 (the atom whose removal leaves the smallest largest piece), non-polar
 hydrogens deleted with their charge moved to their heavy atom, Gasteiger
-charges that sum to the formal charge, records of a multi-record file,
+charges that sum to the formal charge, a salt stripped to its largest
+piece, records of a multi-record file,
 V3000 records read as their V2000 twins, and a round trip of the synthetic
 ligands (PDBQT -> SDF -> PDBQT) that keeps every heavy atom where it was and
 yields a model.
@@ -293,3 +294,11 @@ def test_v3000_records_read_as_their_v2000_twins():
     assert sb.pdbqt_from_sdf(sdf3000("s", syn, sb_)) == sb.pdbqt_from_sdf(sdf("s", syn, sb_))
     with pytest.raises(sb.SminaError):  # counts that do not match the blocks
         sb.pdbqt_from_sdf(sdf3000("m", atoms, bonds).replace("COUNTS 4 3", "COUNTS 5 3"))
+
+
+def test_salt_stripped_to_its_largest_piece():
+    # sodium acetate: the Na+ counter-ion is a piece of its own and goes (StripSalts)
+    atoms = [("C", 0, 0, 0), ("C", 1.5, 0, 0), ("O", 2.1, 1.05, 0), ("O", 2.1, -1.05, 0)]
+    bonds = [(1, 2, 1), (2, 3, 2), (2, 4, 1)]
+    salt = sdf("NaOAc", atoms + [("Na", 5.0, 0, 0)], bonds, charges=[(4, -1), (5, 1)])
+    assert sb.pdbqt_from_sdf(salt).replace("NaOAc", "m") == sb.pdbqt_from_sdf(sdf("m", atoms, bonds, charges=[(4, -1)]))
