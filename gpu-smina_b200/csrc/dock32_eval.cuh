@@ -1,4 +1,5 @@
-// Mixed-precision path, part 1: one warp evaluates model::eval_deriv in FP32.
+// Mixed-precision path, part 1: one warp, or a team of warps that share out
+// the grid and pair terms, evaluates model::eval_deriv in FP32.
 //
 // Energy, gradient and torsion-tree math run in FP32; the conf (position,
 // orientation quaternion, torsions) stays in FP64 and is narrowed when the

@@ -3,13 +3,14 @@
 // A persistent kernel: every warp takes chains from a global queue (ordered
 // longest first on the host) until the queue is empty, so ligands of very
 // different sizes and step counts share the GPU without a tail.  One warp
+// (or a team of 2 or 4, whose other warps take shares of every evaluation)
 // runs one chain: mutate, BFGS on the hunt-capped energy, Metropolis test,
 // BFGS on the authentic energy for accepted poses, and the chain's output
 // container in global memory.  Confs, the inverse Hessian, the Armijo test
 // and the orientation increment stay in FP64; energies and gradients come
 // from the FP32 evaluation.  Random numbers: Philox4x32-10 keyed by the
 // request seed, counter (draw, ligand key, chain) -- independent of the
-// batch composition and of the launch shape.
+// batch composition and of the launch shape (for a given team size).
 // Reference semantics: monte_carlo.cpp:95-130; mutate.cpp:35-63;
 // bfgs.h:30-282; conf.h:98-404; coords.cpp:25-58 (add_to_output_container).
 #include "dock32_eval.cuh"
